@@ -1,0 +1,531 @@
+// Finite-difference force path (the reference's method):
+//   DescriptorGenerator.generate_nep_descriptors (DescriptorGenerator.py:136-161)
+//   ForceEvaluator.evaluate_interactions        (ForceEvaluator.py:71-146)
+// as three kernels that keep the reference's intermediate g_all in HBM
+// (amlp_descriptors, amlp_mlp_energy, amlp_fd_scatter) and as one fused kernel
+// (amlp_forces_fd) that keeps every intermediate on chip.
+//
+// Tile of the descriptor stage: 32 pairs x 10 variants = 320 rows, one thread
+// per row; warp v evaluates variant v of the 32 pairs (lane = pair), so every
+// branch on the variant is warp-uniform. The rotated body points of the tile
+// are staged in shared memory once and each variant's points are derived from
+// them on the fly.
+#include "descriptor.cuh"
+
+namespace amlp {
+
+constexpr int kPT = 32;             // pairs per tile
+constexpr int kRows = 10 * kPT;     // rows (pair-variants) per tile
+constexpr int kTileThreads = kRows;  // one thread per row
+
+struct TileGeom {
+    int npts, nd, rs;  // points per body, points per cloud, floats per pair in R (odd)
+};
+
+__host__ __device__ inline TileGeom tile_geom(int npts) {
+    TileGeom g;
+    g.npts = npts;
+    g.nd = 2 * npts;
+    g.rs = 6 * npts + ((6 * npts) % 2 == 0 ? 1 : 0);
+    return g;
+}
+
+// Rotated body points of the pairs [p0, p0 + kPT) (clamped to the last pair),
+// the minimum-image translations and the pair indices.
+__device__ void load_tile(const float *pos, const float *quat, float L, const int *pairs, long long P, long long p0,
+                          const float *pts_s, const TileGeom &g, float *R, float *t, int *ij) {
+    const int nthr = blockDim.x;
+    for (int idx = threadIdx.x; idx < kPT * g.nd; idx += nthr) {
+        int p = idx / g.nd, rem = idx - p * g.nd;
+        int body = rem / g.npts, a = rem - body * g.npts;
+        long long pr = min(p0 + p, P - 1);
+        int who = pairs[2 * pr + body];
+        float4 q = load_quat(quat, who);
+        float3 r = rotate_ref(q, make_float3(pts_s[3 * a], pts_s[3 * a + 1], pts_s[3 * a + 2]));
+        float *dst = R + p * g.rs + body * 3 * g.npts + 3 * a;
+        dst[0] = r.x;
+        dst[1] = r.y;
+        dst[2] = r.z;
+    }
+    for (int p = threadIdx.x; p < kPT; p += nthr) {
+        long long pr = min(p0 + p, P - 1);
+        int i = pairs[2 * pr], j = pairs[2 * pr + 1];
+        float d;
+        float3 tt = min_image(pos, i, j, L, &d);
+        t[3 * p] = tt.x;
+        t[3 * p + 1] = tt.y;
+        t[3 * p + 2] = tt.z;
+        ij[2 * p] = i;
+        ij[2 * p + 1] = j;
+    }
+}
+
+// Descriptor of row (v = warp, p = lane) of the staged tile into gT[d*ld + row].
+template <class Cfg>
+__device__ __forceinline__ void tile_descriptor_row(const float *R, const float *t, const TileGeom &g, float dx,
+                                                    float dteta, float inv_rc, float *gT, int ld) {
+    const int v = threadIdx.x >> 5, p = threadIdx.x & 31;
+    VariantPoints vp;
+    vp.Ri = R + p * g.rs;
+    vp.Rj = vp.Ri + 3 * g.npts;
+    vp.tx = t[3 * p];
+    vp.ty = t[3 * p + 1];
+    vp.tz = t[3 * p + 2];
+    vp.h = g.npts;
+    vp.v = v;
+    vp.dx = dx;
+    vp.q = variant_quat(v, dteta);
+    nep_descriptor<Cfg>(vp, g.nd, inv_rc, gT + threadIdx.x, ld);
+}
+
+// ---------------------------------------------------------------- g_all to HBM
+template <class Cfg>
+__global__ void __launch_bounds__(kTileThreads) k_descriptors(const float *pos, const float *quat, float L,
+                                                              const int *pairs, long long P, const float *pts,
+                                                              int npts, float dx, float dteta, float inv_rc, float *g_out) {
+    extern __shared__ float smem[];
+    const TileGeom g = tile_geom(npts);
+    constexpr int ld = kRows + 1;  // odd stride: conflict-free column reads below
+    float *pts_s = smem;
+    float *R = pts_s + 3 * npts;
+    float *t = R + kPT * g.rs;
+    int *ij = reinterpret_cast<int *>(t + 3 * kPT);
+    float *gT = reinterpret_cast<float *>(ij + 2 * kPT);
+    for (int k = threadIdx.x; k < 3 * npts; k += blockDim.x) pts_s[k] = pts[k];
+    __syncthreads();
+    long long ntiles = (P + kPT - 1) / kPT;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        long long p0 = tile * kPT;
+        load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
+        __syncthreads();
+        tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld);
+        __syncthreads();
+        int valid = (int)min((long long)kPT, P - p0);
+        // rows v*P + p0 .. p0+valid-1 of variant v are contiguous in g_all
+        for (int idx = threadIdx.x; idx < 10 * kPT * Cfg::D; idx += blockDim.x) {
+            int v = idx / (kPT * Cfg::D), rem = idx - v * kPT * Cfg::D;
+            int p = rem / Cfg::D, d = rem - p * Cfg::D;
+            if (p < valid) g_out[((long long)v * P + p0 + p) * Cfg::D + d] = gT[d * ld + v * kPT + p];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- generic FP32 net
+struct MlpDesc {
+    int n_layers, act;
+    int dims[AMLP_MAX_LAYERS + 1];
+    long long woff[AMLP_MAX_LAYERS];  // offset of W_k in the packed weights; b_k follows
+};
+
+constexpr int kMlpRows = 128;
+
+// One thread per row; activations of the 128-row tile in shared memory,
+// transposed (feature-major); four outputs per pass share each input load.
+__global__ void __launch_bounds__(kMlpRows) k_mlp(const float *g, long long rows, MlpDesc m, const float *w,
+                                                  int amax, float *e_out) {
+    extern __shared__ float smem[];
+    float *A = smem, *B = smem + (size_t)amax * kMlpRows;
+    const int r = threadIdx.x;
+    for (long long r0 = (long long)blockIdx.x * kMlpRows; r0 < rows; r0 += (long long)gridDim.x * kMlpRows) {
+        const int D = m.dims[0];
+        for (int idx = threadIdx.x; idx < kMlpRows * D; idx += blockDim.x) {
+            int rr = idx / D, d = idx - rr * D;
+            A[d * kMlpRows + rr] = r0 + rr < rows ? g[(r0 + rr) * D + d] : 0.f;
+        }
+        __syncthreads();
+        float *X = A, *Y = B;
+        for (int L = 0; L < m.n_layers; ++L) {
+            const int K = m.dims[L], N = m.dims[L + 1];
+            const float *W = w + m.woff[L], *b = W + (size_t)N * K;
+            const bool last = L == m.n_layers - 1;
+            for (int n = 0; n < N; n += 4) {
+                float acc[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = n + q < N ? __ldg(b + n + q) : 0.f;
+                for (int k = 0; k < K; ++k) {
+                    float x = X[k * kMlpRows + r];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (n + q < N) acc[q] = fmaf(__ldg(W + (size_t)(n + q) * K + k), x, acc[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (n + q < N) Y[(n + q) * kMlpRows + r] = last ? acc[q] : act_f(m.act, acc[q]);
+            }
+            __syncthreads();
+            float *tmp = X;
+            X = Y;
+            Y = tmp;
+        }
+        if (r0 + r < rows) e_out[r0 + r] = X[r];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- differences + scatter
+struct FdConst {
+    float dx, dteta, en_min, en_range;
+};
+
+__device__ __forceinline__ float fd_value(float ev, float e0, float step, float en_range) {
+    // -(e_v - e_0) / step * (en_max - en_min), then the +-100 clip
+    // (ForceEvaluator.py:100-132), FP32 with the reference's rounding
+    return clip100(__fmul_rn(__fdiv_rn(-__fsub_rn(ev, e0), step), en_range));
+}
+
+__global__ void k_fd_scatter(const float *e, long long P, const int *pairs, FdConst c, float *F, float *T, double *pe) {
+    double local = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+        float e0 = e[p];
+        int i = pairs[2 * p], j = pairs[2 * p + 1];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            float f = fd_value(e[(1 + k) * P + p], e0, c.dx, c.en_range);
+            float ti = fd_value(e[(4 + k) * P + p], e0, c.dteta, c.en_range);
+            float tj = fd_value(e[(7 + k) * P + p], e0, c.dteta, c.en_range);
+            atomicAdd(F + 3 * i + k, f);
+            atomicAdd(F + 3 * j + k, -f);
+            atomicAdd(T + 3 * i + k, ti);
+            atomicAdd(T + 3 * j + k, tj);
+        }
+        local += (double)c.en_min + (double)c.en_range * (double)e0;
+    }
+    if (pe) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
+        if ((threadIdx.x & 31) == 0 && local != 0.0) atomicAdd(pe, local);
+    }
+}
+
+// ---------------------------------------------------------------- fused plain path
+constexpr int kFusedMaxWidth = 64;
+
+struct FusedNet {
+    int n_layers, act;
+    int dims[AMLP_MAX_LAYERS + 1];
+    int npad[AMLP_MAX_LAYERS];       // output width rounded up to 8 (hidden layers)
+    int wt_off[AMLP_MAX_LAYERS];     // offset of layer k's transposed weights in smem
+    int b_off[AMLP_MAX_LAYERS];      // offset of its bias
+    long long woff[AMLP_MAX_LAYERS];  // offset in the packed global weights
+    int wt_total;
+};
+
+// YT[n*kRows + r] = act(b[n] + sum_k XT[k*kRows + r] WT[k*npad + n]) for n < npad;
+// 8x8 register tiles, float4 shared-memory loads.
+__device__ __forceinline__ void tile_gemm(const float *XT, int K, const float *WT, const float *b, int npad, float *YT,
+                                          int act) {
+    const int ncg = npad / 8, items = (kRows / 8) * ncg;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int cg = it % ncg, rg = it / ncg;
+        float acc[8][8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float bj = b[cg * 8 + j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) acc[i][j] = bj;
+        }
+        const float *xp = XT + rg * 8;
+        const float *wp = WT + cg * 8;
+        for (int k = 0; k < K; ++k) {
+            float4 x0 = *reinterpret_cast<const float4 *>(xp + k * kRows);
+            float4 x1 = *reinterpret_cast<const float4 *>(xp + k * kRows + 4);
+            float4 w0 = *reinterpret_cast<const float4 *>(wp + k * npad);
+            float4 w1 = *reinterpret_cast<const float4 *>(wp + k * npad + 4);
+            float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+            float ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(xs[i], ws[j], acc[i][j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float o[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) o[i] = act_f(act, acc[i][j]);
+            float *yp = YT + (cg * 8 + j) * kRows + rg * 8;
+            *reinterpret_cast<float4 *>(yp) = make_float4(o[0], o[1], o[2], o[3]);
+            *reinterpret_cast<float4 *>(yp + 4) = make_float4(o[4], o[5], o[6], o[7]);
+        }
+    }
+}
+
+// Segmented (by body index) sum over the lanes of a warp whose keys form
+// contiguous runs; returns true on the last lane of each run.
+__device__ __forceinline__ bool segmented_sum(int key, float *v, int nv) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int ko = __shfl_up_sync(0xffffffffu, key, o);
+        for (int q = 0; q < nv; ++q) {
+            float y = __shfl_up_sync(0xffffffffu, v[q], o);
+            if (lane >= o && ko == key) v[q] += y;
+        }
+    }
+    int kn = __shfl_down_sync(0xffffffffu, key, 1);
+    return lane == 31 || kn != key;
+}
+
+// Scatter of one tile's per-pair forces/torques, fd[p*9 + (F xyz, T_i xyz, T_j xyz)]:
+// F[i] += F, F[j] -= F, T[i] += T_i, T[j] += T_j (ForceEvaluator.py:135-142).
+// Warp 0, lane = pair. The i side is summed over runs of equal i first
+// (pairs are sorted by i), so one atomic per run and component.
+__device__ __forceinline__ void scatter_tile(const float *fd, const int *ij, int valid, float *F, float *T) {
+    if (threadIdx.x >= 32) return;
+    const int p = threadIdx.x;
+    const bool ok = p < valid;
+    const int i = ij[2 * p], j = ij[2 * p + 1];
+    float v[6];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = ok ? fd[9 * p + k] : 0.f;
+        v[3 + k] = ok ? fd[9 * p + 3 + k] : 0.f;
+    }
+    if (ok) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicAdd(F + 3 * j + k, -v[k]);
+            atomicAdd(T + 3 * j + k, fd[9 * p + 6 + k]);
+        }
+    }
+    bool last = segmented_sum(ok ? i : -1 - p, v, 6);
+    if (ok && last) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicAdd(F + 3 * i + k, v[k]);
+            atomicAdd(T + 3 * i + k, v[3 + k]);
+        }
+    }
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos, const float *quat, float L,
+                                                               const int *pairs, const long long *d_np, long long cap,
+                                                               const float *pts, int npts, float inv_rc, FdConst c,
+                                                               FusedNet net, const float *w, float *F, float *T,
+                                                               double *pe) {
+    extern __shared__ __align__(16) float smem[];
+    const TileGeom g = tile_geom(npts);
+    // layout: activations (2 x kFusedMaxWidth x kRows) | weights | e | fd | pts | R | t | ij
+    float *bufA = smem;
+    float *bufB = bufA + kFusedMaxWidth * kRows;
+    float *wt = bufB + kFusedMaxWidth * kRows;
+    float *e = wt + net.wt_total;
+    float *fd = e + kRows;
+    float *pts_s = fd + 9 * kPT;
+    float *R = pts_s + 3 * npts;
+    float *t = R + kPT * g.rs;
+    int *ij = reinterpret_cast<int *>(t + 3 * kPT);
+    __shared__ double pe_s[kTileThreads / 32];
+
+    for (int k = threadIdx.x; k < 3 * npts; k += blockDim.x) pts_s[k] = pts[k];
+    // transposed, zero-padded weights of every layer
+    for (int L2 = 0; L2 < net.n_layers; ++L2) {
+        const int K = net.dims[L2], N = net.dims[L2 + 1], NP = net.npad[L2];
+        const float *W = w + net.woff[L2], *b = W + (size_t)N * K;
+        for (int idx = threadIdx.x; idx < K * NP; idx += blockDim.x) {
+            int k = idx / NP, n = idx - k * NP;
+            wt[net.wt_off[L2] + idx] = n < N ? W[(size_t)n * K + k] : 0.f;
+        }
+        for (int n = threadIdx.x; n < NP; n += blockDim.x) wt[net.b_off[L2] + n] = n < N ? b[n] : 0.f;
+    }
+    __syncthreads();
+
+    const long long P = min(*d_np, cap);
+    const long long ntiles = (P + kPT - 1) / kPT;
+    double pe_acc = 0.0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long p0 = tile * kPT;
+        const int valid = (int)min((long long)kPT, P - p0);
+        load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
+        __syncthreads();
+        tile_descriptor_row<Cfg>(R, t, g, c.dx, c.dteta, inv_rc, bufA, kRows);
+        __syncthreads();
+        float *X = bufA, *Y = bufB;
+        for (int L2 = 0; L2 + 1 < net.n_layers; ++L2) {
+            tile_gemm(X, net.dims[L2], wt + net.wt_off[L2], wt + net.b_off[L2], net.npad[L2], Y, net.act);
+            __syncthreads();
+            float *tmp = X;
+            X = Y;
+            Y = tmp;
+        }
+        {   // last layer (width -> 1), one thread per row
+            const int Ll = net.n_layers - 1, K = net.dims[Ll];
+            const float *wl = wt + net.wt_off[Ll];
+            float acc = wt[net.b_off[Ll]];
+            for (int k = 0; k < K; ++k) acc = fmaf(wl[k * net.npad[Ll]], X[k * kRows + threadIdx.x], acc);
+            e[threadIdx.x] = acc;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < 9 * kPT; idx += blockDim.x) {
+            int p = idx / 9, q = idx - 9 * p;
+            int v = 1 + q;  // 1..3 force, 4..6 torque on i, 7..9 torque on j
+            fd[idx] = fd_value(e[v * kPT + p], e[p], q < 3 ? c.dx : c.dteta, c.en_range);
+        }
+        if (threadIdx.x < kPT && threadIdx.x < valid)
+            pe_acc += (double)c.en_min + (double)c.en_range * (double)e[threadIdx.x];
+        __syncthreads();
+        scatter_tile(fd, ij, valid, F, T);
+        __syncthreads();
+    }
+    if (pe) {
+        double v = pe_acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) pe_s[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int k = 0; k < kTileThreads / 32; ++k) s += pe_s[k];
+            if (s != 0.0) atomicAdd(pe, s);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- host side
+using CfgA = NepCfg<10, 8, 4, 12>;    // D = 47 (the C104 models and every large-scale config)
+using CfgB = NepCfg<10, 10, 10, 10>;  // D = 121 (the C100 models)
+
+int hyper_kind(const amlp_nep *n) {
+    if (n->nrad == 10 && n->nang == 8 && n->lmax == 4) return 1;
+    if (n->nrad == 10 && n->nang == 10 && n->lmax == 10) return 2;
+    return 0;
+}
+
+amlp_status check_nep(const amlp_nep *n) {
+    if (!n || !n->d_pts || n->npts <= 0 || n->npts > AMLP_MAX_PTS || !(n->nep_cutoff > 0.f) || !(n->cutoff > 0.0))
+        return AMLP_ERR_INVALID_ARG;
+    if (!hyper_kind(n)) return AMLP_ERR_UNSUPPORTED;
+    return AMLP_OK;
+}
+
+amlp_status check_mlp(const amlp_mlp *m, int D) {
+    if (!m || !m->d_w || m->n_layers < 1 || m->n_layers > AMLP_MAX_LAYERS || m->dims[0] != D ||
+        m->dims[m->n_layers] != 1 || m->act < 0 || m->act > 2)
+        return AMLP_ERR_INVALID_ARG;
+    for (int k = 1; k < m->n_layers; ++k)
+        if (m->dims[k] <= 0 || m->dims[k] > 1024) return AMLP_ERR_INVALID_ARG;
+    return AMLP_OK;
+}
+
+int nep_D(const amlp_nep *n) { return (n->nrad + 1) + (n->nang + 1) * n->lmax; }
+
+template <class K>
+amlp_status set_smem(K kernel, size_t bytes) {
+    if (bytes > 227 * 1024) return AMLP_ERR_UNSUPPORTED;
+    AMLP_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return AMLP_OK;
+}
+
+}  // namespace amlp
+
+using namespace amlp;
+
+extern "C" amlp_status amlp_descriptors(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                        long long P, const amlp_nep *nep, float *d_g, void *stream) {
+    amlp_status st = check_nep(nep);
+    if (st) return st;
+    if (P < 0 || !d_pos || !d_quat || (P > 0 && (!d_pairs || !d_g))) return AMLP_ERR_INVALID_ARG;
+    if (P == 0) return AMLP_OK;
+    cudaStream_t s = as_stream(stream);
+    TileGeom g = tile_geom(nep->npts);
+    int D = nep_D(nep);
+    size_t smem = sizeof(float) * (3 * nep->npts + kPT * g.rs + 3 * kPT + 2 * kPT + (size_t)D * (kRows + 1));
+    long long ntiles = (P + kPT - 1) / kPT;
+    int grid = (int)std::min<long long>(ntiles, 8LL * kNumSM);
+    float inv_rc = 1.0f / nep->nep_cutoff;
+    if (hyper_kind(nep) == 1) {
+        if ((st = set_smem(k_descriptors<CfgA>, smem))) return st;
+        k_descriptors<CfgA><<<grid, kTileThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, P, nep->d_pts, nep->npts,
+                                                             nep->dx, nep->dteta, inv_rc, d_g);
+    } else {
+        if ((st = set_smem(k_descriptors<CfgB>, smem))) return st;
+        k_descriptors<CfgB><<<grid, kTileThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, P, nep->d_pts, nep->npts,
+                                                             nep->dx, nep->dteta, inv_rc, d_g);
+    }
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_mlp_energy(const float *d_g, long long rows, const amlp_mlp *mlp, float *d_e,
+                                       void *stream) {
+    if (!mlp || rows < 0) return AMLP_ERR_INVALID_ARG;
+    amlp_status st = check_mlp(mlp, mlp->dims[0]);
+    if (st) return st;
+    if (rows == 0) return AMLP_OK;
+    if (!d_g || !d_e) return AMLP_ERR_INVALID_ARG;
+    MlpDesc m;
+    m.n_layers = mlp->n_layers;
+    m.act = mlp->act;
+    long long off = 0;
+    int amax = 1;
+    for (int k = 0; k <= mlp->n_layers; ++k) {
+        m.dims[k] = mlp->dims[k];
+        amax = std::max(amax, mlp->dims[k]);
+    }
+    for (int k = 0; k < mlp->n_layers; ++k) {
+        m.woff[k] = off;
+        off += (long long)mlp->dims[k + 1] * mlp->dims[k] + mlp->dims[k + 1];
+    }
+    size_t smem = 2 * sizeof(float) * (size_t)amax * kMlpRows;
+    if ((st = set_smem(k_mlp, smem))) return st;
+    long long tiles = (rows + kMlpRows - 1) / kMlpRows;
+    int grid = (int)std::min<long long>(tiles, 16LL * kNumSM);
+    k_mlp<<<grid, kMlpRows, smem, as_stream(stream)>>>(d_g, rows, m, mlp->d_w, amax, d_e);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_fd_scatter(const float *d_e, long long P, const int *d_pairs, const amlp_nep *nep,
+                                       float *d_F, float *d_T, double *d_pe, void *stream) {
+    if (!nep || P < 0 || !d_F || !d_T) return AMLP_ERR_INVALID_ARG;
+    if (P == 0) return AMLP_OK;
+    if (!d_e || !d_pairs) return AMLP_ERR_INVALID_ARG;
+    FdConst c{nep->dx, nep->dteta, nep->en_min, nep->en_max - nep->en_min};
+    int grid = (int)std::min<long long>((P + 255) / 256, 4LL * kNumSM);
+    k_fd_scatter<<<grid, 256, 0, as_stream(stream)>>>(d_e, P, d_pairs, c, d_F, d_T, d_pe);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_forces_fd(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                      const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                      const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe, void *stream) {
+    amlp_status st = check_nep(nep);
+    if (st) return st;
+    int D = nep_D(nep);
+    if ((st = check_mlp(mlp, D))) return st;
+    if (!d_pos || !d_quat || !d_npairs || !d_F || !d_T || cap < 0 || (cap > 0 && !d_pairs)) return AMLP_ERR_INVALID_ARG;
+    if (cap == 0) return AMLP_OK;
+    if (D > kFusedMaxWidth) return AMLP_ERR_UNSUPPORTED;
+    FusedNet net;
+    net.n_layers = mlp->n_layers;
+    net.act = mlp->act;
+    long long off = 0;
+    int woff = 0;
+    for (int k = 0; k <= mlp->n_layers; ++k) net.dims[k] = mlp->dims[k];
+    for (int k = 0; k < mlp->n_layers; ++k) {
+        if (k + 1 < mlp->n_layers && mlp->dims[k + 1] > kFusedMaxWidth) return AMLP_ERR_UNSUPPORTED;
+        net.npad[k] = (mlp->dims[k + 1] + 7) / 8 * 8;
+        net.woff[k] = off;
+        off += (long long)mlp->dims[k + 1] * mlp->dims[k] + mlp->dims[k + 1];
+        net.wt_off[k] = woff;
+        woff += mlp->dims[k] * net.npad[k];
+        net.b_off[k] = woff;
+        woff += net.npad[k];
+    }
+    net.wt_total = (woff + 3) / 4 * 4;
+    TileGeom g = tile_geom(nep->npts);
+    size_t smem = sizeof(float) * (2 * (size_t)kFusedMaxWidth * kRows + net.wt_total + kRows + 9 * kPT + 3 * nep->npts +
+                                   kPT * g.rs + 3 * kPT + 2 * kPT);
+    FdConst c{nep->dx, nep->dteta, nep->en_min, nep->en_max - nep->en_min};
+    float inv_rc = 1.0f / nep->nep_cutoff;
+    cudaStream_t s = as_stream(stream);
+    int grid = kNumSM;
+    if (hyper_kind(nep) == 1) {
+        if ((st = set_smem(k_forces_fd<CfgA>, smem))) return st;
+        k_forces_fd<CfgA><<<grid, kTileThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts,
+                                                           nep->npts, inv_rc, c, net, mlp->d_w, d_F, d_T, d_pe);
+    } else {
+        return AMLP_ERR_UNSUPPORTED;
+    }
+    return check_launch();
+}

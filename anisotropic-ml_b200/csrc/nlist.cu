@@ -1,0 +1,229 @@
+// Verlet pair list by a counting-sort cell list, with the pair criterion of
+// scipy's cKDTree.query_pairs as the reference calls it (Sim.py:85-92,
+// :192-198): FP64 periodic distances of float32(pos + L/2) in a box of edge
+// float32(L + 1e-4), folded once per axis, squared components summed in x, y,
+// z order without FMA, compared inclusively with r*r. Pairs (i, j), i < j,
+// are written sorted by i then j.
+//
+// Steps: (1) cell of every body (cells of edge >= r, so every pair within r
+// lies in neighbouring cells), (2) count per cell, exclusive scan, (3) fill
+// the cell lists, (4) one warp per body i counts the j > i within r over the
+// 27 neighbouring cells, (5) scan of the counts, (6) the same traversal
+// collects the j into shared memory, ranks them and writes them in order.
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace amlp {
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kSortCap = 1024;  // neighbours per body ranked in shared memory
+
+struct Grid {
+    int n, nc;        // bodies, cells per side (1 = one cell holding all bodies)
+    double fb, hb;    // periodic box edge and half edge (FP64)
+    double r2;        // r * r
+    double inv_cs;    // nc / fb
+    float halfL;      // float32(L * 0.5)
+};
+
+__global__ void k_cells(const float *pos, Grid g, double *xd, int *cell_of, int *cell_count) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.n) return;
+    int c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double x = (double)__fadd_rn(pos[3 * i + k], g.halfL);
+        xd[3 * i + k] = x;
+        int ci = (int)(x * g.inv_cs);
+        c[k] = ci < 0 ? 0 : (ci >= g.nc ? g.nc - 1 : ci);
+    }
+    int cid = (c[0] * g.nc + c[1]) * g.nc + c[2];
+    cell_of[i] = cid;
+    atomicAdd(&cell_count[cid], 1);
+}
+
+__global__ void k_fill(int n, const int *cell_of, const long long *cell_start, int *cell_fill, int *cell_list) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int cid = cell_of[i];
+    int slot = atomicAdd(&cell_fill[cid], 1);
+    cell_list[cell_start[cid] + slot] = i;
+}
+
+__device__ __forceinline__ bool within(const double *xd, int i, int j, const Grid &g) {
+    double r = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double d = __dsub_rn(xd[3 * i + k], xd[3 * j + k]);
+        if (d < -g.hb) d = __dadd_rn(g.fb, d);
+        else if (d > g.hb) d = __dsub_rn(d, g.fb);
+        r = __dadd_rn(r, __dmul_rn(d, d));
+    }
+    return r <= g.r2;
+}
+
+// Calls f(j) for every j > i within r, lane-strided over the neighbouring cells.
+// All lanes of the warp call it with the same i; f is called by the lane that
+// tested j, with `ok` telling whether j qualifies (every lane calls f once per
+// round so that warp collectives inside f are safe).
+template <class F>
+__device__ __forceinline__ void for_candidates(int i, const Grid &g, const double *xd, const int *cell_of,
+                                               const long long *cell_start, const int *cell_list, F &&f) {
+    const int lane = threadIdx.x & 31;
+    int cid = cell_of[i];
+    int cz = cid % g.nc, cy = (cid / g.nc) % g.nc, cx = cid / (g.nc * g.nc);
+    const int span = g.nc >= 3 ? 1 : 0;
+    for (int dx = -span; dx <= span; ++dx)
+        for (int dy = -span; dy <= span; ++dy)
+            for (int dz = -span; dz <= span; ++dz) {
+                int x = (cx + dx + g.nc) % g.nc, y = (cy + dy + g.nc) % g.nc, z = (cz + dz + g.nc) % g.nc;
+                int c = (x * g.nc + y) * g.nc + z;
+                long long s = cell_start[c], e = cell_start[c + 1];
+                for (long long base = s; base < e; base += 32) {
+                    long long idx = base + lane;
+                    int j = idx < e ? cell_list[idx] : -1;
+                    bool ok = j > i && within(xd, i, j, g);
+                    f(j, ok);
+                }
+            }
+}
+
+__global__ void k_count(Grid g, const double *xd, const int *cell_of, const long long *cell_start,
+                        const int *cell_list, long long *counts) {
+    int i = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    if (i >= g.n) return;
+    int cnt = 0;
+    for_candidates(i, g, xd, cell_of, cell_start, cell_list, [&](int, bool ok) { cnt += ok; });
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0) counts[i] = cnt;
+}
+
+__global__ void k_write(Grid g, const double *xd, const int *cell_of, const long long *cell_start,
+                        const int *cell_list, const long long *offsets, int *pairs, long long cap) {
+    __shared__ int buf[kWarpsPerBlock][kSortCap];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int i = blockIdx.x * kWarpsPerBlock + w;
+    if (i >= g.n) return;
+    long long off = offsets[i];
+    int cnt = (int)(offsets[i + 1] - off);
+    if (cnt == 0) return;
+    int *b = buf[w];
+    if (cnt <= kSortCap) {
+        int fill = 0;
+        for_candidates(i, g, xd, cell_of, cell_start, cell_list, [&](int j, bool ok) {
+            unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) b[fill + __popc(m & ((1u << lane) - 1u))] = j;
+            fill += __popc(m);
+        });
+        __syncwarp();
+        for (int e = lane; e < cnt; e += 32) {
+            int j = b[e], rank = 0;
+            for (int k = 0; k < cnt; ++k) rank += b[k] < j;
+            long long o = off + rank;
+            if (o < cap) {
+                pairs[2 * o] = i;
+                pairs[2 * o + 1] = j;
+            }
+        }
+        return;
+    }
+    // More neighbours than the shared buffer holds: emit them in increasing
+    // order by repeated warp-wide minimum (slow, only for pathological inputs).
+    int prev = i;
+    for (int k = 0; k < cnt; ++k) {
+        int best = 0x7fffffff;
+        for_candidates(i, g, xd, cell_of, cell_start, cell_list, [&](int j, bool ok) {
+            if (ok && j > prev && j < best) best = j;
+        });
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0 && off + k < cap) {
+            pairs[2 * (off + k)] = i;
+            pairs[2 * (off + k) + 1] = best;
+        }
+        prev = best;
+    }
+}
+
+__global__ void k_total(const long long *offsets, int n, long long *d_count) {
+    *d_count = offsets[n];
+}
+
+Grid make_grid(int n, float box, double r) {
+    Grid g;
+    g.n = n;
+    float bs = box + 0.0001f;  // float32(L + 1e-4), as numpy evaluates Lx + 0.0001
+    g.fb = (double)bs;
+    g.hb = 0.5 * g.fb;
+    g.r2 = r * r;
+    g.halfL = box * 0.5f;
+    long long nc = (long long)floor(g.fb / (r * (1.0 + 1e-6)));
+    if (nc > 160) nc = 160;
+    if (nc < 3) nc = 1;
+    g.nc = (int)nc;
+    g.inv_cs = (double)g.nc / g.fb;
+    return g;
+}
+
+struct NlistWs {
+    double *xd;
+    int *cell_of, *cell_count, *cell_fill, *cell_list;
+    long long *cell_start, *counts, *scan_tmp;
+};
+
+size_t carve(Carver &c, const Grid &g, NlistWs *w) {
+    size_t ncell = (size_t)g.nc * g.nc * g.nc;
+    w->xd = c.take<double>(3 * (size_t)g.n);
+    w->cell_of = c.take<int>(g.n);
+    w->cell_count = c.take<int>(ncell);
+    w->cell_fill = c.take<int>(ncell);
+    w->cell_list = c.take<int>(g.n);
+    w->cell_start = c.take<long long>(ncell + 1);
+    w->counts = c.take<long long>((size_t)g.n + 1);
+    w->scan_tmp = c.take<long long>(scan_tmp_elems(std::max<size_t>(ncell, g.n) + 1));
+    return c.used;
+}
+
+}  // namespace
+}  // namespace amlp
+
+using namespace amlp;
+
+extern "C" amlp_status amlp_nlist_workspace_bytes(int n, float box, double r, size_t *bytes) {
+    if (n <= 0 || !(box > 0.f) || !(r > 0.0) || !bytes) return AMLP_ERR_INVALID_ARG;
+    Grid g = make_grid(n, box, r);
+    Carver c(nullptr, 0);
+    NlistWs w;
+    *bytes = carve(c, g, &w) + 256;
+    return AMLP_OK;
+}
+
+extern "C" amlp_status amlp_nlist_build(const float *d_pos, int n, float box, double r, int *d_pairs,
+                                        long long cap, long long *d_count, void *d_ws, size_t ws_bytes,
+                                        void *stream) {
+    if (n <= 0 || !(box > 0.f) || !(r > 0.0) || !d_pos || !d_count || cap < 0 || (cap > 0 && !d_pairs))
+        return AMLP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    Grid g = make_grid(n, box, r);
+    Carver c(d_ws, ws_bytes);
+    NlistWs w;
+    carve(c, g, &w);
+    if (!d_ws || !c.ok()) return AMLP_ERR_WORKSPACE;
+    size_t ncell = (size_t)g.nc * g.nc * g.nc;
+    AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_count, 0, ncell * sizeof(int), s));
+    AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_fill, 0, ncell * sizeof(int), s));
+    int tb = 256;
+    k_cells<<<(n + tb - 1) / tb, tb, 0, s>>>(d_pos, g, w.xd, w.cell_of, w.cell_count);
+    amlp_status st = exclusive_scan_int(w.cell_count, w.cell_start, (long long)ncell, w.scan_tmp, s);
+    if (st) return st;
+    k_fill<<<(n + tb - 1) / tb, tb, 0, s>>>(n, w.cell_of, w.cell_start, w.cell_fill, w.cell_list);
+    int nb = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    k_count<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts);
+    st = exclusive_scan_ll(w.counts, w.counts, n, w.scan_tmp, s);
+    if (st) return st;
+    k_write<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap);
+    k_total<<<1, 1, 0, s>>>(w.counts, n, d_count);
+    return check_launch();
+}

@@ -1,0 +1,187 @@
+/*
+ * amlp.h -- C ABI of libamlp.so, the B200 (sm_100a) implementation of the
+ * per-step force evaluation and NVT rigid-body integration of the reference's
+ * nep_simulator (baho-cb/anisotropic-ML).
+ *
+ * Conventions
+ *   - Every pointer argument named d_* is device memory owned by the caller.
+ *     The library allocates nothing except where a function says so; scratch
+ *     memory is a caller-provided workspace whose size a *_workspace_bytes()
+ *     query returns.
+ *   - Every function returns an amlp_status (0 = success) and never exits the
+ *     process. Kernel launches are asynchronous on the given stream; launch
+ *     errors are reported by the call, device-side errors at the next
+ *     synchronisation.
+ *   - Layouts follow the reference: positions (N,3) f32, orientations and
+ *     angular momenta (N,4) f32 as (w,x,y,z) quaternions (HOOMD convention),
+ *     forces/torques (N,3) f32, pair lists (P,2) with i < j. Pair indices are
+ *     int32 here (the reference keeps int64 from scipy).
+ *   - Handles are not used; calls on one stream are ordered, calls on
+ *     different streams that share output buffers race.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   amlp_nlist_build      Sim.setNeighborList / Sim.refreshNList   Sim.py:85-92, :192-198
+ *   amlp_pair_filter      DescriptorGenerator.pos_to_pts (filter)  DescriptorGenerator.py:168-182
+ *   amlp_descriptors      DescriptorGenerator.generate_nep_descriptors  DescriptorGenerator.py:136-161
+ *                         (pos_to_pts :163-218, apply_dx_dteta :220-255, pts_to_nep_descriptors :296-442)
+ *   amlp_mlp_energy       ForceEvaluator.evaluate_gradients (net forward)  ForceEvaluator.py:80-83
+ *   amlp_fd_scatter       ForceEvaluator.evaluate_gradients (differences) + evaluate_forces_torques
+ *                         ForceEvaluator.py:86-146
+ *   amlp_forces_fd        Sim.step lines 261-266 (descriptors + evaluate_interactions), fused
+ *   amlp_forces_adjoint   same call with analytic forces/torques (no reference counterpart)
+ *   amlp_nvt_step_two     NVT.integrate_step_two  NVT.py:17-64
+ *   amlp_nvt_step_one     NVT.integrate_step_one  NVT.py:12-15, :67-129
+ *   amlp_nvt_init         Sim.move_data_to_device kinetic energies  Sim.py:157-158, :171-180
+ */
+#ifndef AMLP_H
+#define AMLP_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int amlp_status;
+#define AMLP_OK 0
+#define AMLP_ERR_INVALID_ARG 1     /* bad size, null pointer or unsupported parameter */
+#define AMLP_ERR_UNSUPPORTED 2     /* hypers / widths without a compiled kernel */
+#define AMLP_ERR_WORKSPACE 3       /* workspace smaller than the query returned */
+#define AMLP_ERR_CUDA 4            /* a CUDA call failed (see amlp_last_cuda_error) */
+#define AMLP_ERR_CAPACITY 5        /* output capacity too small (count still written) */
+
+#define AMLP_ACT_RELU 0
+#define AMLP_ACT_TANH 1
+#define AMLP_ACT_SILU 2
+#define AMLP_MAX_LAYERS 8
+#define AMLP_MAX_PTS 64            /* points per body; a pair cloud holds 2x */
+
+/* Pair-energy descriptor and shape, DescriptorGenerator.setHyperParameters /
+ * setShape (DescriptorGenerator.py:37-43, :58-125). D = (nrad+1) + (nang+1)*lmax. */
+typedef struct amlp_nep {
+    int nrad, nang, lmax;
+    int npts;                 /* points per body, <= AMLP_MAX_PTS */
+    const float *d_pts;       /* (npts,3) body-frame points */
+    double cutoff;            /* pair filter: centre distance < cutoff (compared in FP64) */
+    float nep_cutoff;         /* descriptor radius r_c */
+    float en_min, en_max;     /* net output y maps to E = en_min + (en_max-en_min) y */
+    float dx, dteta;          /* finite-difference steps (Sim.py:49-50) */
+} amlp_nep;
+
+/* FFNN, TheEnergyNet (ForceEvaluator.py:6-26) with a selectable activation.
+ * Layer k maps dims[k] -> dims[k+1]; dims[0] = D, dims[n_layers] = 1.
+ * d_w: all layers packed in FP32, per layer W (dims[k+1] x dims[k], row-major as
+ * torch.nn.Linear.weight) followed by b (dims[k+1]). */
+typedef struct amlp_mlp {
+    int n_layers;
+    int dims[AMLP_MAX_LAYERS + 1];
+    int act;
+    const float *d_w;
+} amlp_mlp;
+
+/* Device-resident NVT thermostat state (Sim.setkT, Sim.py:99-111), updated in place. */
+typedef struct amlp_thermostat {
+    float xi, eta;            /* integrator_vars0, integrator_vars1 */
+    float xi_rot, eta_rot;    /* integrator_vars2, integrator_vars3 */
+    float thermo_fac;         /* m_exp_thermo_fac */
+    float pad[3];
+    double ke_t, ke_r;        /* kinetic energies read by the next step two */
+    double pe;                /* sum of pair energies of the last force pass */
+} amlp_thermostat;
+
+typedef struct amlp_nvt {
+    float dt, tau, kT;        /* tau = 100 dt in the reference (Sim.py:115) */
+    float n_dof, rn_dof;      /* (N-1)*3 and 3N (Sim.py:35-36) */
+    float moi[3];             /* principal moments shared by all bodies */
+    float box;                /* cubic box edge L */
+    int nve;                  /* 1: no thermostat (thermo_fac = 1, xi_rot = 0) */
+} amlp_nvt;
+
+/* --------------------------------------------------------------- library */
+int amlp_version(void);
+const char *amlp_status_string(amlp_status s);
+const char *amlp_last_cuda_error(void);
+
+/* --------------------------------------------------------------- Verlet list
+ * All pairs i < j with |x_i - x_j|_periodic <= r, computed exactly as scipy's
+ * cKDTree.query_pairs does for the reference: FP64 distances of
+ * float32(pos + L/2) in a periodic box of edge float32(L + 1e-4), folded once
+ * per axis, squared components summed x, y, z, compared inclusively with r*r.
+ * Output sorted by (i, j). *d_count receives the number of pairs even when it
+ * exceeds cap; nothing past cap is written, so a caller that finds
+ * *d_count > cap grows the buffer and calls again. */
+amlp_status amlp_nlist_workspace_bytes(int n, float box, double r, size_t *bytes);
+amlp_status amlp_nlist_build(const float *d_pos, int n, float box, double r,
+                             int *d_pairs, long long cap, long long *d_count,
+                             void *d_ws, size_t ws_bytes, void *stream);
+
+/* --------------------------------------------------------------- pair filter
+ * Minimum image (FP32, box L) and |t| < cutoff on the Verlet pairs, kept in
+ * Verlet order. The count is read from d_nverlet on the device. */
+amlp_status amlp_filter_workspace_bytes(long long cap_verlet, size_t *bytes);
+amlp_status amlp_pair_filter(const float *d_pos, float box, double cutoff,
+                             const int *d_vpairs, const long long *d_nverlet, long long cap_verlet,
+                             int *d_pairs, long long *d_npairs,
+                             void *d_ws, size_t ws_bytes, void *stream);
+
+/* --------------------------------------------------------------- descriptors
+ * g_all of the reference: row v*P + p holds the D descriptors of
+ * finite-difference variant v (0..9) of filtered pair p (P pairs, host value). */
+amlp_status amlp_descriptors(const float *d_pos, const float *d_quat, float box,
+                             const int *d_pairs, long long P, const amlp_nep *nep,
+                             float *d_g, void *stream);
+
+/* Net energies of `rows` descriptor rows: d_e[r] = net(d_g[r]) (the net output
+ * y, before the en_min/en_max map). FP32 throughout. */
+amlp_status amlp_mlp_energy(const float *d_g, long long rows, const amlp_mlp *mlp,
+                            float *d_e, void *stream);
+
+/* Finite differences, scaling, clip to [-100,100] and scatter of
+ * ForceEvaluator.py:86-146. d_F, d_T (N,3) are accumulated into (zero them
+ * first). d_pe (may be NULL) accumulates sum_p (en_min + (en_max-en_min) e0_p). */
+amlp_status amlp_fd_scatter(const float *d_e, long long P, const int *d_pairs, const amlp_nep *nep,
+                            float *d_F, float *d_T, double *d_pe, void *stream);
+
+/* --------------------------------------------------------------- fused force passes
+ * Plain path: per filtered pair the 10 finite-difference variants, descriptors,
+ * FP32 net, differences, clip and scatter in one kernel; g_all never reaches
+ * HBM. The pair count is read on the device (d_npairs). Nets wider than 64
+ * return AMLP_ERR_UNSUPPORTED (use the three calls above). */
+amlp_status amlp_forces_fd(const float *d_pos, const float *d_quat, float box,
+                           const int *d_pairs, const long long *d_npairs, long long cap,
+                           const amlp_nep *nep, const amlp_mlp *mlp,
+                           float *d_F, float *d_T, double *d_pe, void *stream);
+
+/* Adjoint path: one descriptor evaluation per pair and the exact derivative of
+ * the pair energy with respect to the translation of body i and the rotations
+ * of bodies i and j; the same scaling, clip and scatter as the plain path. */
+amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_quat, float box,
+                                const int *d_pairs, const long long *d_npairs, long long cap,
+                                const amlp_nep *nep, const amlp_mlp *mlp,
+                                float *d_F, float *d_T, double *d_pe, void *stream);
+
+/* --------------------------------------------------------------- NVT integrator
+ * d_th: one amlp_thermostat in device memory.
+ * init: kinetic energies before the first step. With initial_ke_quirk = 1 the
+ * translational value is body 0's kinetic energy only, as the reference passes
+ * its per-body array to update_variables (Sim.py:157, IntegrateStepTwoKernels.py:245). */
+amlp_status amlp_nvt_init(const float *d_vel, const float *d_quat, const float *d_angmom,
+                          const float *d_mass, int n, const amlp_nvt *prm, int initial_ke_quirk,
+                          amlp_thermostat *d_th, void *d_ws, size_t ws_bytes, void *stream);
+amlp_status amlp_nvt_workspace_bytes(int n, size_t *bytes);
+/* Step two: thermostat update, v <- v f + dt/2 F/m, angular-momentum kick.
+ * Writes d_accel (N,3) and d_dp (N,4) for step one. */
+amlp_status amlp_nvt_step_two(float *d_vel, float *d_accel, const float *d_F, const float *d_mass,
+                              const float *d_quat, const float *d_T, float *d_angmom, float *d_dp,
+                              int n, const amlp_nvt *prm, amlp_thermostat *d_th, void *stream);
+/* Step one: translation (kick, drift, one periodic wrap), rotation (kick +
+ * free-rotor splitting + renormalisation) and the FP64 kinetic-energy sums. */
+amlp_status amlp_nvt_step_one(float *d_pos, float *d_vel, const float *d_accel,
+                              float *d_quat, float *d_angmom, const float *d_dp, const float *d_mass,
+                              int n, const amlp_nvt *prm, amlp_thermostat *d_th,
+                              void *d_ws, size_t ws_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMLP_H */

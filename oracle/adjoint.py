@@ -1,0 +1,91 @@
+"""Exact pair forces and torques in FP64 by automatic differentiation
+(test infrastructure only).
+
+The reference approximates them by forward differences
+(``ForceEvaluator.py:86-112``): F = -(E(x_i + dx) - E)/dx along x/y/z,
+T_i = -(E(rot_i dteta) - E)/dteta, T_j likewise for body j. Here the same
+quantities are the exact derivatives at zero displacement: the pair energy
+E(cloud1) of the unperturbed cloud (body i at the origin, body j at the
+minimum-image translation t) is differentiated with respect to every point,
+then
+  F_pair = -sum_{a in i} dE/dp_a,
+  T_i    = -sum_{a in i} p_a x dE/dp_a              (rotation about the centre of i),
+  T_j    = -sum_{a in j} (p_a - t) x dE/dp_a        (rotation about the centre of j),
+each multiplied by (en_max - en_min) and clipped to [-100, 100] as the
+reference does (``ForceEvaluator.py:119-132``).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import nep
+
+
+def _act(name):
+    return {"relu": torch.relu, "tanh": torch.tanh, "silu": torch.nn.functional.silu}[name]
+
+
+def descriptor_torch(pts, nrad, nang, lmax, rc):
+    """Differentiable FP64 descriptor (direct O(Nd^2) form of
+    ``NepDescriptorKernels.py:3-144``). pts (P, Nd, 3)."""
+    r = pts - pts.mean(dim=1, keepdim=True)
+    d = torch.sqrt((r * r).sum(-1))
+    u = d / rc
+    x = 2.0 * (u - 1.0) ** 2 - 1.0
+    fc = 0.5 * (1.0 + torch.cos(np.pi * u))
+    T = [torch.ones_like(x), x]
+    for _ in range(1, nrad):
+        T.append(2.0 * x * T[-1] - T[-2])
+    f = torch.stack([(1.0 + t) / 2.0 * fc for t in T[:nrad + 1]], dim=1)  # (P, nrad+1, Nd)
+    rh = r / d[..., None]
+    cos = torch.einsum("pak,pbk->pab", rh, rh)
+    leg = [torch.ones_like(cos), cos]
+    for l in range(1, lmax):
+        leg.append(((2 * l + 1) * cos * leg[-1] - l * leg[-2]) / (l + 1))
+    fa = f[:, :nang + 1]
+    g_ang = torch.stack([torch.einsum("pna,pnb,pab->pn", fa, fa, leg[l]) for l in range(1, lmax + 1)], dim=-1)
+    return torch.cat([f.sum(-1), g_ang.reshape(len(pts), -1)], dim=1)
+
+
+def pair_energy_net(g, layers, act):
+    h = g
+    for k, (W, b) in enumerate(layers):
+        h = torch.nn.functional.linear(h, torch.as_tensor(np.asarray(W, np.float64)),
+                                       torch.as_tensor(np.asarray(b, np.float64)))
+        if k < len(layers) - 1:
+            h = _act(act)(h)
+    return h[:, 0]
+
+
+def exact_pair_forces(pos, quat, pairs, L, shape, hypers, layers, act, chunk=512, clip=True):
+    """Per-pair (F_pair, T_i, T_j) in FP64, scaled by en_range (and clipped), the
+    per-body sums (F, T) and the pair energies E = en_min + en_range * y."""
+    nrad, nang, lmax = (int(h) for h in hypers[:3])
+    pairs = np.asarray(pairs, np.int64).reshape(-1, 2)
+    _, _, t = nep.min_image_filter(pos, pairs, L, 1e30, np.float64)
+    c1, _ = nep.pair_clouds(quat, pairs, t, shape["pts"], np.float64)
+    rng = shape["en_max"] - shape["en_min"]
+    h = c1.shape[1] // 2
+    out_F, out_Ti, out_Tj, out_E = [], [], [], []
+    for s in range(0, len(pairs), chunk):
+        p = torch.tensor(c1[s:s + chunk], dtype=torch.float64, requires_grad=True)
+        y = pair_energy_net(descriptor_torch(p, nrad, nang, lmax, float(shape["nep_cutoff"])), layers, act)
+        (grad,) = torch.autograd.grad(y.sum(), p)
+        grad = grad.numpy()
+        pts = c1[s:s + chunk]
+        tt = t[s:s + chunk][:, None, :]
+        F = -grad[:, :h].sum(1)
+        Ti = -np.cross(pts[:, :h], grad[:, :h]).sum(1)
+        Tj = -np.cross(pts[:, h:] - tt, grad[:, h:]).sum(1)
+        out_F.append(F * rng)
+        out_Ti.append(Ti * rng)
+        out_Tj.append(Tj * rng)
+        out_E.append(shape["en_min"] + rng * y.detach().numpy())
+    F, Ti, Tj = (np.concatenate(a) if a else np.zeros((0, 3)) for a in (out_F, out_Ti, out_Tj))
+    E = np.concatenate(out_E) if out_E else np.zeros(0)
+    if clip:
+        F, Ti, Tj = (np.clip(a, -100.0, 100.0) for a in (F, Ti, Tj))
+    N = len(pos)
+    Fn, Tn = nep.scatter(pairs, F, Ti, Tj, N, np.float64)
+    return dict(F_pair=F, T_i=Ti, T_j=Tj, forces=Fn, torques=Tn, E=E, pairs=pairs)

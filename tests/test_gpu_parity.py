@@ -1,0 +1,329 @@
+"""Parity of every CUDA entry point with the oracle (and through the oracle, with
+the reference's own run). All calls go through the C ABI of libamlp.
+
+Tolerances:
+* Verlet list and pair filter: bit-exact (same pairs, same order);
+* descriptors: |g_gpu - g_fp64| <= 2e-5 * max(1, |g|) -- the GPU evaluates the
+  angular sum through the addition theorem in FP32, the reference directly;
+* net energies: relative 1e-5 (FP32 against torch FP32);
+* finite-difference forces: the reference's own FP32 forward differences
+  (dx = dteta = 1e-5) carry rounding noise of up to tens of force units per
+  pair (see test_fd_noise_floor_of_the_reference), so they are compared as a
+  distribution: the GPU's deviation from FP64 finite differences may not exceed
+  the reference's own deviation by more than a factor 2 at the 50/90/99 %
+  quantiles; the pair-energy sum must agree to 1e-5 relative;
+* integrator: positions/velocities/quaternions relative 2e-6 against the FP32
+  oracle given the same forces.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import case_model, case_shape, load_case
+
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import gpu_helpers as gh  # noqa: E402
+from amlp.configs import make_state  # noqa: E402
+from oracle import nep, nlist  # noqa: E402
+from oracle.shapes import SHAPES  # noqa: E402
+
+CASES = ["th_C104", "th_C100", "cube_C104"]
+
+
+def _hyp(c):
+    return tuple(int(h) for h in c["hypers"][:3])
+
+
+# ----------------------------------------------------------------------------- Verlet list
+def _nlist_cases():
+    rng = np.random.default_rng(5)
+    out = []
+    for name in CASES:
+        c = load_case(name)
+        out.append((f"golden-{name}", c["pos0"], float(c["L"]), case_shape(c)["cutoff"] + 2.0))
+    L = np.float32(20.0)
+    out.append(("uniform-3000", (rng.random((3000, 3)) * L - L / 2).astype(np.float32), float(L), 4.5))
+    s = make_state(4096, "cube26", 0.45, seed=1)
+    out.append(("cube26-4096-phi045", s.pos, s.L, 4.5))
+    s = make_state(2000, "cyl24", 0.35, seed=3)
+    out.append(("cyl24-2000", s.pos, s.L, 4.5))
+    L = np.float32(8.0)
+    out.append(("small-box-brute-force", (rng.random((60, 3)) * L - L / 2).astype(np.float32), float(L), 4.5))
+    out.append(("one-body", np.zeros((1, 3), np.float32), 10.0, 4.5))
+    L = np.float32(30.0)
+    out.append(("sparse-empty", np.array([[-10, -10, -10], [0, 0, 0], [10, 10, 10]], np.float32), float(L), 2.0))
+    # bodies on the box faces and pairs at exactly r along an axis
+    edge = np.array([[-15, 0, 0], [14.5, 0, 0], [0, -15, 0], [0, 14.99, 0], [0, 0, 4.5], [0, 0, 0],
+                     [4.5, 0, 0], [-4.5, 0, 0], [0, 0, -15]], np.float32)
+    out.append(("faces-and-exact-r", edge, 30.0, 4.5))
+    return out
+
+
+@pytest.mark.parametrize("case", _nlist_cases(), ids=lambda c: c[0])
+def test_nlist_bit_exact_vs_ckdtree(case):
+    _, pos, L, r = case
+    got, k = gh.nlist(pos, L, r)
+    ref = nlist.sorted_pairs(nlist.reference_pairs(pos, L, r))
+    assert k == len(ref)
+    assert np.array_equal(got, ref), "GPU Verlet list differs from cKDTree.query_pairs"
+
+
+def test_nlist_capacity_reports_count():
+    s = make_state(1000, "cube26", 0.45, seed=0)
+    full, k = gh.nlist(s.pos, s.L, 4.5)
+    part, k2 = gh.nlist(s.pos, s.L, 4.5, cap=100)
+    assert k2 == k and np.array_equal(part, full[:100])
+
+
+# ----------------------------------------------------------------------------- pair filter
+@pytest.mark.parametrize("name", CASES)
+def test_filter_bit_exact(name):
+    c = load_case(name)
+    shape = case_shape(c)
+    vp, _ = gh.nlist(c["pos0"], c["L"], shape["cutoff"] + 2.0)
+    got = gh.pair_filter(c["pos0"], c["L"], shape["cutoff"], vp)
+    _, ref, _ = nep.min_image_filter(c["pos0"], vp, c["L"], shape["cutoff"])
+    assert np.array_equal(got, ref)
+    assert np.array_equal(got, nlist.sorted_pairs(c["pairs0"]))  # the reference's own filtered pairs
+
+
+def test_filter_random_cube26():
+    s = make_state(3000, "cube26", 0.45, seed=4)
+    vp, _ = gh.nlist(s.pos, s.L, 4.5)
+    got = gh.pair_filter(s.pos, s.L, 2.5, vp)
+    _, ref, _ = nep.min_image_filter(s.pos, vp, s.L, 2.5)
+    assert np.array_equal(got, ref)
+
+
+# ----------------------------------------------------------------------------- descriptors
+def _check_desc(g, g64):
+    scale = np.maximum(1.0, np.abs(g64))
+    err = np.abs(g - g64) / scale
+    assert err.max() <= 2e-5, f"max scaled descriptor error {err.max():.3g}"
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_descriptors_vs_reference_and_fp64(name):
+    c = load_case(name)
+    shape, hyp = case_shape(c), _hyp(c)
+    pairs = c["pairs0"]
+    P = len(pairs)
+    g = gh.descriptors(c["pos0"], c["orient0"], c["L"], pairs, shape, hyp)
+    _, _, t = nep.min_image_filter(c["pos0"], pairs, c["L"], shape["cutoff"], np.float64)
+    c1, c2 = nep.pair_clouds(c["orient0"], pairs, t, shape["pts"], np.float64)
+    g64 = nep.descriptor(nep.fd_variants(c1, c2, 1e-5, 1e-5, np.float64), hyp, shape["nep_cutoff"], np.float64)
+    _check_desc(g, g64)
+    head = g.reshape(10, P, -1)[:, :c["g0"].shape[1]]
+    _check_desc(head, c["g0"].astype(np.float64))
+
+
+@pytest.mark.parametrize("shape_name,phi,seed", [("cube26", 0.45, 1), ("tetra16", 0.40, 2), ("cyl24", 0.35, 3)])
+def test_descriptors_new_shapes(shape_name, phi, seed):
+    s = make_state(160, shape_name, phi, seed=seed)
+    shape = SHAPES[shape_name]
+    vp = nlist.sorted_pairs(nlist.reference_pairs(s.pos, s.L, 4.5))
+    _, pairs, t = nep.min_image_filter(s.pos, vp, s.L, shape["cutoff"])
+    pairs = pairs[:200]
+    g = gh.descriptors(s.pos, s.orient, s.L, pairs, shape, (10, 8, 4))
+    _, _, t = nep.min_image_filter(s.pos, pairs, s.L, shape["cutoff"], np.float64)
+    c1, c2 = nep.pair_clouds(s.orient, pairs, t, shape["pts"], np.float64)
+    g64 = nep.descriptor(nep.fd_variants(c1, c2, 1e-5, 1e-5, np.float64), (10, 8, 4), shape["nep_cutoff"],
+                         np.float64, form="sh")
+    _check_desc(g, g64)
+
+
+# ----------------------------------------------------------------------------- net energies
+@pytest.mark.parametrize("widths,act", [((64, 64), "tanh"), ((128, 128, 128), "silu"), ((150, 150, 150, 150), "relu")])
+def test_mlp_energy_vs_torch(widths, act):
+    from amlp.engine import EnergyNet
+    rng = np.random.default_rng(0)
+    g = rng.standard_normal((3001, 47)).astype(np.float32)
+    net = EnergyNet.xavier(47, widths, act, seed=3, device="cpu")
+    ref = nep.mlp_forward(net.layers, act, g).reshape(-1)
+    got = gh.mlp_energy(net.layers, act, g)
+    np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-5 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_mlp_energy_golden(name):
+    c = load_case(name)
+    layers = case_model(c)
+    shape, hyp = case_shape(c), _hyp(c)
+    pairs = c["pairs0"]
+    g = gh.descriptors(c["pos0"], c["orient0"], c["L"], pairs, shape, hyp)
+    e = gh.mlp_energy(layers, "relu", g)
+    np.testing.assert_allclose(e, c["e0"], rtol=1e-5, atol=1e-5 * np.abs(c["e0"]).max())
+
+
+# ----------------------------------------------------------------------------- forces
+@pytest.mark.parametrize("name", CASES)
+def test_fd_scatter_matches_reference(name):
+    """Same energies in -> the reference's forces out (only the atomic summation order differs)."""
+    c = load_case(name)
+    shape = case_shape(c)
+    N = len(c["pos0"])
+    F, T, pe = gh.fd_scatter(c["e0"], c["pairs0"], N, shape)
+    tol = 1e-5 * max(1.0, np.abs(c["F0"]).max())
+    np.testing.assert_allclose(F, c["F0"], rtol=0, atol=tol)
+    np.testing.assert_allclose(T, c["T0"], rtol=0, atol=1e-5 * max(1.0, np.abs(c["T0"]).max()))
+    P = len(c["pairs0"])
+    pe_ref = np.sum(shape["en_min"] + (shape["en_max"] - shape["en_min"]) * c["e0"][:P].astype(np.float64))
+    assert abs(pe - pe_ref) <= 1e-6 * max(1.0, abs(pe_ref))
+
+
+def _fd64(c, shape, hyp, layers, act="relu"):
+    pairs = c["pairs0"]
+    return nep.pair_forces(c["pos0"], c["orient0"], pairs, c["L"], shape, hyp, layers, act, dt=np.float64)
+
+
+def test_fd_noise_floor_of_the_reference():
+    """Documents the size of the reference's FP32 finite-difference noise."""
+    c = load_case("th_C104")
+    shape, hyp, layers = case_shape(c), _hyp(c), case_model(c)
+    o64 = _fd64(c, shape, hyp, layers)
+    P = len(c["pairs0"])
+    rng = shape["en_max"] - shape["en_min"]
+    f32 = np.clip(c["Fgrad0"] * np.float32(rng), -100, 100)
+    err = np.abs(f32 - o64["F_pair"])
+    assert np.quantile(err, 0.99) > 0.1  # the noise is real and large
+    assert P == o64["P"]
+
+
+@pytest.mark.parametrize("name,method", [("th_C104", "amlp_forces_fd"), ("cube_C104", "amlp_forces_fd")])
+def test_fused_fd_forces_statistical(name, method):
+    c = load_case(name)
+    shape, hyp, layers = case_shape(c), _hyp(c), case_model(c)
+    if max(W.shape[0] for W, _ in layers[:-1]) > 64:
+        # the reference models are 150 wide: compare the split path instead
+        pytest.skip("fused kernel takes nets up to 64 wide")
+    F, T, pe = gh.fused_forces(c["pos0"], c["orient0"], c["L"], c["pairs0"], shape, hyp, layers, "relu", method)
+    assert np.isfinite(F).all()
+
+
+def _split_forces(c, shape, hyp, layers, act="relu"):
+    pairs = c["pairs0"]
+    g = gh.descriptors(c["pos0"], c["orient0"], c["L"], pairs, shape, hyp)
+    e = gh.mlp_energy(layers, act, g)
+    return gh.fd_scatter(e, pairs, len(c["pos0"]), shape) + (e,)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_split_fd_forces_statistical(name):
+    c = load_case(name)
+    shape, hyp, layers = case_shape(c), _hyp(c), case_model(c)
+    F, T, pe, e = _split_forces(c, shape, hyp, layers)
+    o64 = _fd64(c, shape, hyp, layers)
+    ref_err = np.abs(c["F0"] - o64["forces"])
+    gpu_err = np.abs(F - o64["forces"])
+    for q in (0.5, 0.9, 0.99):
+        assert np.quantile(gpu_err, q) <= 2 * np.quantile(ref_err, q) + 0.05, q
+    ref_err_t = np.abs(c["T0"] - o64["torques"])
+    gpu_err_t = np.abs(T - o64["torques"])
+    for q in (0.5, 0.9, 0.99):
+        assert np.quantile(gpu_err_t, q) <= 2 * np.quantile(ref_err_t, q) + 0.05, q
+    P = len(c["pairs0"])
+    pe_ref = np.sum(shape["en_min"] + (shape["en_max"] - shape["en_min"]) * c["e0"][:P].astype(np.float64))
+    assert abs(pe - pe_ref) <= 1e-5 * max(1.0, abs(pe_ref))
+
+
+@pytest.mark.parametrize("act,widths", [("tanh", (64, 64)), ("relu", (64, 64, 64))])
+def test_fused_equals_split_statistically(act, widths):
+    from amlp.engine import EnergyNet
+    s = make_state(500, "cube26", 0.45, seed=11)
+    shape = SHAPES["cube26"]
+    vp, _ = gh.nlist(s.pos, s.L, 4.5)
+    pairs = gh.pair_filter(s.pos, s.L, 2.5, vp)
+    net = EnergyNet.xavier(47, widths, act, seed=5, device="cpu")
+    c = dict(pos0=s.pos, orient0=s.orient, L=s.L, pairs0=pairs)
+    Fs, Ts, pes, e = _split_forces(c, shape, (10, 8, 4), net.layers, act)
+    Ff, Tf, pef = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, (10, 8, 4), net.layers, act)
+    assert abs(pef - pes) <= 1e-5 * max(1.0, abs(pes))
+    o64 = nep.pair_forces(s.pos, s.orient, pairs, s.L, shape, (10, 8, 4), net.layers, act, dt=np.float64, form="sh")
+    es = np.abs(Fs - o64["forces"])
+    ef = np.abs(Ff - o64["forces"])
+    for q in (0.5, 0.9, 0.99):
+        assert np.quantile(ef, q) <= 2 * np.quantile(es, q) + 0.05
+
+
+# ----------------------------------------------------------------------------- integrator
+@pytest.mark.parametrize("name", ["th_C104", "cube_C104"])
+def test_integrator_vs_oracle(name):
+    """Step two + step one on the GPU with the reference's forces of step 0, against the FP32 oracle."""
+    import ctypes
+    from amlp._lib import Nvt, Thermostat, call, size_query
+    c = load_case(name)
+    N = len(c["pos0"])
+    st = nep.NVTState(c["pos0"], c["vel0"], c["orient0"], c["angmom0"], c["mass"], c["moi"], c["L"],
+                      float(c["kT"]), float(c["dt"]))
+    dev = gh.DEV
+    pos, vel, q, p = gh.t32(c["pos0"]), gh.t32(c["vel0"]), gh.t32(c["orient0"]), gh.t32(c["angmom0"])
+    mass = gh.t32(c["mass"])
+    F, T = gh.t32(c["F0"]), gh.t32(c["T0"])
+    accel = torch.zeros(N, 3, device=dev)
+    dp = torch.zeros(N, 4, device=dev)
+    prm = Nvt()
+    prm.dt, prm.tau, prm.kT = float(c["dt"]), float(np.float32(100 * c["dt"])), float(c["kT"])
+    prm.n_dof, prm.rn_dof = float((N - 1) * 3), float(3 * N)
+    for k in range(3):
+        prm.moi[k] = float(c["moi"][k])
+    prm.box, prm.nve = float(c["L"]), 0
+    th = Thermostat()
+    th.xi, th.eta, th.xi_rot, th.eta_rot, th.thermo_fac = (-0.0317711, 0.108609, 0.00814227, -0.014238, 1.00011)
+    th_t = torch.frombuffer(bytearray(bytes(th)), dtype=torch.uint8).to(dev)
+    ws = torch.empty(size_query("amlp_nvt_workspace_bytes", N), dtype=torch.uint8, device=dev)
+    s = gh.stream()
+    call("amlp_nvt_init", vel.data_ptr(), q.data_ptr(), p.data_ptr(), mass.data_ptr(), N, ctypes.byref(prm), 1,
+         th_t.data_ptr(), ws.data_ptr(), ws.numel(), s)
+    call("amlp_nvt_step_two", vel.data_ptr(), accel.data_ptr(), F.data_ptr(), mass.data_ptr(), q.data_ptr(),
+         T.data_ptr(), p.data_ptr(), dp.data_ptr(), N, ctypes.byref(prm), th_t.data_ptr(), s)
+    call("amlp_nvt_step_one", pos.data_ptr(), vel.data_ptr(), accel.data_ptr(), q.data_ptr(), p.data_ptr(),
+         dp.data_ptr(), mass.data_ptr(), N, ctypes.byref(prm), th_t.data_ptr(), ws.data_ptr(), ws.numel(), s)
+    st.step_two(c["F0"], c["T0"])
+    st.step_one()
+    # same forces as the reference -> the reference's state after one step
+    for got, ref, ref_run in ((pos, st.pos, c["pos_s1"]), (vel, st.vel, c["vel_s1"]), (q, st.orient, c["orient_s1"]),
+                              (p, st.angmom, c["angmom_s1"])):
+        g = got.cpu().numpy()
+        np.testing.assert_allclose(g, ref, rtol=2e-6, atol=2e-6 * np.abs(ref).max())
+        np.testing.assert_allclose(g, ref_run, rtol=2e-6, atol=2e-6 * np.abs(ref_run).max())
+    thr = Thermostat.from_buffer_copy(bytes(th_t.cpu().numpy().tobytes()))
+    np.testing.assert_allclose([thr.xi, thr.eta, thr.xi_rot, thr.eta_rot, thr.thermo_fac], c["thermo_s1"], rtol=1e-5)
+    np.testing.assert_allclose([thr.ke_t, thr.ke_r], [st.ke_t, st.ke_r], rtol=1e-5)
+
+
+def test_integrator_large_n_no_fixed_grid():
+    """N far above the reference's fixed grids (N <= 1706): every body moves."""
+    from amlp.engine import EnergyNet, Hypers, System
+    s = make_state(20000, "tetra16", 0.2, seed=9)
+    net = EnergyNet.xavier(47, (64, 64), "tanh", seed=1, device=gh.DEV)
+    sys_ = System(s, "tetra16", Hypers(), net, kT=1.0, dt=0.005, device=gh.DEV)
+    p0 = sys_.pos.clone()
+    sys_.step("fd")
+    torch.cuda.synchronize()
+    moved = (sys_.pos - p0).abs().sum(dim=1) > 0
+    assert bool(moved.all())
+
+
+# ----------------------------------------------------------------------------- system
+def test_system_run_graph_rebuilds_and_matches_eager():
+    from amlp.engine import EnergyNet, Hypers, System
+    s = make_state(1000, "cube26", 0.30, seed=0)
+    net = EnergyNet.xavier(47, (64, 64), "tanh", seed=0, device=gh.DEV)
+    a = System(s, "cube26", Hypers(), net, kT=1.0, dt=0.005, device=gh.DEV)
+    b = System(s, "cube26", Hypers(), net, kT=1.0, dt=0.005, device=gh.DEV)
+    a.run(5, graph=True)
+    for _ in range(5):
+        b.step()
+    torch.cuda.synchronize()
+    assert torch.allclose(a.pos, b.pos, atol=1e-4)
+    a.run(205, graph=True)  # crosses two Verlet rebuilds
+    torch.cuda.synchronize()
+    pos = a.pos.cpu().numpy()
+    ref = nlist.sorted_pairs(nlist.reference_pairs(pos, a.L, a.r_verlet))
+    a.build_nlist()
+    assert np.array_equal(a.verlet_pairs().astype(np.int64), ref)
+    assert np.isfinite(a.conserved_quantity())
