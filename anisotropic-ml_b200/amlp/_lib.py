@@ -79,6 +79,7 @@ SIGNATURES = {
     "amlp_fd_scatter": [_P, _LL, _P, ctypes.POINTER(Nep), _P, _P, _P, _P],
     "amlp_forces_fd": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
     "amlp_forces_adjoint": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
+    "amlp_device_error": [ctypes.POINTER(ctypes.c_uint), _I],
     "amlp_nvt_workspace_bytes": [_I, _PSZ],
     "amlp_nvt_init": [_P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _I, _P, _P, _SZ, _P],
     "amlp_nvt_step_two": [_P, _P, _P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _P, _P],
@@ -115,6 +116,13 @@ def size_query(name: str, *args) -> int:
     out = ctypes.c_size_t(0)
     call(name, *args, ctypes.byref(out))
     return int(out.value)
+
+
+def device_error(clear: bool = True) -> int:
+    """Sticky error bits of bounded device-side waits (0 = none)."""
+    v = ctypes.c_uint(0)
+    call("amlp_device_error", ctypes.byref(v), int(clear))
+    return int(v.value)
 
 
 def exported_symbols() -> list[str]:

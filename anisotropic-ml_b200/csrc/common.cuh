@@ -14,7 +14,7 @@ amlp_status check_launch();
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
-inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+__host__ __device__ inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 // Carves a caller workspace into aligned slices.
 struct Carver {

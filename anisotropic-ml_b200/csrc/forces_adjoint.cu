@@ -1,0 +1,761 @@
+// Adjoint force path: exact forces and torques of the pair energy
+// E = en_min + (en_max - en_min) * net(g(cloud)) instead of the reference's
+// ten finite-difference evaluations (ForceEvaluator.py:86-112).
+//
+// One CTA works on tiles of 128 pairs with 256 threads; thread t handles pair
+// p = t % 128 and the half h = t / 128 of the harmonics (and the same TMEM
+// lane p in the tensor-core epilogues). Per tile:
+//   1  stage the rotated body points of the pairs in shared memory;
+//   2  descriptor forward (FP32): g = [sum_a f_n(a) | sum_m A_{n,lm}^2];
+//   3  net forward and backward on the tensor cores: every product is three
+//      bf16 x bf16 -> fp32 MMAs (hi*hi + hi*lo + lo*hi of the bf16 splits of
+//      activations and weights), accumulators in TMEM; gives dE/dg;
+//   4  descriptor backward (FP32), recomputing the per-point quantities instead
+//      of keeping them: dE/dA = 2 dE/dg_ang A, then per point
+//      dE/dr_a = sum_n dE/df_n f_n'(d) rhat + sum_lm dE/dY_lm grad Y_lm;
+//   5  F_pair = -sum_{a in i} dE/dp_a, T_i = -sum_{a in i} p_a x dE/dp_a,
+//      T_j = -sum_{a in j} (p_a - t) x dE/dp_a (dE/dp_a = dE/dr_a minus the mean,
+//      the centroid moving with every point), times (en_max - en_min), clipped
+//      to [-100, 100] and scattered like the reference (ForceEvaluator.py:119-142).
+// Nets: 1 to 3 hidden layers of width <= 64, D <= 64.
+#include "descriptor.cuh"
+#include "tcgen05.cuh"
+
+namespace amlp {
+
+__device__ unsigned int g_amlp_device_error = 0;
+
+namespace {
+
+constexpr int kAP = 128;          // pairs per tile (MMA M)
+constexpr int kAThreads = 256;
+constexpr int kMaxHidden = 3;
+constexpr int kWpad = 64;          // hidden widths padded to 64 in TMEM regions
+constexpr uint32_t kErrMbarTimeout = 1u;
+
+struct AdjNet {
+    int nh;                         // hidden layers
+    int act;
+    int kin[kMaxHidden + 1];        // padded input width of hidden layer k (multiple of 16)
+    int nout[kMaxHidden + 1];       // padded output width of hidden layer k (multiple of 16)
+    int dims[kMaxHidden + 2];       // true dims: D, h1, .., h_nh, 1
+    long long woff[kMaxHidden + 1];  // offset of W_k in the packed global weights (k = 0..nh)
+    int wsm_off[kMaxHidden];        // byte offset of W_k (hi) in the weight area; lo follows
+    int wsm_total;                  // bytes of the weight area
+    int bias_off[kMaxHidden + 1];   // float offsets of b_k in the fp32 parameter area; last = w_last
+    int par_total;
+};
+
+// Derivative of f_n with respect to the distance d, together with f_n.
+template <int NR>
+__device__ __forceinline__ void radial_basis_grad(float d, float inv_rc, float *f, float *df) {
+    float u = d * inv_rc;
+    float x = fmaf(2.0f * (u - 1.0f), (u - 1.0f), -1.0f);
+    float dx = 4.0f * (u - 1.0f) * inv_rc;                  // dx/dd
+    float s, c;
+    sincospif(u, &s, &c);
+    float fc = 0.5f * (1.0f + c);
+    float dfc = -0.5f * 3.14159265358979f * s * inv_rc;     // dfc/dd
+    float tm1 = 1.0f, t = x, dtm1 = 0.0f, dt = 1.0f;        // T_n and dT_n/dx
+    f[0] = fc;
+    df[0] = dfc;
+    if (NR > 1) {
+        f[1] = 0.5f * (1.0f + x) * fc;
+        df[1] = 0.5f * (dx * fc + (1.0f + x) * dfc);
+    }
+#pragma unroll
+    for (int n = 2; n < NR; ++n) {
+        float tn = fmaf(2.0f * x, t, -tm1);
+        float dtn = 2.0f * t + fmaf(2.0f * x, dt, -dtm1);
+        tm1 = t;
+        t = tn;
+        dtm1 = dt;
+        dt = dtn;
+        f[n] = 0.5f * (1.0f + tn) * fc;
+        df[n] = 0.5f * (dtn * dx * fc + (1.0f + tn) * dfc);
+    }
+}
+
+// Harmonics and their gradients as polynomials of (x, y, z) (before the
+// projection onto the sphere's tangent plane).
+template <int LMAX>
+__device__ __forceinline__ void sh_eval_grad(float x, float y, float z, float *Y, float (*G)[3]) {
+    float C[LMAX + 1], S[LMAX + 1];
+    C[0] = 1.0f;
+    S[0] = 0.0f;
+#pragma unroll
+    for (int m = 1; m <= LMAX; ++m) {
+        C[m] = fmaf(x, C[m - 1], -y * S[m - 1]);
+        S[m] = fmaf(x, S[m - 1], y * C[m - 1]);
+    }
+    float Q[LMAX + 2][LMAX + 2];  // Q[l][m] = d^m P_l / dz^m (0 for m > l)
+#pragma unroll
+    for (int l = 0; l <= LMAX + 1; ++l)
+#pragma unroll
+        for (int m = 0; m <= LMAX + 1; ++m) Q[l][m] = 0.0f;
+#pragma unroll
+    for (int m = 0; m <= LMAX; ++m) {
+#pragma unroll
+        for (int l = m; l <= LMAX; ++l) {
+            if (l == m) Q[l][m] = (float)dfact_odd(m);
+            else if (l == m + 1) Q[l][m] = (float)(2 * m + 1) * z * Q[l - 1][m];
+            else Q[l][m] = ((float)(2 * l - 1) * z * Q[l - 1][m] - (float)(l + m - 1) * Q[l - 2][m]) * (1.0f / (float)(l - m));
+        }
+    }
+#pragma unroll
+    for (int l = 1; l <= LMAX; ++l) {
+        const int base = l * l - 1;
+        Y[base] = Q[l][0];
+        G[base][0] = 0.0f;
+        G[base][1] = 0.0f;
+        G[base][2] = Q[l][1];
+#pragma unroll
+        for (int m = 1; m <= l; ++m) {
+            const float nm = c_shnorm[l][m];
+            const float q = nm * Q[l][m], q1 = nm * Q[l][m + 1], mq = (float)m * q;
+            Y[base + 2 * m - 1] = q * C[m];
+            Y[base + 2 * m] = q * S[m];
+            G[base + 2 * m - 1][0] = mq * C[m - 1];
+            G[base + 2 * m - 1][1] = -mq * S[m - 1];
+            G[base + 2 * m - 1][2] = q1 * C[m];
+            G[base + 2 * m][0] = mq * S[m - 1];
+            G[base + 2 * m][1] = mq * C[m - 1];
+            G[base + 2 * m][2] = q1 * S[m];
+        }
+    }
+}
+
+// Point a of cloud 1 (body i at the origin, body j moved by t).
+__device__ __forceinline__ float3 cloud1_point(const float *Ri, const float *Rj, float3 t, int h, int a) {
+    if (a < h) return make_float3(Ri[3 * a], Ri[3 * a + 1], Ri[3 * a + 2]);
+    int b = a - h;
+    return make_float3(__fadd_rn(Rj[3 * b], t.x), __fadd_rn(Rj[3 * b + 1], t.y), __fadd_rn(Rj[3 * b + 2], t.z));
+}
+
+template <class Cfg>
+struct Half {
+    static constexpr int KC = (Cfg::K + 1) / 2;  // harmonics per half
+};
+
+// sum_a f_n(a) Y_k(a) for this half's harmonics k0..k0+KC-1 (and the radial sums).
+template <class Cfg, int KC, int k0>
+__device__ __forceinline__ void accumulate_A(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
+                                             float inv_rc, float (*A)[KC], float *R) {
+#pragma unroll
+    for (int n = 0; n < Cfg::NA; ++n)
+#pragma unroll
+        for (int kk = 0; kk < KC; ++kk) A[n][kk] = 0.f;
+#pragma unroll
+    for (int n = 0; n < Cfg::NR; ++n) R[n] = 0.f;
+    const int nd = 2 * npts;
+    for (int a = 0; a < nd; ++a) {
+        float3 p = cloud1_point(Ri, Rj, t, npts, a);
+        float rx = p.x - c.x, ry = p.y - c.y, rz = p.z - c.z;
+        float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+        float inv_d = rsqrtf(d2);
+        float f[Cfg::NR];
+        radial_basis<Cfg::NR>(d2 * inv_d, inv_rc, f);
+#pragma unroll
+        for (int n = 0; n < Cfg::NR; ++n) R[n] += f[n];
+        float Y[Cfg::K];
+        sh_eval<Cfg::LMAX>(rx * inv_d, ry * inv_d, rz * inv_d, Y);
+#pragma unroll
+        for (int n = 0; n < Cfg::NA; ++n)
+#pragma unroll
+            for (int kk = 0; kk < KC; ++kk)
+                if (k0 + kk < Cfg::K) A[n][kk] = fmaf(f[n], Y[k0 + kk], A[n][kk]);
+    }
+}
+
+
+// Forward of one half of the harmonics: radial sums (half 0) and the partial
+// sums of squares of this half's harmonics, written to gp[0..47] (zeros elsewhere).
+template <class Cfg, int H>
+__device__ __forceinline__ void half_forward(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
+                                             float inv_rc, float *gp) {
+    constexpr int KC = Half<Cfg>::KC;
+    float A[Cfg::NA][KC], Rr[Cfg::NR];
+    accumulate_A<Cfg, KC, H * KC>(Ri, Rj, t, npts, c, inv_rc, A, Rr);
+    for (int k = 0; k < 48; ++k) gp[k] = 0.f;
+    if (H == 0) {
+#pragma unroll
+        for (int n = 0; n < Cfg::NR; ++n) gp[n] = Rr[n];
+    }
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk) {
+        if (H * KC + kk < Cfg::K) {
+            const int l = sh_l_of(H * KC + kk);
+#pragma unroll
+            for (int n = 0; n < Cfg::NA; ++n) gp[Cfg::NR + n * Cfg::LMAX + l - 1] += A[n][kk] * A[n][kk];
+        }
+    }
+}
+
+// Backward of one half: given dE/dg (dg), the partial sums over points of
+// dE/dr_a needed for the pair force and torques: sum_{a in i} G_a, sum_a G_a,
+// sum_{a in i} p_a x G_a, sum_{a in j} (p_a - t) x G_a -> out[12].
+template <class Cfg, int H>
+__device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
+                                              float inv_rc, const float *dg, float *out) {
+    constexpr int KC = Half<Cfg>::KC;
+    float A[Cfg::NA][KC], Rr[Cfg::NR];
+    accumulate_A<Cfg, KC, H * KC>(Ri, Rj, t, npts, c, inv_rc, A, Rr);
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk) {
+        if (H * KC + kk < Cfg::K) {
+            const int l = sh_l_of(H * KC + kk);
+#pragma unroll
+            for (int n = 0; n < Cfg::NA; ++n) A[n][kk] *= 2.0f * dg[Cfg::NR + n * Cfg::LMAX + l - 1];
+        } else {
+#pragma unroll
+            for (int n = 0; n < Cfg::NA; ++n) A[n][kk] = 0.f;
+        }
+    }
+    float grad_rad[Cfg::NR];
+#pragma unroll
+    for (int n = 0; n < Cfg::NR; ++n) grad_rad[n] = H == 0 ? dg[n] : 0.f;
+    float Si[3] = {0, 0, 0}, Sa[3] = {0, 0, 0}, Xi[3] = {0, 0, 0}, Xj[3] = {0, 0, 0};
+    const int nd = 2 * npts;
+    for (int a = 0; a < nd; ++a) {
+        float3 q = cloud1_point(Ri, Rj, t, npts, a);
+        float rx = q.x - c.x, ry = q.y - c.y, rz = q.z - c.z;
+        float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+        float inv_d = rsqrtf(d2);
+        float d = d2 * inv_d;
+        float ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
+        float f[Cfg::NR], df[Cfg::NR];
+        radial_basis_grad<Cfg::NR>(d, inv_rc, f, df);
+        float Y[Cfg::K], GY[Cfg::K][3];
+        sh_eval_grad<Cfg::LMAX>(ux, uy, uz, Y, GY);
+        float gr = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+        for (int n = 0; n < Cfg::NR; ++n) {
+            float s = grad_rad[n];
+            if (n < Cfg::NA) {
+#pragma unroll
+                for (int kk = 0; kk < KC; ++kk)
+                    if (H * KC + kk < Cfg::K) s = fmaf(A[n][kk], Y[H * KC + kk], s);
+            }
+            gr = fmaf(s, df[n], gr);
+        }
+#pragma unroll
+        for (int kk = 0; kk < KC; ++kk) {
+            if (H * KC + kk < Cfg::K) {
+                float s = 0.f;
+#pragma unroll
+                for (int n = 0; n < Cfg::NA; ++n) s = fmaf(A[n][kk], f[n], s);
+                gx = fmaf(s, GY[H * KC + kk][0], gx);
+                gy = fmaf(s, GY[H * KC + kk][1], gy);
+                gz = fmaf(s, GY[H * KC + kk][2], gz);
+            }
+        }
+        // dE/dr = gr rhat + (g - rhat (rhat . g)) / d
+        float dot = ux * gx + uy * gy + uz * gz;
+        float Gx = gr * ux + (gx - ux * dot) * inv_d;
+        float Gy = gr * uy + (gy - uy * dot) * inv_d;
+        float Gz = gr * uz + (gz - uz * dot) * inv_d;
+        Sa[0] += Gx;
+        Sa[1] += Gy;
+        Sa[2] += Gz;
+        if (a < npts) {
+            Si[0] += Gx;
+            Si[1] += Gy;
+            Si[2] += Gz;
+            Xi[0] += q.y * Gz - q.z * Gy;
+            Xi[1] += q.z * Gx - q.x * Gz;
+            Xi[2] += q.x * Gy - q.y * Gx;
+        } else {
+            float bx = q.x - t.x, by = q.y - t.y, bz = q.z - t.z;
+            Xj[0] += by * Gz - bz * Gy;
+            Xj[1] += bz * Gx - bx * Gz;
+            Xj[2] += bx * Gy - by * Gx;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        out[k] = Si[k];
+        out[3 + k] = Sa[k];
+        out[6 + k] = Xi[k];
+        out[9 + k] = Xj[k];
+    }
+}
+
+struct AdjShared {
+    float *R;          // rotated body points, kAP x rs (aliases the MLP operand area)
+    char *ops;         // MLP operand area (bf16 hi/lo tiles)
+    char *wts;         // weights (bf16 hi/lo), resident
+    float *par;        // biases + last-layer weights (fp32)
+    float *g0, *g1;    // per-half descriptor partials, kAP x 48 each; g0 later holds dE/dg
+    float *t;          // translations, kAP x 3
+    float *cen;        // centroids, kAP x 3
+    float *part;       // per-half gradient partial sums, 2 x kAP x 12
+    float *eps;        // per-half energy partials, 2 x kAP
+    float *fd;         // per-pair F, T_i, T_j, kAP x 9
+    int *ij;           // pair indices, kAP x 2
+    float *pts;        // body points
+};
+
+// Activation tile of layer k in the operand area (hi at its base, lo after it).
+// Only two are live at a time (the one an MMA reads and the one its epilogue
+// writes), so the layers alternate between two buffers.
+__device__ __forceinline__ char *op_tile(char *ops, int k) { return ops + (k & 1) * (2 * kAP * kWpad * 2); }
+
+// A (128 x K) times B, three split terms, into TMEM columns at d_tmem.
+__device__ __forceinline__ void mma3(uint32_t d_tmem, const char *a_hi, int K, const char *b_hi, size_t b_lo_off,
+                                     int N, bool b_mn, int b_kstride /* bytes per K-step of 16 */, uint32_t b_lbo,
+                                     uint32_t b_sbo) {
+    const uint32_t idesc = tc::idesc_bf16(N, b_mn ? 1 : 0);
+    const uint32_t a0 = tc::smem_u32(a_hi), a1 = a0 + (uint32_t)(kAP * K * 2);
+    const uint32_t b0 = tc::smem_u32(b_hi), b1 = b0 + (uint32_t)b_lo_off;
+    const uint32_t a_sbo = (uint32_t)K * 16;
+    for (int ks = 0; ks < K / 16; ++ks) {
+        const uint32_t ao = ks * 256, bo = ks * b_kstride;
+        tc::mma_bf16(d_tmem, tc::smem_desc(a0 + ao, 128, a_sbo), tc::smem_desc(b0 + bo, b_lbo, b_sbo), idesc,
+                     ks > 0 ? 1u : 0u);
+        tc::mma_bf16(d_tmem, tc::smem_desc(a0 + ao, 128, a_sbo), tc::smem_desc(b1 + bo, b_lbo, b_sbo), idesc, 1u);
+        tc::mma_bf16(d_tmem, tc::smem_desc(a1 + ao, 128, a_sbo), tc::smem_desc(b0 + bo, b_lbo, b_sbo), idesc, 1u);
+    }
+}
+
+// Write 8 consecutive values of row p, columns c0..c0+7 into a K-major bf16
+// hi/lo tile of width K.
+__device__ __forceinline__ void store_split8(char *tile_hi, int K, int p, int c0, const float *v) {
+    __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) tc::split_bf16(v[k], hi[k], lo[k]);
+    uint32_t off = tc::kmajor_offset(p, c0, K);
+    *reinterpret_cast<uint4 *>(tile_hi + off) = *reinterpret_cast<uint4 *>(hi);
+    *reinterpret_cast<uint4 *>(tile_hi + kAP * K * 2 + off) = *reinterpret_cast<uint4 *>(lo);
+}
+
+template <class Cfg>
+__global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *pos, const float *quat, float L,
+                                                                const int *pairs, const long long *d_np, long long cap,
+                                                                const float *pts, int npts, float inv_rc, float en_min,
+                                                                float en_range, AdjNet net, const float *w, float *F,
+                                                                float *T, double *pe) {
+    constexpr int KC = Half<Cfg>::KC;
+    constexpr int DP = 48;  // padded descriptor width in fp32 staging
+    extern __shared__ __align__(128) char smem_raw[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    __shared__ double pe_s[kAThreads / 32];
+
+    const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
+    const int rs = 6 * npts + 1 - ((6 * npts) & 1);
+    const int Kg = net.kin[0];
+
+    // ---- shared memory carve-up (offsets are multiples of 128 bytes)
+    AdjShared S;
+    size_t off = 0;
+    const size_t r_bytes = (size_t)kAP * rs * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
+    S.ops = smem_raw;
+    S.R = reinterpret_cast<float *>(smem_raw);
+    off = align_up(r_bytes > ops_bytes ? r_bytes : ops_bytes, 128);
+    S.wts = smem_raw + off;
+    off += align_up(net.wsm_total, 128);
+    S.par = reinterpret_cast<float *>(smem_raw + off);
+    off += align_up((size_t)net.par_total * 4, 128);
+    S.g0 = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * DP * 4;
+    S.g1 = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * DP * 4;
+    S.t = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * 3 * 4;
+    S.cen = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * 3 * 4;
+    S.part = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)2 * kAP * 12 * 4;
+    S.eps = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)2 * kAP * 4;
+    S.fd = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * 9 * 4;
+    S.ij = reinterpret_cast<int *>(smem_raw + off);
+    off += (size_t)kAP * 2 * 4;
+    S.pts = reinterpret_cast<float *>(smem_raw + off);
+
+    // ---- one-time set-up: weights (bf16 hi/lo, K-major), biases, TMEM, mbarrier
+    for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = pts[k];
+    for (int L2 = 0; L2 < net.nh; ++L2) {
+        const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
+        const float *W = w + net.woff[L2];
+        char *hi = S.wts + net.wsm_off[L2];
+        char *lo = hi + Np * Kp * 2;
+        for (int idx = tid; idx < Np * Kp; idx += kAThreads) {
+            int n = idx / Kp, k = idx - n * Kp;
+            float v = (n < N && k < K) ? W[(size_t)n * K + k] : 0.f;
+            __nv_bfloat16 a, b;
+            tc::split_bf16(v, a, b);
+            uint32_t o = tc::kmajor_offset(n, k, Kp);
+            *reinterpret_cast<__nv_bfloat16 *>(hi + o) = a;
+            *reinterpret_cast<__nv_bfloat16 *>(lo + o) = b;
+        }
+        const float *b = W + (size_t)N * K;
+        for (int n = tid; n < Np; n += kAThreads) S.par[net.bias_off[L2] + n] = n < N ? b[n] : 0.f;
+    }
+    {
+        const int K = net.dims[net.nh];
+        const float *Wl = w + net.woff[net.nh];
+        for (int k = tid; k < kWpad; k += kAThreads) S.par[net.bias_off[net.nh] + k] = k < K ? Wl[k] : 0.f;
+        if (tid == 0) S.par[net.bias_off[net.nh] + kWpad] = Wl[K];  // last bias
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, 256);
+    if (tid == 0) {
+        tc::mbar_init(&mbar, 1);
+        abort_flag = 0;
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t bar = tc::smem_u32(&mbar);
+    uint32_t phase = 0;
+    // TMEM column regions: Z_k (hidden layer k) at 64k, backward product at 192, dE/dg at 192 too
+    auto zcol = [&](int k) { return (uint32_t)(k * kWpad); };
+    const uint32_t bcol = (uint32_t)(3 * kWpad);
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+
+    auto wait_mma = [&]() -> bool {
+        if (!tc::mbar_wait(bar, phase)) {
+            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
+            abort_flag = 1;
+        }
+        phase ^= 1u;
+        tc::fence_after();
+        return true;
+    };
+
+    const long long P = min(*d_np, cap);
+    const long long ntiles = (P + kAP - 1) / kAP;
+    double pe_acc = 0.0;
+    const int nd = 2 * npts;
+
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long p0 = tile * kAP;
+        const int valid = (int)min((long long)kAP, P - p0);
+        // ---- 1. rotated body points, translations, pair indices
+        for (int idx = tid; idx < kAP * nd; idx += kAThreads) {
+            int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
+            long long pr = min(p0 + q, P - 1);
+            float4 qq = load_quat(quat, pairs[2 * pr + body]);
+            float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
+            float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
+            dst[0] = r.x;
+            dst[1] = r.y;
+            dst[2] = r.z;
+        }
+        if (tid < kAP) {
+            long long pr = min(p0 + tid, P - 1);
+            int i = pairs[2 * pr], j = pairs[2 * pr + 1];
+            float dd;
+            float3 tt = min_image(pos, i, j, L, &dd);
+            S.t[3 * tid] = tt.x;
+            S.t[3 * tid + 1] = tt.y;
+            S.t[3 * tid + 2] = tt.z;
+            S.ij[2 * tid] = i;
+            S.ij[2 * tid + 1] = j;
+        }
+        __syncthreads();
+        // ---- 2. descriptor forward
+        const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
+        const float3 t = make_float3(S.t[3 * p], S.t[3 * p + 1], S.t[3 * p + 2]);
+        float3 c = make_float3(0.f, 0.f, 0.f);
+        for (int a = 0; a < nd; ++a) {
+            float3 q = cloud1_point(Ri, Rj, t, npts, a);
+            c.x += q.x;
+            c.y += q.y;
+            c.z += q.z;
+        }
+        {
+            float inv = 1.0f / (float)nd;
+            c.x *= inv;
+            c.y *= inv;
+            c.z *= inv;
+        }
+        if (h == 0) {
+            S.cen[3 * p] = c.x;
+            S.cen[3 * p + 1] = c.y;
+            S.cen[3 * p + 2] = c.z;
+        }
+        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP);
+        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * DP);
+        __syncthreads();
+        // ---- 3. net forward + backward on the tensor cores
+        {
+            char *tG = op_tile(S.ops, 0);
+            for (int c0 = h * (Kg / 2); c0 < (h + 1) * (Kg / 2); c0 += 8) {
+                float v[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    int d = c0 + k;
+                    v[k] = d < Cfg::D ? S.g0[p * DP + d] + S.g1[p * DP + d] : 0.f;
+                }
+                store_split8(tG, Kg, p, c0, v);
+            }
+        }
+        tc::fence_async_smem();
+        __syncthreads();
+        // forward layers
+        for (int L2 = 0; L2 < net.nh; ++L2) {
+            const int Kp = net.kin[L2], Np = net.nout[L2];
+            if (tid == 0 && !abort_flag) {
+                tc::fence_after();
+                const char *wb = S.wts + net.wsm_off[L2];
+                mma3(tmem + zcol(L2), op_tile(S.ops, L2), Kp, wb, (size_t)Np * Kp * 2, Np, false, 256, 128,
+                     (uint32_t)Kp * 16);
+                tc::commit(bar);
+            }
+            wait_mma();
+            // epilogue: a = act(z + b) into the next operand tile; the last hidden
+            // layer also forms e and delta = w_last * act'(z)
+            const bool last = L2 == net.nh - 1;
+            const float *bias = S.par + net.bias_off[L2];
+            const float *wl = S.par + net.bias_off[net.nh];
+            char *dst = op_tile(S.ops, L2 + 1);
+            float esum = 0.f;
+            for (int c0 = h * (Np / 2); c0 < (h + 1) * (Np / 2); c0 += 8) {
+                float z[8], v[8];
+                tc::tmem_ld8(tmem + lane_base + zcol(L2) + c0, z);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    float zz = z[k] + bias[c0 + k];
+                    if (last) {
+                        esum = fmaf(wl[c0 + k], act_f(net.act, zz), esum);
+                        v[k] = wl[c0 + k] * act_df(net.act, zz);
+                    } else {
+                        v[k] = act_f(net.act, zz);
+                    }
+                }
+                store_split8(dst, Np, p, c0, v);
+            }
+            if (last) S.eps[h * kAP + p] = esum;
+            tc::fence_before();
+            tc::fence_async_smem();
+            __syncthreads();
+        }
+        // backward layers: delta_{k-1} = (delta_k W_k) * act'(z_{k-1}); dE/dg = delta_1 W_1
+        for (int L2 = net.nh - 1; L2 >= 0; --L2) {
+            const int Kp = net.kin[L2], Np = net.nout[L2];
+            if (tid == 0 && !abort_flag) {
+                tc::fence_after();
+                const char *wb = S.wts + net.wsm_off[L2];
+                // B = W_k read as MN-major (the transpose): N' = Kp, K' = Np
+                mma3(tmem + bcol, op_tile(S.ops, L2 + 1), Np, wb, (size_t)Np * Kp * 2, Kp, true,
+                     2 * Kp * 16, (uint32_t)Kp * 16, 128);
+                tc::commit(bar);
+            }
+            wait_mma();
+            if (L2 > 0) {
+                const float *bias = S.par + net.bias_off[L2 - 1];
+                char *dst = op_tile(S.ops, L2);
+                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
+                    float dz[8], z[8], v[8];
+                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
+                    tc::tmem_ld8(tmem + lane_base + zcol(L2 - 1) + c0, z);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_df(net.act, z[k] + bias[c0 + k]);
+                    store_split8(dst, Kp, p, c0, v);
+                }
+                tc::fence_async_smem();
+            } else {
+                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
+                    float dg[8];
+                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dg);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) S.g0[p * DP + c0 + k] = dg[k];
+                }
+            }
+            tc::fence_before();
+            __syncthreads();
+        }
+        if (h == 0 && p < valid)
+            pe_acc += (double)en_min + (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
+        // ---- 4. recompute the rotated points (their area held the MLP tiles)
+        for (int idx = tid; idx < kAP * nd; idx += kAThreads) {
+            int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
+            long long pr = min(p0 + q, P - 1);
+            float4 qq = load_quat(quat, pairs[2 * pr + body]);
+            float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
+            float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
+            dst[0] = r.x;
+            dst[1] = r.y;
+            dst[2] = r.z;
+        }
+        __syncthreads();
+        // ---- descriptor backward
+        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + p * 12);
+        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * 12);
+        __syncthreads();
+        // ---- 5. per-pair forces and torques
+        if (tid < kAP) {
+            const float *a0 = S.part + p * 12, *a1 = S.part + (kAP + p) * 12;
+            float Si[3], Sa[3], Xi[3], Xj[3], Pi[3] = {0, 0, 0}, Qj[3] = {0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                Si[k] = a0[k] + a1[k];
+                Sa[k] = a0[3 + k] + a1[3 + k];
+                Xi[k] = a0[6 + k] + a1[6 + k];
+                Xj[k] = a0[9 + k] + a1[9 + k];
+            }
+            for (int a = 0; a < npts; ++a) {
+                Pi[0] += Ri[3 * a];
+                Pi[1] += Ri[3 * a + 1];
+                Pi[2] += Ri[3 * a + 2];
+                Qj[0] += Rj[3 * a];
+                Qj[1] += Rj[3 * a + 1];
+                Qj[2] += Rj[3 * a + 2];
+            }
+            const float inv_nd = 1.0f / (float)nd;
+            float Gm[3] = {Sa[0] * inv_nd, Sa[1] * inv_nd, Sa[2] * inv_nd};  // mean gradient
+            float Fp[3], Ti[3], Tj[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Fp[k] = -(Si[k] - (float)npts * Gm[k]);
+            Ti[0] = -(Xi[0] - (Pi[1] * Gm[2] - Pi[2] * Gm[1]));
+            Ti[1] = -(Xi[1] - (Pi[2] * Gm[0] - Pi[0] * Gm[2]));
+            Ti[2] = -(Xi[2] - (Pi[0] * Gm[1] - Pi[1] * Gm[0]));
+            Tj[0] = -(Xj[0] - (Qj[1] * Gm[2] - Qj[2] * Gm[1]));
+            Tj[1] = -(Xj[1] - (Qj[2] * Gm[0] - Qj[0] * Gm[2]));
+            Tj[2] = -(Xj[2] - (Qj[0] * Gm[1] - Qj[1] * Gm[0]));
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                S.fd[9 * p + k] = clip100(Fp[k] * en_range);
+                S.fd[9 * p + 3 + k] = clip100(Ti[k] * en_range);
+                S.fd[9 * p + 6 + k] = clip100(Tj[k] * en_range);
+            }
+        }
+        __syncthreads();
+        // ---- scatter: warps 0..3, lane = pair within a 32-pair group
+        if (warp < 4) {
+            const int q = warp * 32 + lane;
+            const bool ok = q < valid;
+            const int i = S.ij[2 * q], j = S.ij[2 * q + 1];
+            float v[6];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                v[k] = ok ? S.fd[9 * q + k] : 0.f;
+                v[3 + k] = ok ? S.fd[9 * q + 3 + k] : 0.f;
+            }
+            if (ok) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    atomicAdd(F + 3 * j + k, -v[k]);
+                    atomicAdd(T + 3 * j + k, S.fd[9 * q + 6 + k]);
+                }
+            }
+            int key = ok ? i : -1 - q;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int ko = __shfl_up_sync(0xffffffffu, key, o);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    float y = __shfl_up_sync(0xffffffffu, v[k], o);
+                    if (lane >= o && ko == key) v[k] += y;
+                }
+            }
+            int kn = __shfl_down_sync(0xffffffffu, key, 1);
+            if (ok && (lane == 31 || kn != key)) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    atomicAdd(F + 3 * i + k, v[k]);
+                    atomicAdd(T + 3 * i + k, v[3 + k]);
+                }
+            }
+        }
+        __syncthreads();
+        if (abort_flag) break;
+    }
+    // ---- pair-energy sum, TMEM release
+    if (pe) {
+        double v = pe_acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) pe_s[warp] = v;
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (pe && tid == 0) {
+        double s = 0.0;
+        for (int k = 0; k < kAThreads / 32; ++k) s += pe_s[k];
+        if (s != 0.0) atomicAdd(pe, s);
+    }
+    if (abort_flag && tid == 0) tc::mbar_wait(bar, phase);  // let an MMA still in flight finish
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after();
+        tc::tmem_dealloc(tmem, 256);
+    }
+}
+
+}  // namespace
+
+amlp_status check_nep(const amlp_nep *n);
+int hyper_kind(const amlp_nep *n);
+int nep_D(const amlp_nep *n);
+amlp_status check_mlp(const amlp_mlp *m, int D);
+
+}  // namespace amlp
+
+using namespace amlp;
+
+extern "C" amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                           const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                           const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe,
+                                           void *stream) {
+    amlp_status st = check_nep(nep);
+    if (st) return st;
+    const int D = nep_D(nep);
+    if ((st = check_mlp(mlp, D))) return st;
+    if (!d_pos || !d_quat || !d_npairs || !d_F || !d_T || cap < 0 || (cap > 0 && !d_pairs)) return AMLP_ERR_INVALID_ARG;
+    if (cap == 0) return AMLP_OK;
+    if (hyper_kind(nep) != 1 || D > 48) return AMLP_ERR_UNSUPPORTED;
+    const int nh = mlp->n_layers - 1;
+    if (nh < 1 || nh > kMaxHidden) return AMLP_ERR_UNSUPPORTED;
+    AdjNet net{};
+    net.nh = nh;
+    net.act = mlp->act;
+    long long off = 0;
+    int wsm = 0, par = 0;
+    for (int k = 0; k <= mlp->n_layers; ++k) net.dims[k] = mlp->dims[k];
+    for (int k = 0; k <= nh; ++k) {
+        net.woff[k] = off;
+        off += (long long)mlp->dims[k + 1] * mlp->dims[k] + mlp->dims[k + 1];
+    }
+    for (int k = 0; k < nh; ++k) {
+        if (mlp->dims[k + 1] > kWpad) return AMLP_ERR_UNSUPPORTED;
+        net.kin[k] = k == 0 ? 48 : net.nout[k - 1];
+        net.nout[k] = (mlp->dims[k + 1] + 15) / 16 * 16;
+        net.wsm_off[k] = wsm;
+        wsm += 2 * net.nout[k] * net.kin[k] * 2;
+        net.bias_off[k] = par;
+        par += net.nout[k];
+    }
+    net.bias_off[nh] = par;
+    par += kWpad + 4;
+    net.wsm_total = wsm;
+    net.par_total = par;
+    const int npts = nep->npts;
+    const int rs = 6 * npts + 1 - ((6 * npts) & 1);
+    size_t r_bytes = (size_t)kAP * rs * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
+    size_t smem = align_up(std::max(r_bytes, ops_bytes), 128) + align_up(wsm, 128) + align_up((size_t)par * 4, 128) +
+                  (size_t)kAP * 48 * 4 * 2 + (size_t)kAP * 3 * 4 * 2 + (size_t)2 * kAP * 12 * 4 + (size_t)2 * kAP * 4 +
+                  (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 + 128;
+    if (smem > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
+    using Cfg = NepCfg<10, 8, 4, 12>;
+    AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_forces_adjoint<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_forces_adjoint<Cfg><<<kNumSM, kAThreads, smem, as_stream(stream)>>>(
+        d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, 1.0f / nep->nep_cutoff, nep->en_min,
+        nep->en_max - nep->en_min, net, mlp->d_w, d_F, d_T, d_pe);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_device_error(unsigned int *flags, int clear) {
+    if (!flags) return AMLP_ERR_INVALID_ARG;
+    AMLP_CHECK_CUDA(cudaMemcpyFromSymbol(flags, g_amlp_device_error, sizeof(unsigned int)));
+    if (clear) {
+        unsigned int z = 0;
+        AMLP_CHECK_CUDA(cudaMemcpyToSymbol(g_amlp_device_error, &z, sizeof(unsigned int)));
+    }
+    return AMLP_OK;
+}

@@ -7,7 +7,10 @@ quaternions, seed 1, NEP hypers (10, 8, 4), FFNN 47 -> 64 -> 64 -> 1 tanh with
 seeded Xavier weights, dt 0.005, kT 1.0 (synthetic; no dataset involved).
 
 Arms:
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--method fd|adjoint]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--method both|fd|adjoint]
+      "value" is the tuned method (exact adjoint forces, net on the tensor
+      cores); with "both" the plain FP32 finite-difference drop-in is measured
+      in the same run under "plain"
   python bench.py --impl reference ...   CPU restatement of the reference's
       step (the oracle, bit-identical to the reference's own classes) on the
       host cores, timed on a bounded sample of the same workload.
@@ -100,38 +103,58 @@ def measured_peaks() -> dict:
 
 
 # ----------------------------------------------------------------------------- reference arm / CPU baseline
-def cpu_step_sample(state, budget_s: float = 15.0, pairs_sample: int = 1500):
-    """Seconds per full step of the CPU oracle on this workload, estimated from a
-    bounded sample: the force pass on `pairs_sample` filtered pairs scaled to all
-    pairs, plus the integrator on all bodies and 1/100 of a cKDTree rebuild."""
-    import numpy as np
-    import torch
-    from amlp.engine import EnergyNet
-    from oracle import nep, nlist
-    from oracle.shapes import SHAPES
-    torch.set_num_threads(os.cpu_count() or 1)
-    shape = SHAPES["cube26"]
-    net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device="cpu")
-    t0 = time.perf_counter()
-    vp = nlist.reference_pairs(state.pos, state.L, shape["cutoff"] + 2.0)
-    t_nl = time.perf_counter() - t0
-    keep, pairs, _ = nep.min_image_filter(state.pos, vp, state.L, shape["cutoff"])
-    P = len(pairs)
-    rng = np.random.default_rng(0)
-    sel = np.sort(rng.choice(P, size=min(pairs_sample, P), replace=False))
-    t0 = time.perf_counter()
-    o = nep.pair_forces(state.pos, state.orient, pairs[sel], state.L, shape, (10, 8, 4), net.layers, ACT)
-    t_f = (time.perf_counter() - t0) * P / len(sel)
-    st = nep.NVTState(state.pos, state.vel, state.orient, state.angmom, state.mass, state.moi, state.L, KT, DT)
-    t0 = time.perf_counter()
-    st.step_two(o["forces"], o["torques"])
-    st.step_one()
-    t_i = time.perf_counter() - t0
-    step = t_f + t_i + t_nl / 100.0
-    sample = (f"force pass on {len(sel)} of {P} filtered pairs (scaled by {P / len(sel):.0f}x), integrator on "
-              f"all {state.N} bodies, cKDTree rebuild/100; oracle FP32 path (numpy + torch CPU, "
-              f"{torch.get_num_threads()} threads)")
-    return step, sample, P
+class CpuReferenceStep:
+    """One step of the reference's algorithm on the host cores, through the
+    oracle (bit-identical to the reference's own classes run on the CPU): FP32
+    descriptors of the 10 finite-difference clouds, torch-CPU net, differences,
+    scatter, both NVT halves, and 1/100 of a cKDTree Verlet rebuild. The force
+    pass runs on a random sample of the filtered pairs and is scaled to all."""
+
+    def __init__(self, state, pairs_sample: int = 256):
+        import numpy as np
+        import torch
+        from amlp.engine import EnergyNet
+        from oracle import nep, nlist
+        from oracle.shapes import SHAPES
+        torch.set_num_threads(os.cpu_count() or 1)
+        self.np, self.nep = np, nep
+        self.state = state
+        self.shape = SHAPES["cube26"]
+        self.net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device="cpu")
+        t0 = time.perf_counter()
+        vp = nlist.reference_pairs(state.pos, state.L, self.shape["cutoff"] + 2.0)
+        self.t_nlist = time.perf_counter() - t0
+        _, self.pairs, _ = nep.min_image_filter(state.pos, vp, state.L, self.shape["cutoff"])
+        self.P = len(self.pairs)
+        self.sample = min(pairs_sample, self.P)
+        self.rng = np.random.default_rng(0)
+        self.st = nep.NVTState(state.pos, state.vel, state.orient, state.angmom, state.mass, state.moi, state.L,
+                               KT, DT)
+        self.threads = torch.get_num_threads()
+
+    def step_seconds(self) -> float:
+        np, nep = self.np, self.nep
+        sel = np.sort(self.rng.choice(self.P, size=self.sample, replace=False))
+        t0 = time.perf_counter()
+        o = nep.pair_forces(self.st.pos, self.st.orient, self.pairs[sel], self.state.L, self.shape, (10, 8, 4),
+                            self.net.layers, ACT)
+        t_f = (time.perf_counter() - t0) * self.P / self.sample
+        t0 = time.perf_counter()
+        self.st.step_two(o["forces"], o["torques"])
+        self.st.step_one()
+        t_i = time.perf_counter() - t0
+        return t_f + t_i + self.t_nlist / 100.0
+
+    def describe(self) -> str:
+        return (f"per step: force pass on {self.sample} of {self.P} filtered pairs scaled by "
+                f"{self.P / self.sample:.0f}x, both NVT halves on all {self.state.N} bodies, 1/100 of a cKDTree "
+                f"rebuild; oracle FP32 path (numpy + torch CPU, {self.threads} threads)")
+
+
+def cpu_step_sample(state, steps: int = 3):
+    ref = CpuReferenceStep(state)
+    t = statistics.mean(ref.step_seconds() for _ in range(steps))
+    return t, ref.describe(), ref.P
 
 
 def run_reference(args, rank: int, world: int) -> None:
@@ -139,44 +162,35 @@ def run_reference(args, rank: int, world: int) -> None:
         return
     from amlp.configs import make_state
     state = make_state(N_BODIES, "cube26", PHI, kT=KT, seed=SEED)
-    times = []
-    sample = ""
-    for _ in range(args.warmup + args.steps):
-        t, sample, P = cpu_step_sample(state)
-        times.append(t)
-    per_step = statistics.mean(times[args.warmup:])
+    ref = CpuReferenceStep(state)
+    for _ in range(args.warmup):
+        ref.step_seconds()
+    times = [ref.step_seconds() for _ in range(args.steps)]
+    per_step = statistics.mean(times)
     value = N_BODIES / per_step
     cores = os.cpu_count() or 1
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "bodies": N_BODIES, "filtered_pairs": P, "parallelism": "replicas"},
+            "config": {"workload": WORKLOAD, "bodies": N_BODIES, "filtered_pairs": ref.P, "parallelism": "replicas",
+                       "method": "fd (the reference's finite differences)"},
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-                             "sample": sample},
+                             "sample": ref.describe()},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
 # ----------------------------------------------------------------------------- GPU arm
-def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
-    import numpy as np
+def _measure(system, method: str, steps: int, warmup: int, dist, dev):
+    """Device time of `steps` full steps (L2 flushed between steps, outside the
+    events) and of the force kernel inside them. Returns a dict."""
+    import ctypes
     import torch
     from amlp import _lib
-    from amlp.configs import make_state
-    from amlp.engine import EnergyNet, Hypers, System
-
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    state = make_state(N_BODIES, "cube26", PHI, kT=KT, seed=SEED)
-    net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device=dev)
-    system = System(state, "cube26", Hypers(), net, kT=KT, dt=DT, device=dev)
-    method = args.method
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    launches = [0]
+    entry = "amlp_forces_" + ("fd" if method == "fd" else "adjoint")
 
     def one_step(ev_force=None):
         if system.timestep % system.nlist_every == 0 and system.timestep > 0:
@@ -188,11 +202,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         system.filter_pairs()
         if ev_force is not None:
             ev_force[0].record(stream)
-        import ctypes
-        _lib.call("amlp_forces_" + ("fd" if method == "fd" else "adjoint"), system.pos.data_ptr(),
-                  system.quat.data_ptr(), system.L, system.fpairs.data_ptr(), system.nf.data_ptr(), system.cap,
-                  ctypes.byref(system.nep), ctypes.byref(system.net.struct), system.F.data_ptr(),
-                  system.T.data_ptr(), system._pe_ptr(), stream.cuda_stream)
+        _lib.call(entry, system.pos.data_ptr(), system.quat.data_ptr(), system.L, system.fpairs.data_ptr(),
+                  system.nf.data_ptr(), system.cap, ctypes.byref(system.nep), ctypes.byref(system.net.struct),
+                  system.F.data_ptr(), system.T.data_ptr(), system._pe_ptr(), stream.cuda_stream)
         if ev_force is not None:
             ev_force[1].record(stream)
         system.integrate_step_two()
@@ -200,20 +212,17 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         system.timestep += 1
         launches[0] += LAUNCHES["amlp_pair_filter"] + 1 + LAUNCHES["amlp_nvt_step_two"] + LAUNCHES["amlp_nvt_step_one"]
 
-    launches = [0]
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         one_step()
     torch.cuda.synchronize()
-    P = int(system.nf.item())
-    NV = int(system.nv.item())
+    P, NV = int(system.nf.item()), int(system.nv.item())
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     launches[0] = 0
-    clocks = ClockSampler(local_rank)
     step_ms, force_ms = [], []
-    for _ in range(args.steps):
-        flush.zero_()  # L2 flush between timed steps, outside the events
+    for _ in range(steps):
+        flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -222,67 +231,114 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         force_ms.append(f0.elapsed_time(f1))
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    total_ms = sum(step_ms)
+    total = sum(step_ms)
     if dist:
-        t = torch.tensor([total_ms], device=dev)
+        t = torch.tensor([total], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        total_ms = float(t.item())
-    value = world * N_BODIES * args.steps / (total_ms / 1e3)
+        total = float(t.item())
+    assert _lib.device_error() == 0, "a bounded device wait gave up"
+    return {"total_ms": total, "force_ms": statistics.mean(force_ms), "force_share": sum(force_ms) / sum(step_ms),
+            "P": P, "NV": NV, "launches": launches[0]}
 
-    # end to end through the public API with host buffers: every step copies the
-    # state in from pinned host memory, runs the step and reads the state back
-    host = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
-            (("pos", system.pos.cpu().numpy()), ("quat", system.quat.cpu().numpy()),
-             ("vel", system.vel.cpu().numpy()), ("angmom", system.angmom.cpu().numpy()))}
-    dev_t = {"pos": system.pos, "quat": system.quat, "vel": system.vel, "angmom": system.angmom}
+
+def _e2e(system, method, steps, dist, dev):
+    """Same metric through the public API with host buffers: every step copies the
+    state in from pinned host memory, runs System.step and reads the state back."""
+    import numpy as np
+    import torch
+    stream = torch.cuda.current_stream()
+    host = {k: torch.from_numpy(np.ascontiguousarray(getattr(system, k).cpu().numpy())).pin_memory()
+            for k in ("pos", "quat", "vel", "angmom")}
     nbytes = sum(t.numel() * t.element_size() for t in host.values())
-    e2e_steps = max(3, min(args.steps, 20))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(e2e_steps):
+    for _ in range(steps):
         for k in host:
-            dev_t[k].copy_(host[k], non_blocking=True)
+            getattr(system, k).copy_(host[k], non_blocking=True)
         system.step(method)
         for k in host:
-            host[k].copy_(dev_t[k], non_blocking=True)
+            host[k].copy_(getattr(system, k), non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    ms = e0.elapsed_time(e1)
     if dist:
-        t = torch.tensor([e2e_ms], device=dev)
+        t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * N_BODIES * e2e_steps / (e2e_ms / 1e3)
+        ms = float(t.item())
+    return ms, nbytes
 
+
+def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    from amlp.configs import make_state
+    from amlp.engine import EnergyNet, Hypers, System
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    state = make_state(N_BODIES, "cube26", PHI, kT=KT, seed=SEED)
+    net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device=dev)
+    methods = ["adjoint", "fd"] if args.method == "both" else [args.method]
     peaks = measured_peaks()
-    fl_pair = algorithmic_flops_per_pair(method)
-    f_avg = statistics.mean(force_ms) / 1e3
-    achieved_tf = fl_pair * P / f_avg / 1e12
     clk_mhz = peaks["sm_max_mhz"] or 1965.0
     fp32_peak = 148 * 128 * 2 * clk_mhz * 1e6 / 1e12
-    line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+    results = {}
+    clocks = ClockSampler(local_rank)
+    for m in methods:
+        system = System(state, "cube26", Hypers(), net, kT=KT, dt=DT, device=dev)
+        r = _measure(system, m, args.steps, args.warmup, dist, dev)
+        e2e_steps = max(3, min(args.steps, 20))
+        r["e2e_ms"], r["e2e_bytes"] = _e2e(system, m, e2e_steps, dist, dev)
+        r["e2e_steps"] = e2e_steps
+        results[m] = r
+        del system
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+
+    def summary(m):
+        r = results[m]
+        fl_pair = algorithmic_flops_per_pair(m)
+        achieved = fl_pair * r["P"] / (r["force_ms"] / 1e3) / 1e12
+        return {"value": world * N_BODIES * args.steps / (r["total_ms"] / 1e3), "ms_per_step": r["total_ms"] / args.steps,
+                "roofline": {"bound": "fp32", "kernel": "k_forces_" + m, "achieved": achieved, "peak": fp32_peak,
+                             "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                             "flops_per_pair": fl_pair, "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
+                             "force_share_of_step": r["force_share"],
+                             "peak_source": f"nominal FP32 SIMT 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz (no measured "
+                                            f"FP32 peak; HBM {peaks['hbm_gbs']} GB/s {peaks['source']})"},
+                "e2e": {"value": world * N_BODIES * r["e2e_steps"] / (r["e2e_ms"] / 1e3), "unit": "particle-steps/s",
+                        "h2d_bytes_per_step": r["e2e_bytes"], "d2h_bytes_per_step": r["e2e_bytes"],
+                        "steps": r["e2e_steps"]},
+                "gpu_launches": r["launches"]}
+
+    head = methods[0]
+    hs = summary(head)
+    line = {"metric": METRIC, "value": hs["value"], "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": hs["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, Xavier weights)",
-            "config": {"workload": WORKLOAD, "method": method, "bodies": N_BODIES, "verlet_pairs": NV,
-                       "filtered_pairs": P, "nlist_every": 100, "l2": "flushed between timed steps (256 MB write)",
-                       "parallelism": "replicas" if world > 1 else "single"},
-            "roofline": {"bound": "fp32", "kernel": "k_forces_" + ("fd" if method == "fd" else "adjoint"),
-                         "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved_tf / fp32_peak,
-                         "traffic": None, "flops_per_pair": fl_pair, "pairs_per_launch": P,
-                         "launch_ms": f_avg * 1e3, "force_share_of_step": sum(force_ms) / sum(step_ms),
-                         "peak_source": f"FP32 SIMT: 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz "
-                                        f"(no measured FP32 peak; HBM {peaks['hbm_gbs']} GB/s {peaks['source']})"},
-            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps},
-            "gpu_launches": launches[0], "clocks": clk}
+            "config": {"workload": WORKLOAD, "method": head, "bodies": N_BODIES,
+                       "verlet_pairs": results[head]["NV"], "filtered_pairs": results[head]["P"], "nlist_every": 100,
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "precision": ("FP32 descriptors; net on tensor cores as bf16x3 splits with FP32 accumulation"
+                                     if head == "adjoint" else "FP32 throughout")},
+            "roofline": hs["roofline"], "e2e": hs["e2e"], "gpu_launches": hs["gpu_launches"], "clocks": clk}
+    if len(methods) > 1:
+        ps = summary("fd")
+        line["plain"] = {"method": "fd", "value": ps["value"], "ms_per_step": ps["ms_per_step"],
+                         "roofline": ps["roofline"], "e2e": ps["e2e"]}
+        line["tuned_over_plain"] = hs["value"] / ps["value"]
+        line["gpu_launches"] += ps["gpu_launches"]
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        t_cpu, sample, _ = cpu_step_sample(state)
+        from amlp.configs import make_state as _ms
+        t_cpu, sample, _ = cpu_step_sample(_ms(N_BODIES, "cube26", PHI, kT=KT, seed=SEED))
         line["cpu_baseline"] = {"value": N_BODIES / t_cpu, "unit": "particle-steps/s", "cores": os.cpu_count() or 1,
                                 "kind": "port", "sample": sample}
     if rank == 0:
@@ -298,9 +354,14 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--method", choices=["fd", "adjoint"], default="fd")
+    ap.add_argument("--method", choices=["both", "fd", "adjoint"], default="both")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bodies", type=int, default=N_BODIES,
+                    help="system size (the benchmark workload is 131072; smaller sizes are for profiling)")
     args = ap.parse_args()
+    if args.bodies != N_BODIES:
+        globals()["WORKLOAD"] = WORKLOAD.replace(str(N_BODIES), str(args.bodies))
+        globals()["N_BODIES"] = args.bodies
     if args.warmup < 3:
         args.warmup = 3
     rank = int(os.environ.get("RANK", 0))

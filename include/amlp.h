@@ -32,6 +32,7 @@
  *   amlp_nvt_step_two     NVT.integrate_step_two  NVT.py:17-64
  *   amlp_nvt_step_one     NVT.integrate_step_one  NVT.py:12-15, :67-129
  *   amlp_nvt_init         Sim.move_data_to_device kinetic energies  Sim.py:157-158, :171-180
+ *   amlp_device_error     (no reference counterpart: error flags of bounded device waits)
  */
 #ifndef AMLP_H
 #define AMLP_H
@@ -159,6 +160,10 @@ amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_quat, float b
                                 const int *d_pairs, const long long *d_npairs, long long cap,
                                 const amlp_nep *nep, const amlp_mlp *mlp,
                                 float *d_F, float *d_T, double *d_pe, void *stream);
+
+/* Sticky error bits raised by device code since the last clear (1 = a bounded
+ * wait for tensor-core completion gave up; the kernel then stops early). */
+amlp_status amlp_device_error(unsigned int *flags, int clear);
 
 /* --------------------------------------------------------------- NVT integrator
  * d_th: one amlp_thermostat in device memory.

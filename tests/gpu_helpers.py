@@ -24,11 +24,14 @@ def nlist(pos, L, r, cap=None):
     n = len(pos)
     ws = torch.empty(size_query("amlp_nlist_workspace_bytes", n, float(L), float(r)), dtype=torch.uint8, device=DEV)
     cnt = torch.zeros(1, dtype=torch.int64, device=DEV)
+    cap_given = cap
     cap = cap if cap is not None else max(16, n * 64)
     out = torch.empty(cap, 2, dtype=torch.int32, device=DEV)
     call("amlp_nlist_build", pos_t.data_ptr(), n, float(L), float(r), out.data_ptr(), cap, cnt.data_ptr(),
          ws.data_ptr(), ws.numel(), stream())
     k = int(cnt.item())
+    if k > cap and cap_given is None:
+        return nlist(pos, L, r, cap=k)
     return out[:min(k, cap)].cpu().numpy().astype(np.int64), k
 
 
@@ -65,7 +68,8 @@ def descriptors(pos, quat, L, pairs, shape, hypers):
     g = torch.empty(10 * P, D, dtype=torch.float32, device=DEV)
     pr = torch.tensor(np.asarray(pairs, np.int32).reshape(-1, 2), device=DEV).contiguous()
     n = nep_struct(shape, hypers, pts_t)
-    call("amlp_descriptors", t32(pos).data_ptr(), t32(quat).data_ptr(), float(L), pr.data_ptr(), P, ctypes.byref(n),
+    pos_t, quat_t = t32(pos), t32(quat)  # keep the inputs alive across the asynchronous call
+    call("amlp_descriptors", pos_t.data_ptr(), quat_t.data_ptr(), float(L), pr.data_ptr(), P, ctypes.byref(n),
          g.data_ptr(), stream())
     return g.cpu().numpy()
 
@@ -86,7 +90,8 @@ def fd_scatter(e, pairs, N, shape):
     T = torch.zeros(N, 3, dtype=torch.float32, device=DEV)
     pe = torch.zeros(1, dtype=torch.float64, device=DEV)
     pr = torch.tensor(np.asarray(pairs, np.int32).reshape(-1, 2), device=DEV).contiguous()
-    call("amlp_fd_scatter", t32(e).data_ptr(), P, pr.data_ptr(), ctypes.byref(n), F.data_ptr(), T.data_ptr(),
+    e_t = t32(e)
+    call("amlp_fd_scatter", e_t.data_ptr(), P, pr.data_ptr(), ctypes.byref(n), F.data_ptr(), T.data_ptr(),
          pe.data_ptr(), stream())
     return F.cpu().numpy(), T.cpu().numpy(), float(pe.item())
 
@@ -104,6 +109,7 @@ def fused_forces(pos, quat, L, pairs, shape, hypers, layers, act, method="amlp_f
     if P:
         pr[:P] = torch.tensor(np.asarray(pairs, np.int32).reshape(-1, 2), device=DEV)
     npairs = torch.tensor([P], dtype=torch.int64, device=DEV)
-    call(method, t32(pos).data_ptr(), t32(quat).data_ptr(), float(L), pr.data_ptr(), npairs.data_ptr(), max(P, 1),
+    pos_t, quat_t = t32(pos), t32(quat)
+    call(method, pos_t.data_ptr(), quat_t.data_ptr(), float(L), pr.data_ptr(), npairs.data_ptr(), max(P, 1),
          ctypes.byref(n), ctypes.byref(net.struct), F.data_ptr(), T.data_ptr(), pe.data_ptr(), stream())
     return F.cpu().numpy(), T.cpu().numpy(), float(pe.item())
