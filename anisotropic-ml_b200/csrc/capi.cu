@@ -31,6 +31,7 @@ extern "C" const char *amlp_status_string(amlp_status s) {
         case AMLP_ERR_WORKSPACE: return "workspace missing or too small";
         case AMLP_ERR_CUDA: return "CUDA error";
         case AMLP_ERR_CAPACITY: return "output capacity too small";
+        case AMLP_ERR_TOO_LARGE: return "size beyond the fixed scratch of the allocation-free entry point";
         default: return "unknown status";
     }
 }

@@ -10,6 +10,8 @@
 // the cell lists, (4) one warp per body i counts the j > i within r over the
 // 27 neighbouring cells, (5) scan of the counts, (6) the same traversal
 // collects the j into shared memory, ranks them and writes them in order.
+#include <mutex>
+
 #include "common.cuh"
 #include "scan.cuh"
 
@@ -223,6 +225,91 @@ extern "C" amlp_status amlp_nlist_build(const float *d_pos, int n, float box, do
     k_count<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts);
     st = exclusive_scan_ll(w.counts, w.counts, n, w.scan_tmp, s);
     if (st) return st;
+    k_write<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap);
+    k_total<<<1, 1, 0, s>>>(w.counts, n, d_count);
+    return check_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of amlp_nlist_build.
+//
+// Some callers cannot allocate device memory at all, not even a workspace:
+// for example a host program (an MD engine or a serving process) that hands
+// this library only the buffers it owns, under a fixed GPU-memory budget, and
+// does not let plug-ins call cudaMalloc or cudaFree. This entry point needs
+// nothing beyond its inputs and outputs. Its scratch is the file-scope
+// device array below: every GPU that loads the library holds it (13
+// MiB) until the process exits.
+//
+// Limits: at most kNoAllocMaxBodies bodies, and at most kNoAllocMaxCells cells
+// per box edge. Larger boxes simply use larger cells, which gives the same
+// list. Every call shares the one array: calls that overlap on the GPU (on
+// different streams, or from different host threads without ordering) race
+// and must not be issued. The counters that must start at zero are cleared
+// on the stream at the start of every call.
+// ---------------------------------------------------------------------------
+namespace amlp {
+namespace {
+
+constexpr int kNoAllocMaxBodies = 262144;
+constexpr int kNoAllocMaxCells = 48;
+constexpr size_t kNoAllocScratchBytes = 13u << 20;
+
+__device__ __align__(256) unsigned char g_nlist_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the host-side name is only a stand-in, not a device address).
+amlp_status noalloc_scratch(void **out) {
+    int dev = 0;
+    AMLP_CHECK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return AMLP_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        AMLP_CHECK_CUDA(cudaGetSymbolAddress(&p, g_nlist_noalloc_scratch));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return AMLP_OK;
+}
+
+}  // namespace
+}  // namespace amlp
+
+extern "C" amlp_status amlp_nlist_build_noalloc(const float *d_pos, int n, float box, double r, int *d_pairs,
+                                                long long cap, long long *d_count, void *stream) {
+    if (n <= 0 || !(box > 0.f) || !(r > 0.0) || !d_pos || !d_count || cap < 0 || (cap > 0 && !d_pairs))
+        return AMLP_ERR_INVALID_ARG;
+    if (n > kNoAllocMaxBodies) return AMLP_ERR_TOO_LARGE;
+    Grid g = make_grid(n, box, r);
+    if (g.nc > kNoAllocMaxCells) {
+        g.nc = kNoAllocMaxCells;
+        g.inv_cs = (double)g.nc / g.fb;
+    }
+    Carver probe(nullptr, kNoAllocScratchBytes);
+    NlistWs w;
+    carve(probe, g, &w);
+    if (!probe.ok()) return AMLP_ERR_TOO_LARGE;
+    void *scratch = nullptr;
+    amlp_status st = noalloc_scratch(&scratch);
+    if (st) return st;
+    Carver c(scratch, kNoAllocScratchBytes);
+    carve(c, g, &w);
+    cudaStream_t s = as_stream(stream);
+    size_t ncell = (size_t)g.nc * g.nc * g.nc;
+    AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_count, 0, ncell * sizeof(int), s));
+    AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_fill, 0, ncell * sizeof(int), s));
+    int tb = 256;
+    k_cells<<<(n + tb - 1) / tb, tb, 0, s>>>(d_pos, g, w.xd, w.cell_of, w.cell_count);
+    if ((st = exclusive_scan_int(w.cell_count, w.cell_start, (long long)ncell, w.scan_tmp, s))) return st;
+    k_fill<<<(n + tb - 1) / tb, tb, 0, s>>>(n, w.cell_of, w.cell_start, w.cell_fill, w.cell_list);
+    int nb = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    k_count<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts);
+    if ((st = exclusive_scan_ll(w.counts, w.counts, n, w.scan_tmp, s))) return st;
     k_write<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap);
     k_total<<<1, 1, 0, s>>>(w.counts, n, d_count);
     return check_launch();

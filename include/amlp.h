@@ -50,6 +50,7 @@ typedef int amlp_status;
 #define AMLP_ERR_WORKSPACE 3       /* workspace smaller than the query returned */
 #define AMLP_ERR_CUDA 4            /* a CUDA call failed (see amlp_last_cuda_error) */
 #define AMLP_ERR_CAPACITY 5        /* output capacity too small (count still written) */
+#define AMLP_ERR_TOO_LARGE 6       /* size beyond the fixed scratch of an allocation-free entry point */
 
 #define AMLP_ACT_RELU 0
 #define AMLP_ACT_TANH 1
@@ -115,6 +116,16 @@ amlp_status amlp_nlist_workspace_bytes(int n, float box, double r, size_t *bytes
 amlp_status amlp_nlist_build(const float *d_pos, int n, float box, double r,
                              int *d_pairs, long long cap, long long *d_count,
                              void *d_ws, size_t ws_bytes, void *stream);
+
+/* Same list, for callers that cannot allocate device memory at all (not even a
+ * workspace), e.g. plug-ins of a host program that owns every GPU buffer under
+ * a fixed memory budget. No reference counterpart. Scratch is a fixed array
+ * inside the library (13 MiB per GPU, held until exit); n is limited to
+ * 262,144 bodies (AMLP_ERR_TOO_LARGE beyond). The first call on a device looks
+ * up the array's device address and should come before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU race. */
+amlp_status amlp_nlist_build_noalloc(const float *d_pos, int n, float box, double r,
+                                     int *d_pairs, long long cap, long long *d_count, void *stream);
 
 /* --------------------------------------------------------------- pair filter
  * Minimum image (FP32, box L) and |t| < cutoff on the Verlet pairs, kept in
