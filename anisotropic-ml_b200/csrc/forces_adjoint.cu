@@ -10,8 +10,9 @@
 //   3  net forward and backward on the tensor cores: every product is three
 //      bf16 x bf16 -> fp32 MMAs (hi*hi + hi*lo + lo*hi of the bf16 splits of
 //      activations and weights), accumulators in TMEM; gives dE/dg;
-//   4  descriptor backward (FP32), recomputing the per-point quantities instead
-//      of keeping them: dE/dA = 2 dE/dg_ang A, then per point
+//   4  descriptor backward (FP32): the per-point quantities are recomputed
+//      instead of stored (only the per-pair sums A stay in registers across the
+//      net): dE/dA = 2 dE/dg_ang A, then per point
 //      dE/dr_a = sum_n dE/df_n f_n'(d) rhat + sum_lm dE/dY_lm grad Y_lm;
 //   5  F_pair = -sum_{a in i} dE/dp_a, T_i = -sum_{a in i} p_a x dE/dp_a,
 //      T_j = -sum_{a in j} (p_a - t) x dE/dp_a (dE/dp_a = dE/dr_a minus the mean,
@@ -169,12 +170,14 @@ __device__ __forceinline__ void accumulate_A(const float *Ri, const float *Rj, f
 
 
 // Forward of one half of the harmonics: radial sums (half 0) and the partial
-// sums of squares of this half's harmonics, written to gp[0..47] (zeros elsewhere).
+// sums of squares of this half's harmonics, written to gp[0..47] (zeros
+// elsewhere). The sums A of this half stay in the caller's registers for the
+// backward.
 template <class Cfg, int H>
 __device__ __forceinline__ void half_forward(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
-                                             float inv_rc, float *gp) {
+                                             float inv_rc, float *gp, float (&A)[Cfg::NA][Half<Cfg>::KC]) {
     constexpr int KC = Half<Cfg>::KC;
-    float A[Cfg::NA][KC], Rr[Cfg::NR];
+    float Rr[Cfg::NR];
     accumulate_A<Cfg, KC, H * KC>(Ri, Rj, t, npts, c, inv_rc, A, Rr);
     for (int k = 0; k < 48; ++k) gp[k] = 0.f;
     if (H == 0) {
@@ -191,15 +194,15 @@ __device__ __forceinline__ void half_forward(const float *Ri, const float *Rj, f
     }
 }
 
-// Backward of one half: given dE/dg (dg), the partial sums over points of
+// Backward of one half: given dE/dg (dg) and the forward sums A of this half
+// (overwritten), the partial sums over points of
 // dE/dr_a needed for the pair force and torques: sum_{a in i} G_a, sum_a G_a,
 // sum_{a in i} p_a x G_a, sum_{a in j} (p_a - t) x G_a -> out[12].
 template <class Cfg, int H>
 __device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
-                                              float inv_rc, const float *dg, float *out) {
+                                              float inv_rc, const float *dg, float *out,
+                                              float (&A)[Cfg::NA][Half<Cfg>::KC]) {
     constexpr int KC = Half<Cfg>::KC;
-    float A[Cfg::NA][KC], Rr[Cfg::NR];
-    accumulate_A<Cfg, KC, H * KC>(Ri, Rj, t, npts, c, inv_rc, A, Rr);
 #pragma unroll
     for (int kk = 0; kk < KC; ++kk) {
         if (H * KC + kk < Cfg::K) {
@@ -479,8 +482,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             S.cen[3 * p + 1] = c.y;
             S.cen[3 * p + 2] = c.z;
         }
-        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP);
-        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * DP);
+        float A[Cfg::NA][KC];  // this half's sum_a f_n Y_k, kept in registers for the backward
+        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, A);
+        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * DP, A);
         __syncthreads();
         // ---- 3. net forward + backward on the tensor cores
         {
@@ -585,8 +589,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         }
         __syncthreads();
         // ---- descriptor backward
-        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + p * 12);
-        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * 12);
+        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + p * 12, A);
+        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * 12, A);
         __syncthreads();
         // ---- 5. per-pair forces and torques
         if (tid < kAP) {
