@@ -60,6 +60,12 @@ class Nvt(ctypes.Structure):
                 ("nve", ctypes.c_int)]
 
 
+class Replica(ctypes.Structure):
+    """``amlp_replica``: per-system parameters of a multi-system launch."""
+    _fields_ = [("kT", ctypes.c_float), ("n_dof", ctypes.c_float), ("rn_dof", ctypes.c_float),
+                ("box", ctypes.c_float), ("nve", ctypes.c_int), ("pad", ctypes.c_int * 3)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _LL = ctypes.c_longlong
@@ -85,6 +91,12 @@ SIGNATURES = {
     "amlp_nvt_init": [_P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _I, _P, _P, _SZ, _P],
     "amlp_nvt_step_two": [_P, _P, _P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _P, _P],
     "amlp_nvt_step_one": [_P, _P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _P, _P, _SZ, _P],
+    "amlp_multi_pair_filter": [_P, _P, _P, _D, _P, _P, _LL, _P, _P, _P, _SZ, _P],
+    "amlp_multi_forces_adjoint": [_P, _P, _P, _P, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp),
+                                  _P, _P, _P, _P],
+    "amlp_multi_nvt_init": [_P, _P, _P, _P, _P, _I, _I, ctypes.POINTER(Nvt), _P, _P],
+    "amlp_multi_nvt_step_two": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, ctypes.POINTER(Nvt), _P, _P],
+    "amlp_multi_nvt_step_one": [_P, _P, _P, _P, _P, _P, _P, _P, _I, _P, ctypes.POINTER(Nvt), _P, _P],
 }
 
 lib.amlp_version.restype = ctypes.c_int

@@ -11,9 +11,19 @@ namespace {
 constexpr int kFilterBlocks = 4 * kNumSM;
 constexpr int kFilterThreads = 256;
 
-__device__ __forceinline__ bool keep_pair(const float *pos, const int *vp, long long k, float L, double cutoff) {
+// Box of pair k: L, or with several systems in one launch the box of the
+// system of body i.
+struct BoxOf {
+    float L;
+    const int *rep;
+    const amlp_replica *rp;
+    __device__ __forceinline__ float operator()(int i) const { return rep ? rp[rep[i]].box : L; }
+};
+
+__device__ __forceinline__ bool keep_pair(const float *pos, const int *vp, long long k, BoxOf box, double cutoff) {
     float d;
-    min_image(pos, vp[2 * k], vp[2 * k + 1], L, &d);
+    int i = vp[2 * k];
+    min_image(pos, i, vp[2 * k + 1], box(i), &d);
     return (double)d < cutoff;
 }
 
@@ -23,7 +33,7 @@ __device__ __forceinline__ void chunk_range(long long nv, long long *s, long lon
     *e = min(nv, *s + chunk);
 }
 
-__global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *pos, float L, double cutoff, const int *vp,
+__global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *pos, BoxOf L, double cutoff, const int *vp,
                                                                  const long long *d_nv, long long cap, int *counts) {
     long long nv = min(*d_nv, cap), s, e;
     chunk_range(nv, &s, &e);
@@ -41,7 +51,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *po
     }
 }
 
-__global__ void __launch_bounds__(kFilterThreads) k_filter_write(const float *pos, float L, double cutoff, const int *vp,
+__global__ void __launch_bounds__(kFilterThreads) k_filter_write(const float *pos, BoxOf L, double cutoff, const int *vp,
                                                                  const long long *d_nv, long long cap, const int *counts,
                                                                  int *out, long long *d_np) {
     __shared__ long long base_s;
@@ -100,8 +110,24 @@ extern "C" amlp_status amlp_pair_filter(const float *d_pos, float box, double cu
     cudaStream_t s = as_stream(stream);
     int *counts = static_cast<int *>(d_ws);
     double c = cutoff;
-    k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, box, c, d_vpairs, d_nverlet, cap_verlet, counts);
-    k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, box, c, d_vpairs, d_nverlet, cap_verlet, counts,
+    BoxOf b{box, nullptr, nullptr};
+    k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, c, d_vpairs, d_nverlet, cap_verlet, counts);
+    k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, c, d_vpairs, d_nverlet, cap_verlet, counts,
+                                                            d_pairs, d_npairs);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_multi_pair_filter(const float *d_pos, const int *d_rep, const amlp_replica *d_rp,
+                                              double cutoff, const int *d_vpairs, const long long *d_nverlet,
+                                              long long cap_verlet, int *d_pairs, long long *d_npairs, void *d_ws,
+                                              size_t ws_bytes, void *stream) {
+    if (!d_pos || !d_rep || !d_rp || !d_nverlet || !d_npairs || cap_verlet < 0) return AMLP_ERR_INVALID_ARG;
+    if (!d_ws || ws_bytes < kFilterBlocks * sizeof(int)) return AMLP_ERR_WORKSPACE;
+    cudaStream_t s = as_stream(stream);
+    int *counts = static_cast<int *>(d_ws);
+    BoxOf b{0.f, d_rep, d_rp};
+    k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, cutoff, d_vpairs, d_nverlet, cap_verlet, counts);
+    k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, cutoff, d_vpairs, d_nverlet, cap_verlet, counts,
                                                             d_pairs, d_npairs);
     return check_launch();
 }

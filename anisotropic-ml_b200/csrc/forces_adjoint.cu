@@ -331,12 +331,16 @@ __device__ __forceinline__ void store_split8(char *tile_hi, int K, int p, int c0
     *reinterpret_cast<uint4 *>(tile_hi + kAP * K * 2 + off) = *reinterpret_cast<uint4 *>(lo);
 }
 
-template <class Cfg>
+// MULTI: the pairs come from many systems in one launch; body i's system is
+// rep[i], its box rp[rep[i]].box, and the pair energies are summed per system
+// into pe[rep[i]].
+template <class Cfg, bool MULTI>
 __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *pos, const float *quat, float L,
                                                                 const int *pairs, const long long *d_np, long long cap,
                                                                 const float *pts, int npts, float inv_rc, float en_min,
                                                                 float en_range, AdjNet net, const float *w, float *F,
-                                                                float *T, double *pe) {
+                                                                float *T, double *pe, const int *rep,
+                                                                const amlp_replica *rp) {
     constexpr int KC = Half<Cfg>::KC;
     constexpr int DP = 48;  // padded descriptor width in fp32 staging
     extern __shared__ __align__(128) char smem_raw[];
@@ -453,7 +457,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             long long pr = min(p0 + tid, P - 1);
             int i = pairs[2 * pr], j = pairs[2 * pr + 1];
             float dd;
-            float3 tt = min_image(pos, i, j, L, &dd);
+            float3 tt = min_image(pos, i, j, MULTI ? rp[rep[i]].box : L, &dd);
             S.t[3 * tid] = tt.x;
             S.t[3 * tid + 1] = tt.y;
             S.t[3 * tid + 2] = tt.z;
@@ -574,7 +578,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             tc::fence_before();
             __syncthreads();
         }
-        if (h == 0 && p < valid)
+        if (!MULTI && h == 0 && p < valid)
             pe_acc += (double)en_min + (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
         // ---- 4. recompute the rotated points (their area held the MLP tiles)
         for (int idx = tid; idx < kAP * nd; idx += kAThreads) {
@@ -666,12 +670,26 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                     atomicAdd(T + 3 * i + k, v[3 + k]);
                 }
             }
+            if (MULTI && pe) {  // pair energies summed per system (systems own contiguous bodies)
+                double e = ok ? (double)en_min + (double)en_range *
+                                    (double)(S.eps[q] + S.eps[kAP + q] + S.par[net.bias_off[net.nh] + kWpad])
+                              : 0.0;
+                int rk = ok ? rep[i] : -1 - lane;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    int ro = __shfl_up_sync(0xffffffffu, rk, o);
+                    double y = __shfl_up_sync(0xffffffffu, e, o);
+                    if (lane >= o && ro == rk) e += y;
+                }
+                int rn = __shfl_down_sync(0xffffffffu, rk, 1);
+                if (ok && (lane == 31 || rn != rk)) atomicAdd(pe + rk, e);
+            }
         }
         __syncthreads();
         if (abort_flag) break;
     }
     // ---- pair-energy sum, TMEM release
-    if (pe) {
+    if (!MULTI && pe) {
         double v = pe_acc;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -679,7 +697,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     }
     tc::fence_before();
     __syncthreads();
-    if (pe && tid == 0) {
+    if (!MULTI && pe && tid == 0) {
         double s = 0.0;
         for (int k = 0; k < kAThreads / 32; ++k) s += pe_s[k];
         if (s != 0.0) atomicAdd(pe, s);
@@ -703,10 +721,10 @@ amlp_status check_mlp(const amlp_mlp *m, int D);
 
 using namespace amlp;
 
-extern "C" amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
-                                           const long long *d_npairs, long long cap, const amlp_nep *nep,
-                                           const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe,
-                                           void *stream) {
+static amlp_status launch_adjoint(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                  const long long *d_npairs, long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
+                                  float *d_F, float *d_T, double *d_pe, const int *d_rep, const amlp_replica *d_rp,
+                                  void *stream) {
     amlp_status st = check_nep(nep);
     if (st) return st;
     const int D = nep_D(nep);
@@ -747,11 +765,39 @@ extern "C" amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_qu
                   (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 + 128;
     if (smem > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
-    AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_forces_adjoint<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_forces_adjoint<Cfg><<<kNumSM, kAThreads, smem, as_stream(stream)>>>(
-        d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, 1.0f / nep->nep_cutoff, nep->en_min,
-        nep->en_max - nep->en_min, net, mlp->d_w, d_F, d_T, d_pe);
+    cudaStream_t s = as_stream(stream);
+    const float inv_rc = 1.0f / nep->nep_cutoff, rng = nep->en_max - nep->en_min;
+    if (d_rep) {
+        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_forces_adjoint<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+        k_forces_adjoint<Cfg, true><<<kNumSM, kAThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                                                    nep->d_pts, npts, inv_rc, nep->en_min, rng, net,
+                                                                    mlp->d_w, d_F, d_T, d_pe, d_rep, d_rp);
+    } else {
+        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_forces_adjoint<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+        k_forces_adjoint<Cfg, false><<<kNumSM, kAThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                                                     nep->d_pts, npts, inv_rc, nep->en_min, rng, net,
+                                                                     mlp->d_w, d_F, d_T, d_pe, nullptr, nullptr);
+    }
     return check_launch();
+}
+
+extern "C" amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                           const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                           const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe,
+                                           void *stream) {
+    return launch_adjoint(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, nullptr, nullptr,
+                          stream);
+}
+
+extern "C" amlp_status amlp_multi_forces_adjoint(const float *d_pos, const float *d_quat, const int *d_rep,
+                                                 const amlp_replica *d_rp, const int *d_pairs,
+                                                 const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                                 const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe,
+                                                 void *stream) {
+    if (!d_rep || !d_rp) return AMLP_ERR_INVALID_ARG;
+    return launch_adjoint(d_pos, d_quat, 0.f, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, d_rep, d_rp, stream);
 }
 
 extern "C" amlp_status amlp_device_error(unsigned int *flags, int clear) {

@@ -13,36 +13,40 @@ namespace {
 
 constexpr int kIntThreads = 256;
 
-// update_variables (IntegrateStepTwoKernels.py:74-130), one thread.
-__global__ void k_thermo_update(amlp_nvt p, amlp_thermostat *th) {
-    if (threadIdx.x != 0) return;
-    if (p.nve) {
+// update_variables (IntegrateStepTwoKernels.py:74-130) of one thermostat.
+__device__ __forceinline__ void thermo_update(float ts, float tau, float kT, float n_dof, float rn_dof, int nve,
+                                              amlp_thermostat *th) {
+    if (nve) {
         th->thermo_fac = 1.0f;
         return;
     }
-    const float ts = p.dt, tau = p.tau, kT = p.kT;
     const float c = __fdiv_rn(__fdiv_rn(ts, tau), tau);
-    const float trans_temp = __fmul_rn(__fdiv_rn(2.0f, p.n_dof), (float)th->ke_t);
+    const float trans_temp = __fmul_rn(__fdiv_rn(2.0f, n_dof), (float)th->ke_t);
     const float gt = __fsub_rn(__fdiv_rn(trans_temp, kT), 1.0f);
     const float xi_p = __fadd_rn(th->xi, __fmul_rn(__fmul_rn(0.5f, c), gt));
     const float xi_new = __fadd_rn(xi_p, __fmul_rn(__fmul_rn(0.5f, c), gt));
     th->eta = __fadd_rn(th->eta, __fmul_rn(xi_p, ts));
     th->thermo_fac = expf(__fmul_rn(__fmul_rn(-0.5f, xi_new), ts));
     th->xi = xi_new;
-    const float rot_temp = __fdiv_rn(__fmul_rn(2.0f, (float)th->ke_r), p.rn_dof);
+    const float rot_temp = __fdiv_rn(__fmul_rn(2.0f, (float)th->ke_r), rn_dof);
     const float gr = __fsub_rn(__fdiv_rn(rot_temp, kT), 1.0f);
     const float xr_p = __fadd_rn(th->xi_rot, __fmul_rn(__fmul_rn(0.5f, c), gr));
     th->xi_rot = __fadd_rn(xr_p, __fmul_rn(__fmul_rn(0.5f, c), gr));
     th->eta_rot = __fadd_rn(th->eta_rot, __fmul_rn(xr_p, ts));
 }
 
-// NVT.py:42-62: accel = F/m, v <- v f + (dt/2) accel, and step_two_rotation
-// (IntegrateStepTwoKernels.py:2-71): torque into the body frame, dp, p kick.
-__global__ void k_step_two(float *vel, float *accel, const float *F, const float *mass, const float *quat,
-                           const float *T, float *angmom, float *dp, int n, amlp_nvt p, const amlp_thermostat *th) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float f = th->thermo_fac, m = mass[i], hdt = __fmul_rn(0.5f, p.dt);
+__global__ void k_thermo_update(amlp_nvt p, amlp_thermostat *th) {
+    if (threadIdx.x != 0) return;
+    thermo_update(p.dt, p.tau, p.kT, p.n_dof, p.rn_dof, p.nve, th);
+}
+
+// NVT.py:42-62 for body i: accel = F/m, v <- v f + (dt/2) accel, and
+// step_two_rotation (IntegrateStepTwoKernels.py:2-71): torque into the body
+// frame, dp, angular-momentum kick. f and xi_rot come from the body's thermostat.
+__device__ __forceinline__ void step_two_body(int i, float *vel, float *accel, const float *F, const float *mass,
+                                              const float *quat, const float *T, float *angmom, float *dp, float ts,
+                                              float f, float xi_rot) {
+    const float m = mass[i], hdt = __fmul_rn(0.5f, ts);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         float a = __fdiv_rn(F[3 * i + k], m);
@@ -60,19 +64,25 @@ __global__ void k_step_two(float *vel, float *accel, const float *F, const float
     const float tx = __fadd_rn(__fadd_rn(__fmul_rn(t1, coef1), t2x), __fmul_rn(__fmul_rn(2.0f, ss), c1));
     const float ty = __fadd_rn(__fadd_rn(__fmul_rn(t2, coef1), t2y), __fmul_rn(__fmul_rn(2.0f, ss), c2));
     const float tz = __fadd_rn(__fadd_rn(__fmul_rn(t3, coef1), t2z), __fmul_rn(__fmul_rn(2.0f, ss), c3));
-    const float ts = p.dt;
     float d[4];
     d[0] = __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(c1, tx), __fmul_rn(c2, ty)), __fmul_rn(c3, tz)), ts);
     d[1] = __fmul_rn(__fadd_rn(__fsub_rn(-__fmul_rn(c2, tz), -__fmul_rn(c3, ty)), __fmul_rn(c0, tx)), ts);
     d[2] = __fmul_rn(__fadd_rn(__fsub_rn(-__fmul_rn(c3, tx), -__fmul_rn(c1, tz)), __fmul_rn(c0, ty)), ts);
     d[3] = __fmul_rn(__fadd_rn(__fsub_rn(-__fmul_rn(c1, ty), -__fmul_rn(c2, tx)), __fmul_rn(c0, tz)), ts);
     // expf((-dt/2.0) * xi_rot) with the product in double (IntegrateStepTwoKernels.py:62)
-    const float ef = expf((float)(((double)(-ts) / 2.0) * (double)th->xi_rot));
+    const float ef = expf((float)(((double)(-ts) / 2.0) * (double)xi_rot));
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         dp[4 * i + k] = d[k];
         angmom[4 * i + k] = __fadd_rn(__fmul_rn(angmom[4 * i + k], ef), d[k]);
     }
+}
+
+__global__ void k_step_two(float *vel, float *accel, const float *F, const float *mass, const float *quat,
+                           const float *T, float *angmom, float *dp, int n, amlp_nvt p, const amlp_thermostat *th) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    step_two_body(i, vel, accel, F, mass, quat, T, angmom, dp, p.dt, th->thermo_fac, th->xi_rot);
 }
 
 struct Q4 {
@@ -164,50 +174,55 @@ __device__ void reduce_ke(double kt, double kr, double *part, unsigned int *done
     }
 }
 
-// step_one_translation + step_one_rotation + kinetic energies
-// (IntegrateStepOneKernels.py:3-251, NVT.py:67-129).
+// step_one_translation + step_one_rotation of body i (IntegrateStepOneKernels.py:3-210,
+// NVT.py:67-106); returns its translational and rotational kinetic energies.
+__device__ __forceinline__ void step_one_body(int i, float *pos, float *vel, const float *accel, float *quat,
+                                              float *angmom, const float *dp, const float *mass, float ts, float f,
+                                              float xi_rot, float L, const float *moi, double *kt, double *kr) {
+    float v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float nv = __fmul_rn(__fadd_rn(vel[3 * i + k], __fmul_rn(__fmul_rn(accel[3 * i + k], 0.5f), ts)), f);
+        vel[3 * i + k] = nv;
+        v[k] = nv;
+        float np = __fadd_rn(pos[3 * i + k], __fmul_rn(nv, ts));
+        np = np > 0.5f * L ? __fsub_rn(np, L) : np;
+        np = np < -0.5f * L ? __fadd_rn(np, L) : np;
+        pos[3 * i + k] = np;
+    }
+    // rotation: exp factor with the FP32 literal 2.0f (IntegrateStepOneKernels.py:19)
+    const float ef = expf(__fmul_rn(__fdiv_rn(-ts, 2.0f), xi_rot));
+    Q4 ang, ori;
+    float4 q = load_quat(quat, i);
+    ori = {{q.x, q.y, q.z, q.w}};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ang.a[k] = __fmul_rn(__fadd_rn(angmom[4 * i + k], dp[4 * i + k]), ef);
+    const float hts = __fmul_rn(0.5f, ts);
+    perm_rotate(ang, ori, 1, moi[2], hts);
+    perm_rotate(ang, ori, 2, moi[1], hts);
+    perm_rotate(ang, ori, 3, moi[0], ts);
+    perm_rotate(ang, ori, 2, moi[1], hts);
+    perm_rotate(ang, ori, 1, moi[2], hts);
+    float nrm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(ori.a[0], ori.a[0]), __fmul_rn(ori.a[1], ori.a[1])),
+                                               __fmul_rn(ori.a[2], ori.a[2])), __fmul_rn(ori.a[3], ori.a[3])));
+    float4 qn = make_float4(__fdiv_rn(ori.a[0], nrm), __fdiv_rn(ori.a[1], nrm), __fdiv_rn(ori.a[2], nrm),
+                            __fdiv_rn(ori.a[3], nrm));
+    reinterpret_cast<float4 *>(quat)[i] = qn;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) angmom[4 * i + k] = ang.a[k];
+    *kt = (double)trans_ke(v, mass[i]);
+    *kr = (double)rot_ke(qn, ang.a, moi);
+}
+
+// Step one of all bodies plus the kinetic-energy sums (NVT.py:67-129).
 __global__ void __launch_bounds__(kIntThreads) k_step_one(float *pos, float *vel, const float *accel, float *quat,
                                                           float *angmom, const float *dp, const float *mass, int n,
                                                           amlp_nvt p, amlp_thermostat *th, double *part,
                                                           unsigned int *done) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double kt = 0.0, kr = 0.0;
-    if (i < n) {
-        const float ts = p.dt, f = th->thermo_fac, L = p.box;
-        float v[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            float nv = __fmul_rn(__fadd_rn(vel[3 * i + k], __fmul_rn(__fmul_rn(accel[3 * i + k], 0.5f), ts)), f);
-            vel[3 * i + k] = nv;
-            v[k] = nv;
-            float np = __fadd_rn(pos[3 * i + k], __fmul_rn(nv, ts));
-            np = np > 0.5f * L ? __fsub_rn(np, L) : np;
-            np = np < -0.5f * L ? __fadd_rn(np, L) : np;
-            pos[3 * i + k] = np;
-        }
-        // rotation: exp factor with the FP32 literal 2.0f (IntegrateStepOneKernels.py:19)
-        const float ef = expf(__fmul_rn(__fdiv_rn(-ts, 2.0f), th->xi_rot));
-        Q4 ang, ori;
-        float4 q = load_quat(quat, i);
-        ori = {{q.x, q.y, q.z, q.w}};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) ang.a[k] = __fmul_rn(__fadd_rn(angmom[4 * i + k], dp[4 * i + k]), ef);
-        const float hts = __fmul_rn(0.5f, ts);
-        perm_rotate(ang, ori, 1, p.moi[2], hts);
-        perm_rotate(ang, ori, 2, p.moi[1], hts);
-        perm_rotate(ang, ori, 3, p.moi[0], ts);
-        perm_rotate(ang, ori, 2, p.moi[1], hts);
-        perm_rotate(ang, ori, 1, p.moi[2], hts);
-        float nrm = __fsqrt_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(ori.a[0], ori.a[0]), __fmul_rn(ori.a[1], ori.a[1])),
-                                                   __fmul_rn(ori.a[2], ori.a[2])), __fmul_rn(ori.a[3], ori.a[3])));
-        float4 qn = make_float4(__fdiv_rn(ori.a[0], nrm), __fdiv_rn(ori.a[1], nrm), __fdiv_rn(ori.a[2], nrm),
-                                __fdiv_rn(ori.a[3], nrm));
-        reinterpret_cast<float4 *>(quat)[i] = qn;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) angmom[4 * i + k] = ang.a[k];
-        kt = (double)trans_ke(v, mass[i]);
-        kr = (double)rot_ke(qn, ang.a, p.moi);
-    }
+    if (i < n) step_one_body(i, pos, vel, accel, quat, angmom, dp, mass, p.dt, th->thermo_fac, th->xi_rot, p.box,
+                             p.moi, &kt, &kr);
     reduce_ke(kt, kr, part, done, th);
 }
 
@@ -228,6 +243,87 @@ __global__ void __launch_bounds__(kIntThreads) k_nvt_init(const float *vel, cons
 }
 
 int blocks_for(int n) { return (n + kIntThreads - 1) / kIntThreads; }
+
+// ---------------------------------------------------------------- many systems
+// Segmented (by system) sum of (kt, kr) over the lanes of a warp whose keys form
+// contiguous runs; one FP64 atomic per run into the system's thermostat.
+__device__ __forceinline__ void add_ke_by_system(int key, double kt, double kr, amlp_thermostat *th) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int ko = __shfl_up_sync(0xffffffffu, key, o);
+        double a = __shfl_up_sync(0xffffffffu, kt, o), b = __shfl_up_sync(0xffffffffu, kr, o);
+        if (lane >= o && ko == key) {
+            kt += a;
+            kr += b;
+        }
+    }
+    int kn = __shfl_down_sync(0xffffffffu, key, 1);
+    if (key >= 0 && (lane == 31 || kn != key)) {
+        atomicAdd(&th[key].ke_t, kt);
+        atomicAdd(&th[key].ke_r, kr);
+    }
+}
+
+__global__ void k_multi_zero_ke(int nrep, amlp_thermostat *th) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrep) {
+        th[r].ke_t = 0.0;
+        th[r].ke_r = 0.0;
+    }
+}
+
+__global__ void k_multi_nvt_init(const float *vel, const float *quat, const float *angmom, const float *mass,
+                                 const int *rep, int n, amlp_nvt p, amlp_thermostat *th) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double kt = 0.0, kr = 0.0;
+    int key = -1 - (int)(threadIdx.x & 31);
+    if (i < n) {
+        float v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+        float a[4] = {angmom[4 * i], angmom[4 * i + 1], angmom[4 * i + 2], angmom[4 * i + 3]};
+        kt = (double)trans_ke(v, mass[i]);
+        kr = (double)rot_ke(load_quat(quat, i), a, p.moi);
+        key = rep[i];
+    }
+    add_ke_by_system(key, kt, kr, th);
+}
+
+// Thermostat update of every system; clears its kinetic-energy sums for the
+// step one that follows.
+__global__ void k_multi_thermo_update(int nrep, const amlp_replica *rp, amlp_nvt p, amlp_thermostat *th) {
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrep) return;
+    const amlp_replica q = rp[r];
+    thermo_update(p.dt, p.tau, q.kT, q.n_dof, q.rn_dof, q.nve, th + r);
+    th[r].ke_t = 0.0;
+    th[r].ke_r = 0.0;
+}
+
+__global__ void k_multi_step_two(float *vel, float *accel, const float *F, const float *mass, const float *quat,
+                                 const float *T, float *angmom, float *dp, const int *rep, int n, amlp_nvt p,
+                                 const amlp_thermostat *th) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const amlp_thermostat *t = th + rep[i];
+    step_two_body(i, vel, accel, F, mass, quat, T, angmom, dp, p.dt, t->thermo_fac, t->xi_rot);
+}
+
+__global__ void __launch_bounds__(kIntThreads) k_multi_step_one(float *pos, float *vel, const float *accel,
+                                                                float *quat, float *angmom, const float *dp,
+                                                                const float *mass, const int *rep, int n,
+                                                                const amlp_replica *rp, amlp_nvt p,
+                                                                amlp_thermostat *th) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double kt = 0.0, kr = 0.0;
+    int key = -1 - (int)(threadIdx.x & 31);
+    if (i < n) {
+        key = rep[i];
+        const amlp_thermostat *t = th + key;
+        step_one_body(i, pos, vel, accel, quat, angmom, dp, mass, p.dt, t->thermo_fac, t->xi_rot, rp[key].box, p.moi,
+                      &kt, &kr);
+    }
+    add_ke_by_system(key, kt, kr, th);
+}
 
 }  // namespace
 }  // namespace amlp
@@ -290,5 +386,42 @@ extern "C" amlp_status amlp_nvt_step_one(float *d_pos, float *d_vel, const float
     AMLP_CHECK_CUDA(cudaMemsetAsync(done, 0, sizeof(unsigned int), s));
     k_step_one<<<blocks_for(n), kIntThreads, 0, s>>>(d_pos, d_vel, d_accel, d_quat, d_angmom, d_dp,
                                                                      d_mass, n, *prm, d_th, part, done);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_multi_nvt_init(const float *d_vel, const float *d_quat, const float *d_angmom,
+                                           const float *d_mass, const int *d_rep, int n, int nrep,
+                                           const amlp_nvt *prm, amlp_thermostat *d_th, void *stream) {
+    if (n <= 0 || nrep <= 0 || !prm || !d_vel || !d_quat || !d_angmom || !d_mass || !d_rep || !d_th)
+        return AMLP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    k_multi_zero_ke<<<(nrep + 127) / 128, 128, 0, s>>>(nrep, d_th);
+    k_multi_nvt_init<<<blocks_for(n), kIntThreads, 0, s>>>(d_vel, d_quat, d_angmom, d_mass, d_rep, n, *prm, d_th);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_multi_nvt_step_two(float *d_vel, float *d_accel, const float *d_F, const float *d_mass,
+                                               const float *d_quat, const float *d_T, float *d_angmom, float *d_dp,
+                                               const int *d_rep, int n, int nrep, const amlp_replica *d_rp,
+                                               const amlp_nvt *prm, amlp_thermostat *d_th, void *stream) {
+    if (n <= 0 || nrep <= 0 || !prm || !d_vel || !d_accel || !d_F || !d_mass || !d_quat || !d_T || !d_angmom ||
+        !d_dp || !d_rep || !d_rp || !d_th)
+        return AMLP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    k_multi_thermo_update<<<(nrep + 127) / 128, 128, 0, s>>>(nrep, d_rp, *prm, d_th);
+    k_multi_step_two<<<blocks_for(n), kIntThreads, 0, s>>>(d_vel, d_accel, d_F, d_mass, d_quat, d_T, d_angmom, d_dp,
+                                                           d_rep, n, *prm, d_th);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_multi_nvt_step_one(float *d_pos, float *d_vel, const float *d_accel, float *d_quat,
+                                               float *d_angmom, const float *d_dp, const float *d_mass,
+                                               const int *d_rep, int n, const amlp_replica *d_rp,
+                                               const amlp_nvt *prm, amlp_thermostat *d_th, void *stream) {
+    if (n <= 0 || !prm || !d_pos || !d_vel || !d_accel || !d_quat || !d_angmom || !d_dp || !d_mass || !d_rep ||
+        !d_rp || !d_th)
+        return AMLP_ERR_INVALID_ARG;
+    k_multi_step_one<<<blocks_for(n), kIntThreads, 0, as_stream(stream)>>>(d_pos, d_vel, d_accel, d_quat, d_angmom,
+                                                                          d_dp, d_mass, d_rep, n, d_rp, *prm, d_th);
     return check_launch();
 }

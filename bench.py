@@ -271,6 +271,50 @@ def _e2e(system, method, steps, dist, dev):
     return ms, nbytes
 
 
+def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) -> dict:
+    """Mixed request stream served by continuous batching, and the same requests
+    run one after another with the plain FP32 method (a subsample, timed)."""
+    import torch
+    from amlp.configs import make_state
+    from amlp.engine import EnergyNet, Hypers, System
+    from amlp.serving import Server, request_stream
+    nets = {name: EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED + k, device=dev)
+            for k, name in enumerate(("cube26", "tetra16", "cyl24"))}
+    reqs = request_stream(n_requests, seed=SEED, steps=steps, rate=rate)
+    srv = Server(nets, hbm_budget=24 << 30, segment=100, device=dev)
+    stats = srv.run(reqs).summary()
+    seq_reqs = reqs
+    seq_steps = 20
+    body_steps, ms = 0, 0.0
+    for r in seq_reqs:
+        st = make_state(r.n, r.shape, r.phi, kT=r.kT, seed=r.seed)
+        sysm = System(st, r.shape, Hypers(), nets[r.shape], kT=r.kT, dt=DT, device=dev)
+        sysm.run(3, method="fd")  # warm-up: graph capture (the timed steps replay the same graph size)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sysm.run(seq_steps, method="fd")
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        body_steps += r.n * seq_steps
+        del sysm
+    seq_rate = body_steps / (ms / 1e3)
+    return {"value": stats["particle_steps_per_s"], "unit": "particle-steps/s",
+            "segment_ms_p50": stats["segment_ms_p50"], "segment_ms_p99": stats["segment_ms_p99"],
+            "request_latency_s_p50": stats["request_latency_s_p50"],
+            "request_latency_s_p99": stats["request_latency_s_p99"],
+            "max_concurrent": stats["max_concurrent"], "requests": stats["requests"],
+            "graphs_captured": stats["graphs_captured"], "wall_s": stats["wall_s"],
+            "stream": f"{n_requests} requests, {steps} steps each, Poisson arrivals at {rate}/s, N log-uniform "
+                      f"[500, 50000], shape uniform {{cube26, tetra16, cyl24}}, phi U[0.25, 0.45], kT U[0.5, 2.0], "
+                      f"seed {SEED}; adjoint forces, bf16x3 tensor-core net, 100-step segments, 24 GiB budget",
+            "sequential_plain": {"value": seq_rate, "unit": "particle-steps/s",
+                                 "sample": f"all {len(seq_reqs)} requests x {seq_steps} steps, one after "
+                                           f"another, plain FP32 finite differences, CUDA graphs"},
+            "served_over_sequential_plain": stats["particle_steps_per_s"] / seq_rate}
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     import torch
     from amlp.configs import make_state
@@ -336,6 +380,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                          "roofline": ps["roofline"], "e2e": ps["e2e"]}
         line["tuned_over_plain"] = hs["value"] / ps["value"]
         line["gpu_launches"] += ps["gpu_launches"]
+    if rank == 0 and world == 1 and not args.no_serving:
+        line["serving"] = run_serving(dev)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         from amlp.configs import make_state as _ms
         t_cpu, sample, _ = cpu_step_sample(_ms(N_BODIES, "cube26", PHI, kT=KT, seed=SEED))
@@ -356,6 +402,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--method", choices=["both", "fd", "adjoint"], default="both")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--bodies", type=int, default=N_BODIES,
                     help="system size (the benchmark workload is 131072; smaller sizes are for profiling)")
     args = ap.parse_args()

@@ -99,6 +99,14 @@ typedef struct amlp_nvt {
     int nve;                  /* 1: no thermostat (thermo_fac = 1, xi_rot = 0) */
 } amlp_nvt;
 
+/* One system of a multi-system launch (serving): systems own contiguous body
+ * ranges; the per-body int32 array `rep` gives each body's system. */
+typedef struct amlp_replica {
+    float kT, n_dof, rn_dof, box;
+    int nve;
+    int pad[3];
+} amlp_replica;
+
 /* --------------------------------------------------------------- library */
 int amlp_version(void);
 const char *amlp_status_string(amlp_status s);
@@ -196,6 +204,32 @@ amlp_status amlp_nvt_step_one(float *d_pos, float *d_vel, const float *d_accel,
                               float *d_quat, float *d_angmom, const float *d_dp, const float *d_mass,
                               int n, const amlp_nvt *prm, amlp_thermostat *d_th,
                               void *d_ws, size_t ws_bytes, void *stream);
+
+/* --------------------------------------------------------------- many systems in one launch
+ * Serving path: the bodies of independent systems (different sizes, boxes,
+ * temperatures; one shape and one net per call) are concatenated, pair lists
+ * hold global body indices, and every kernel looks up the body's system.
+ * No reference counterpart (the reference runs one system per process).
+ * d_rp: nrep amlp_replica; d_th: nrep amlp_thermostat; d_pe: nrep doubles. */
+amlp_status amlp_multi_pair_filter(const float *d_pos, const int *d_rep, const amlp_replica *d_rp, double cutoff,
+                                   const int *d_vpairs, const long long *d_nverlet, long long cap_verlet,
+                                   int *d_pairs, long long *d_npairs, void *d_ws, size_t ws_bytes, void *stream);
+amlp_status amlp_multi_forces_adjoint(const float *d_pos, const float *d_quat, const int *d_rep,
+                                      const amlp_replica *d_rp, const int *d_pairs, const long long *d_npairs,
+                                      long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
+                                      float *d_F, float *d_T, double *d_pe, void *stream);
+/* prm supplies dt, tau and moi shared by the systems; the rest is per system. */
+amlp_status amlp_multi_nvt_init(const float *d_vel, const float *d_quat, const float *d_angmom, const float *d_mass,
+                                const int *d_rep, int n, int nrep, const amlp_nvt *prm, amlp_thermostat *d_th,
+                                void *stream);
+amlp_status amlp_multi_nvt_step_two(float *d_vel, float *d_accel, const float *d_F, const float *d_mass,
+                                    const float *d_quat, const float *d_T, float *d_angmom, float *d_dp,
+                                    const int *d_rep, int n, int nrep, const amlp_replica *d_rp, const amlp_nvt *prm,
+                                    amlp_thermostat *d_th, void *stream);
+amlp_status amlp_multi_nvt_step_one(float *d_pos, float *d_vel, const float *d_accel, float *d_quat,
+                                    float *d_angmom, const float *d_dp, const float *d_mass, const int *d_rep, int n,
+                                    const amlp_replica *d_rp, const amlp_nvt *prm, amlp_thermostat *d_th,
+                                    void *stream);
 
 #ifdef __cplusplus
 }
