@@ -86,6 +86,11 @@ SIGNATURES = {
     "amlp_fd_scatter": [_P, _LL, _P, ctypes.POINTER(Nep), _P, _P, _P, _P],
     "amlp_forces_fd": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
     "amlp_forces_adjoint": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
+    "amlp_adjoint_workspace_bytes": [_LL, _PSZ],
+    "amlp_forces_adjoint_wide": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P,
+                                 _P, _SZ, _P],
+    "amlp_multi_forces_adjoint_wide": [_P, _P, _P, _P, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp),
+                                       _P, _P, _P, _P, _SZ, _P],
     "amlp_device_error": [ctypes.POINTER(ctypes.c_uint), _I],
     "amlp_nvt_workspace_bytes": [_I, _PSZ],
     "amlp_nvt_init": [_P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _I, _P, _P, _SZ, _P],

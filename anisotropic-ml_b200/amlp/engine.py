@@ -70,6 +70,10 @@ class EnergyNet:
     def n_inputs(self) -> int:
         return self.dims[0]
 
+    @property
+    def max_hidden(self) -> int:
+        return max(self.dims[1:-1]) if len(self.dims) > 2 else 0
+
     @classmethod
     def from_state_dict(cls, sd, act: str = "relu", device="cuda"):
         """Weights stored with the reference's key names (``layer_first``,
@@ -185,6 +189,10 @@ class System:
         self.fpairs = torch.empty(self.cap, 2, dtype=torch.int32, device=self.device)
         self.f_ws = torch.empty(max(1, size_query("amlp_filter_workspace_bytes", self.cap)), dtype=torch.uint8,
                                 device=self.device)
+        self.adj_ws = None
+        if self.net.max_hidden > 64:  # nets wider than the fused adjoint kernel take the three-kernel path
+            self.adj_ws = torch.empty(size_query("amlp_adjoint_workspace_bytes", self.cap), dtype=torch.uint8,
+                                      device=self.device)
         self._graphs.clear()
 
     def build_nlist(self, check: bool = True) -> int:
@@ -231,7 +239,10 @@ class System:
         if method == "fd":
             call("amlp_forces_fd", *args)
         elif method == "adjoint":
-            call("amlp_forces_adjoint", *args)
+            if self.adj_ws is None:
+                call("amlp_forces_adjoint", *args)
+            else:
+                call("amlp_forces_adjoint_wide", *args[:-1], self.adj_ws.data_ptr(), self.adj_ws.numel(), args[-1])
         elif method == "fd_split":
             self._forces_split()
         else:

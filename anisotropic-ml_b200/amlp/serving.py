@@ -162,6 +162,10 @@ class _Bucket:
                                      for s in systems), dtype=torch.uint8, device=self.device)
         self.f_ws = torch.empty(size_query("amlp_filter_workspace_bytes", self.cap), dtype=torch.uint8,
                                 device=self.device)
+        self.adj_ws = None
+        if self.net.max_hidden > 64:  # wider nets take the three-kernel adjoint path
+            self.adj_ws = torch.empty(size_query("amlp_adjoint_workspace_bytes", self.cap), dtype=torch.uint8,
+                                      device=self.device)
         call("amlp_multi_nvt_init", self.vel.data_ptr(), self.quat.data_ptr(), self.angmom.data_ptr(),
              self.mass.data_ptr(), self.rep.data_ptr(), self.N, len(systems), ctypes.byref(self.prm),
              self.th.data_ptr(), _stream())
@@ -217,9 +221,13 @@ class _Bucket:
         call("amlp_multi_pair_filter", self.pos.data_ptr(), self.rep.data_ptr(), self.rp.data_ptr(),
              float(self.shape.cutoff), self.vpairs.data_ptr(), self.nv.data_ptr(), self.cap, self.fpairs.data_ptr(),
              self.nf.data_ptr(), self.f_ws.data_ptr(), self.f_ws.numel(), st)
-        call("amlp_multi_forces_adjoint", self.pos.data_ptr(), self.quat.data_ptr(), self.rep.data_ptr(),
-             self.rp.data_ptr(), self.fpairs.data_ptr(), self.nf.data_ptr(), self.cap, ctypes.byref(self.nep),
-             ctypes.byref(self.net.struct), self.F.data_ptr(), self.T.data_ptr(), self.pe.data_ptr(), st)
+        args = [self.pos.data_ptr(), self.quat.data_ptr(), self.rep.data_ptr(), self.rp.data_ptr(),
+                self.fpairs.data_ptr(), self.nf.data_ptr(), self.cap, ctypes.byref(self.nep),
+                ctypes.byref(self.net.struct), self.F.data_ptr(), self.T.data_ptr(), self.pe.data_ptr()]
+        if self.adj_ws is None:
+            call("amlp_multi_forces_adjoint", *args, st)
+        else:
+            call("amlp_multi_forces_adjoint_wide", *args, self.adj_ws.data_ptr(), self.adj_ws.numel(), st)
         call("amlp_multi_nvt_step_two", self.vel.data_ptr(), self.accel.data_ptr(), self.F.data_ptr(),
              self.mass.data_ptr(), self.quat.data_ptr(), self.T.data_ptr(), self.angmom.data_ptr(),
              self.dp.data_ptr(), self.rep.data_ptr(), self.N, len(self.systems), self.rp.data_ptr(),

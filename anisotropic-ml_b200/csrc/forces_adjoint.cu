@@ -710,6 +710,389 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     }
 }
 
+// ============================================================================
+// Wide nets (hidden widths up to 128): three kernels instead of one, since the
+// descriptor state and the resident weights of a 128-wide net do not share one
+// CTA's shared memory. g, dE/dg and the net output go through a caller
+// workspace:
+//   k_adj_desc<..., false>  descriptor forward per pair -> g (P x 48 fp32);
+//   k_mlp_grad              net forward + backward on the tensor cores per row,
+//                           weights staged layer by layer -> y and dE/dg;
+//   k_adj_desc<..., true>   recomputes the per-pair sums, descriptor backward,
+//                           forces, torques, scatter.
+// ============================================================================
+constexpr int kWideMax = 128;
+constexpr int kGP = 48;  // padded descriptor width in the workspace rows
+
+// Per-pair force/torque from the two halves' partial sums, scaled, clipped, then
+// scattered with runs of equal i summed in the warp (warps 0..3, lane = pair).
+template <bool MULTI>
+__device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int npts, int valid, float en_min,
+                                                float en_range, const float *y_rows, long long p0, float *F, float *T,
+                                                double *pe, const int *rep, double &pe_acc) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nd = 2 * npts;
+    if (tid < kAP) {
+        const int p = tid;
+        const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
+        const float *a0 = S.part + p * 12, *a1 = S.part + (kAP + p) * 12;
+        float Si[3], Sa[3], Xi[3], Xj[3], Pi[3] = {0, 0, 0}, Qj[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            Si[k] = a0[k] + a1[k];
+            Sa[k] = a0[3 + k] + a1[3 + k];
+            Xi[k] = a0[6 + k] + a1[6 + k];
+            Xj[k] = a0[9 + k] + a1[9 + k];
+        }
+        for (int a = 0; a < npts; ++a) {
+            Pi[0] += Ri[3 * a];
+            Pi[1] += Ri[3 * a + 1];
+            Pi[2] += Ri[3 * a + 2];
+            Qj[0] += Rj[3 * a];
+            Qj[1] += Rj[3 * a + 1];
+            Qj[2] += Rj[3 * a + 2];
+        }
+        const float inv_nd = 1.0f / (float)nd;
+        float Gm[3] = {Sa[0] * inv_nd, Sa[1] * inv_nd, Sa[2] * inv_nd};
+        float Fp[3], Ti[3], Tj[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Fp[k] = -(Si[k] - (float)npts * Gm[k]);
+        Ti[0] = -(Xi[0] - (Pi[1] * Gm[2] - Pi[2] * Gm[1]));
+        Ti[1] = -(Xi[1] - (Pi[2] * Gm[0] - Pi[0] * Gm[2]));
+        Ti[2] = -(Xi[2] - (Pi[0] * Gm[1] - Pi[1] * Gm[0]));
+        Tj[0] = -(Xj[0] - (Qj[1] * Gm[2] - Qj[2] * Gm[1]));
+        Tj[1] = -(Xj[1] - (Qj[2] * Gm[0] - Qj[0] * Gm[2]));
+        Tj[2] = -(Xj[2] - (Qj[0] * Gm[1] - Qj[1] * Gm[0]));
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            S.fd[9 * p + k] = clip100(Fp[k] * en_range);
+            S.fd[9 * p + 3 + k] = clip100(Ti[k] * en_range);
+            S.fd[9 * p + 6 + k] = clip100(Tj[k] * en_range);
+        }
+        if (!MULTI && p < valid) pe_acc += (double)en_min + (double)en_range * (double)y_rows[p0 + p];
+    }
+    __syncthreads();
+    if (warp < 4) {
+        const int q = warp * 32 + lane;
+        const bool ok = q < valid;
+        const int i = S.ij[2 * q], j = S.ij[2 * q + 1];
+        float v[6];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = ok ? S.fd[9 * q + k] : 0.f;
+            v[3 + k] = ok ? S.fd[9 * q + 3 + k] : 0.f;
+        }
+        if (ok) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                atomicAdd(F + 3 * j + k, -v[k]);
+                atomicAdd(T + 3 * j + k, S.fd[9 * q + 6 + k]);
+            }
+        }
+        int key = ok ? i : -1 - q;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int ko = __shfl_up_sync(0xffffffffu, key, o);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                float yv = __shfl_up_sync(0xffffffffu, v[k], o);
+                if (lane >= o && ko == key) v[k] += yv;
+            }
+        }
+        int kn = __shfl_down_sync(0xffffffffu, key, 1);
+        if (ok && (lane == 31 || kn != key)) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                atomicAdd(F + 3 * i + k, v[k]);
+                atomicAdd(T + 3 * i + k, v[3 + k]);
+            }
+        }
+        if (MULTI && pe) {
+            double e = ok ? (double)en_min + (double)en_range * (double)y_rows[p0 + q] : 0.0;
+            int rk = ok ? rep[i] : -1 - lane;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int ro = __shfl_up_sync(0xffffffffu, rk, o);
+                double yv = __shfl_up_sync(0xffffffffu, e, o);
+                if (lane >= o && ro == rk) e += yv;
+            }
+            int rn = __shfl_down_sync(0xffffffffu, rk, 1);
+            if (ok && (lane == 31 || rn != rk)) atomicAdd(pe + rk, e);
+        }
+    }
+    __syncthreads();
+}
+
+// Descriptor pass of the wide path: BWD = false writes g rows; BWD = true reads
+// dE/dg rows and the net outputs and produces forces, torques and energies.
+template <class Cfg, bool MULTI, bool BWD>
+__global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, const float *quat, float L,
+                                                          const int *pairs, const long long *d_np, long long cap,
+                                                          const float *pts, int npts, float inv_rc, float en_min,
+                                                          float en_range, float *g_rows, const float *dg_rows,
+                                                          const float *y_rows, float *F, float *T, double *pe,
+                                                          const int *rep, const amlp_replica *rp) {
+    constexpr int KC = Half<Cfg>::KC;
+    extern __shared__ __align__(128) char smem_raw[];
+    __shared__ double pe_s[kAThreads / 32];
+    const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
+    const int rs = 6 * npts + 1 - ((6 * npts) & 1);
+    const int nd = 2 * npts;
+    AdjShared S;
+    size_t off = 0;
+    S.R = reinterpret_cast<float *>(smem_raw);
+    off = align_up((size_t)kAP * rs * 4, 128);
+    S.g0 = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * kGP * 4;
+    S.g1 = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * kGP * 4;
+    S.t = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * 3 * 4;
+    S.part = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)2 * kAP * 12 * 4;
+    S.fd = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * 9 * 4;
+    S.ij = reinterpret_cast<int *>(smem_raw + off);
+    off += (size_t)kAP * 2 * 4;
+    S.pts = reinterpret_cast<float *>(smem_raw + off);
+    for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = pts[k];
+    __syncthreads();
+    const long long P = min(*d_np, cap);
+    const long long ntiles = (P + kAP - 1) / kAP;
+    double pe_acc = 0.0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long p0 = tile * kAP;
+        const int valid = (int)min((long long)kAP, P - p0);
+        for (int idx = tid; idx < kAP * nd; idx += kAThreads) {
+            int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
+            long long pr = min(p0 + q, P - 1);
+            float4 qq = load_quat(quat, pairs[2 * pr + body]);
+            float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
+            float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
+            dst[0] = r.x;
+            dst[1] = r.y;
+            dst[2] = r.z;
+        }
+        if (tid < kAP) {
+            long long pr = min(p0 + tid, P - 1);
+            int i = pairs[2 * pr], j = pairs[2 * pr + 1];
+            float dd;
+            float3 tt = min_image(pos, i, j, MULTI ? rp[rep[i]].box : L, &dd);
+            S.t[3 * tid] = tt.x;
+            S.t[3 * tid + 1] = tt.y;
+            S.t[3 * tid + 2] = tt.z;
+            S.ij[2 * tid] = i;
+            S.ij[2 * tid + 1] = j;
+        }
+        __syncthreads();
+        const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
+        const float3 t = make_float3(S.t[3 * p], S.t[3 * p + 1], S.t[3 * p + 2]);
+        float3 c = make_float3(0.f, 0.f, 0.f);
+        for (int a = 0; a < nd; ++a) {
+            float3 q = cloud1_point(Ri, Rj, t, npts, a);
+            c.x += q.x;
+            c.y += q.y;
+            c.z += q.z;
+        }
+        {
+            float inv = 1.0f / (float)nd;
+            c.x *= inv;
+            c.y *= inv;
+            c.z *= inv;
+        }
+        float A[Cfg::NA][KC];
+        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, A);
+        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGP, A);
+        __syncthreads();
+        if (!BWD) {
+            for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
+                int q = idx / kGP, d = idx - q * kGP;
+                if (q < valid) g_rows[(p0 + q) * kGP + d] = d < Cfg::D ? S.g0[idx] + S.g1[idx] : 0.f;
+            }
+            __syncthreads();
+            continue;
+        }
+        for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
+            int q = idx / kGP;
+            S.g0[idx] = q < valid ? dg_rows[p0 * kGP + idx] : 0.f;
+        }
+        __syncthreads();
+        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, S.part + p * 12, A);
+        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, S.part + (kAP + p) * 12, A);
+        __syncthreads();
+        adj_finish_tile<MULTI>(S, rs, npts, valid, en_min, en_range, y_rows, p0, F, T, pe, rep, pe_acc);
+    }
+    if (BWD && !MULTI && pe) {
+        double v = pe_acc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) pe_s[warp] = v;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int k = 0; k < kAThreads / 32; ++k) s += pe_s[k];
+            if (s != 0.0) atomicAdd(pe, s);
+        }
+    }
+}
+
+// Net forward and backward over rows of g on the tensor cores (bf16x3 splits,
+// fp32 TMEM accumulators). Weights are staged into shared memory one layer at
+// a time. Outputs per row: y = net(g) and dE/dg (kGP floats).
+__global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
+                                                          AdjNet net, const float *w, float *y_rows, float *dg_rows) {
+    extern __shared__ __align__(128) char smem_raw[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5;
+    const size_t tile_bytes = (size_t)2 * kAP * kWideMax * 2;  // hi + lo, 128 rows x 128
+    char *ops = smem_raw;                                         // two activation tiles
+    char *wbuf = smem_raw + 2 * tile_bytes;                       // one layer's weights, hi + lo
+    float *par = reinterpret_cast<float *>(wbuf + (size_t)2 * kWideMax * kWideMax * 2);
+    float *eps = par + net.par_total;
+    auto tile = [&](int k) { return ops + (k & 1) * tile_bytes; };
+    for (int L2 = 0; L2 < net.nh; ++L2) {
+        const int N = net.dims[L2 + 1], Np = net.nout[L2];
+        const float *b = w + net.woff[L2] + (size_t)N * net.dims[L2];
+        for (int n = tid; n < Np; n += kAThreads) par[net.bias_off[L2] + n] = n < N ? b[n] : 0.f;
+    }
+    {
+        const int K = net.dims[net.nh];
+        const float *Wl = w + net.woff[net.nh];
+        for (int k = tid; k < kWideMax; k += kAThreads) par[net.bias_off[net.nh] + k] = k < K ? Wl[k] : 0.f;
+        if (tid == 0) par[net.bias_off[net.nh] + kWideMax] = Wl[K];
+    }
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);
+    if (tid == 0) {
+        tc::mbar_init(&mbar, 1);
+        abort_flag = 0;
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = tmem_slot, bar = tc::smem_u32(&mbar);
+    uint32_t phase = 0;
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    const uint32_t bcol = 3u * kWideMax;
+    auto wait_mma = [&]() {
+        if (!tc::mbar_wait(bar, phase)) {
+            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
+            abort_flag = 1;
+        }
+        phase ^= 1u;
+        tc::fence_after();
+    };
+    // stage layer L's weights, bf16 hi/lo, K-major (rows = outputs)
+    auto stage = [&](int L2) {
+        const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
+        const float *W = w + net.woff[L2];
+        char *lo = wbuf + (size_t)Np * Kp * 2;
+        for (int idx = tid; idx < Np * Kp; idx += kAThreads) {
+            int n = idx / Kp, k = idx - n * Kp;
+            float v = (n < N && k < K) ? __ldg(W + (size_t)n * K + k) : 0.f;
+            __nv_bfloat16 a, bb;
+            tc::split_bf16(v, a, bb);
+            uint32_t o = tc::kmajor_offset(n, k, Kp);
+            *reinterpret_cast<__nv_bfloat16 *>(wbuf + o) = a;
+            *reinterpret_cast<__nv_bfloat16 *>(lo + o) = bb;
+        }
+        tc::fence_async_smem();
+    };
+    const long long P = min(*d_np, cap);
+    const long long ntiles = (P + kAP - 1) / kAP;
+    const int Kg = net.kin[0];
+    for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        const long long r0 = tl * kAP;
+        const int valid = (int)min((long long)kAP, P - r0);
+        for (int c0 = h * (Kg / 2); c0 < (h + 1) * (Kg / 2); c0 += 8) {
+            float v[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = p < valid ? g_rows[(r0 + p) * kGP + c0 + k] : 0.f;
+            store_split8(tile(0), Kg, p, c0, v);
+        }
+        for (int L2 = 0; L2 < net.nh; ++L2) {
+            const int Kp = net.kin[L2], Np = net.nout[L2];
+            stage(L2);
+            tc::fence_async_smem();
+            __syncthreads();
+            if (tid == 0 && !abort_flag) {
+                tc::fence_after();
+                mma3(tmem + (uint32_t)(L2 * kWideMax), tile(L2), Kp, wbuf, (size_t)Np * Kp * 2, Np, false, 256, 128,
+                     (uint32_t)Kp * 16);
+                tc::commit(bar);
+            }
+            wait_mma();
+            const bool last = L2 == net.nh - 1;
+            const float *bias = par + net.bias_off[L2];
+            const float *wl = par + net.bias_off[net.nh];
+            float esum = 0.f;
+            for (int c0 = h * (Np / 2); c0 < (h + 1) * (Np / 2); c0 += 8) {
+                float z[8], v[8];
+                tc::tmem_ld8(tmem + lane_base + (uint32_t)(L2 * kWideMax) + c0, z);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    float zz = z[k] + bias[c0 + k];
+                    if (last) {
+                        esum = fmaf(wl[c0 + k], act_f(net.act, zz), esum);
+                        v[k] = wl[c0 + k] * act_df(net.act, zz);
+                    } else {
+                        v[k] = act_f(net.act, zz);
+                    }
+                }
+                store_split8(tile(L2 + 1), Np, p, c0, v);
+            }
+            if (last) eps[h * kAP + p] = esum;
+            tc::fence_before();
+            tc::fence_async_smem();
+            __syncthreads();
+        }
+        if (tid < kAP && p < valid) y_rows[r0 + p] = eps[p] + eps[kAP + p] + par[net.bias_off[net.nh] + kWideMax];
+        for (int L2 = net.nh - 1; L2 >= 0; --L2) {
+            const int Kp = net.kin[L2], Np = net.nout[L2];
+            stage(L2);
+            tc::fence_async_smem();
+            __syncthreads();
+            if (tid == 0 && !abort_flag) {
+                tc::fence_after();
+                mma3(tmem + bcol, tile(L2 + 1), Np, wbuf, (size_t)Np * Kp * 2, Kp, true, 2 * Kp * 16,
+                     (uint32_t)Kp * 16, 128);
+                tc::commit(bar);
+            }
+            wait_mma();
+            if (L2 > 0) {
+                const float *bias = par + net.bias_off[L2 - 1];
+                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
+                    float dz[8], z[8], v[8];
+                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
+                    tc::tmem_ld8(tmem + lane_base + (uint32_t)((L2 - 1) * kWideMax) + c0, z);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_df(net.act, z[k] + bias[c0 + k]);
+                    store_split8(tile(L2), Kp, p, c0, v);
+                }
+            } else {
+                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
+                    float dg[8];
+                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dg);
+                    if (p < valid)
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) dg_rows[(r0 + p) * kGP + c0 + k] = dg[k];
+                }
+            }
+            tc::fence_before();
+            tc::fence_async_smem();
+            __syncthreads();
+        }
+        if (abort_flag) break;
+    }
+    if (abort_flag && tid == 0) tc::mbar_wait(bar, phase);
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after();
+        tc::tmem_dealloc(tmem, 512);
+    }
+}
+
 }  // namespace
 
 amlp_status check_nep(const amlp_nep *n);
@@ -798,6 +1181,101 @@ extern "C" amlp_status amlp_multi_forces_adjoint(const float *d_pos, const float
                                                  void *stream) {
     if (!d_rep || !d_rp) return AMLP_ERR_INVALID_ARG;
     return launch_adjoint(d_pos, d_quat, 0.f, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, d_rep, d_rp, stream);
+}
+
+
+static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
+    const int nh = mlp->n_layers - 1;
+    if (nh < 1 || nh > kMaxHidden) return AMLP_ERR_UNSUPPORTED;
+    *net = AdjNet{};
+    net->nh = nh;
+    net->act = mlp->act;
+    long long off = 0;
+    int par = 0;
+    for (int k = 0; k <= mlp->n_layers; ++k) net->dims[k] = mlp->dims[k];
+    for (int k = 0; k <= nh; ++k) {
+        net->woff[k] = off;
+        off += (long long)mlp->dims[k + 1] * mlp->dims[k] + mlp->dims[k + 1];
+    }
+    for (int k = 0; k < nh; ++k) {
+        if (mlp->dims[k + 1] > kWideMax) return AMLP_ERR_UNSUPPORTED;
+        net->kin[k] = k == 0 ? kGP : net->nout[k - 1];
+        net->nout[k] = (mlp->dims[k + 1] + 15) / 16 * 16;
+        net->bias_off[k] = par;
+        par += net->nout[k];
+    }
+    net->bias_off[nh] = par;
+    par += kWideMax + 4;
+    net->par_total = par;
+    return AMLP_OK;
+}
+
+extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes) {
+    if (cap < 0 || !bytes) return AMLP_ERR_INVALID_ARG;
+    *bytes = align_up((size_t)cap * kGP * 4) * 2 + align_up((size_t)cap * 4) + 256;
+    return AMLP_OK;
+}
+
+static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                       const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                       const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe, const int *d_rep,
+                                       const amlp_replica *d_rp, void *d_ws, size_t ws_bytes, void *stream) {
+    amlp_status st = check_nep(nep);
+    if (st) return st;
+    const int D = nep_D(nep);
+    if ((st = check_mlp(mlp, D))) return st;
+    if (!d_pos || !d_quat || !d_npairs || !d_F || !d_T || cap < 0 || (cap > 0 && !d_pairs)) return AMLP_ERR_INVALID_ARG;
+    if (cap == 0) return AMLP_OK;
+    if (hyper_kind(nep) != 1 || D > kGP) return AMLP_ERR_UNSUPPORTED;
+    size_t need;
+    amlp_adjoint_workspace_bytes(cap, &need);
+    if (!d_ws || ws_bytes < need) return AMLP_ERR_WORKSPACE;
+    AdjNet net;
+    if ((st = wide_net(mlp, &net))) return st;
+    Carver c(d_ws, ws_bytes);
+    float *g_rows = c.take<float>((size_t)cap * kGP);
+    float *dg_rows = c.take<float>((size_t)cap * kGP);
+    float *y_rows = c.take<float>((size_t)cap);
+    const int npts = nep->npts;
+    const int rs = 6 * npts + 1 - ((6 * npts) & 1);
+    const size_t smem_desc = align_up((size_t)kAP * rs * 4, 128) + (size_t)kAP * kGP * 4 * 2 + (size_t)kAP * 3 * 4 +
+                             (size_t)2 * kAP * 12 * 4 + (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4;
+    const size_t smem_mlp = (size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
+                            (size_t)(net.par_total + 2 * kAP) * 4;
+    if (smem_desc > 220 * 1024 || smem_mlp > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
+    using Cfg = NepCfg<10, 8, 4, 12>;
+    cudaStream_t s = as_stream(stream);
+    const float inv_rc = 1.0f / nep->nep_cutoff, rng = nep->en_max - nep->en_min;
+    const bool multi = d_rep != nullptr;
+    auto fwd = multi ? k_adj_desc<Cfg, true, false> : k_adj_desc<Cfg, false, false>;
+    auto bwd = multi ? k_adj_desc<Cfg, true, true> : k_adj_desc<Cfg, false, true>;
+    AMLP_CHECK_CUDA(cudaFuncSetAttribute(fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
+    AMLP_CHECK_CUDA(cudaFuncSetAttribute(bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
+    AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mlp));
+    fwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
+                                             nep->en_min, rng, g_rows, nullptr, nullptr, d_F, d_T, d_pe, d_rep, d_rp);
+    k_mlp_grad<<<kNumSM, kAThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, y_rows, dg_rows);
+    bwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
+                                             nep->en_min, rng, nullptr, dg_rows, y_rows, d_F, d_T, d_pe, d_rep, d_rp);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_forces_adjoint_wide(const float *d_pos, const float *d_quat, float box,
+                                                const int *d_pairs, const long long *d_npairs, long long cap,
+                                                const amlp_nep *nep, const amlp_mlp *mlp, float *d_F, float *d_T,
+                                                double *d_pe, void *d_ws, size_t ws_bytes, void *stream) {
+    return launch_adjoint_wide(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, nullptr,
+                               nullptr, d_ws, ws_bytes, stream);
+}
+
+extern "C" amlp_status amlp_multi_forces_adjoint_wide(const float *d_pos, const float *d_quat, const int *d_rep,
+                                                      const amlp_replica *d_rp, const int *d_pairs,
+                                                      const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                                      const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe,
+                                                      void *d_ws, size_t ws_bytes, void *stream) {
+    if (!d_rep || !d_rp) return AMLP_ERR_INVALID_ARG;
+    return launch_adjoint_wide(d_pos, d_quat, 0.f, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, d_rep, d_rp,
+                               d_ws, ws_bytes, stream);
 }
 
 extern "C" amlp_status amlp_device_error(unsigned int *flags, int clear) {

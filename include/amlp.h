@@ -180,6 +180,17 @@ amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_quat, float b
                                 const amlp_nep *nep, const amlp_mlp *mlp,
                                 float *d_F, float *d_T, double *d_pe, void *stream);
 
+/* Same forces for nets with hidden widths up to 128 (amlp_forces_adjoint takes
+ * widths up to 64): the descriptor forward, the net forward/backward on the
+ * tensor cores (weights staged layer by layer) and the descriptor backward run
+ * as three kernels that pass g, dE/dg and the net output through a workspace
+ * of amlp_adjoint_workspace_bytes(cap). */
+amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes);
+amlp_status amlp_forces_adjoint_wide(const float *d_pos, const float *d_quat, float box,
+                                     const int *d_pairs, const long long *d_npairs, long long cap,
+                                     const amlp_nep *nep, const amlp_mlp *mlp,
+                                     float *d_F, float *d_T, double *d_pe, void *d_ws, size_t ws_bytes, void *stream);
+
 /* Sticky error bits raised by device code since the last clear (1 = a bounded
  * wait for tensor-core completion gave up; the kernel then stops early). */
 amlp_status amlp_device_error(unsigned int *flags, int clear);
@@ -218,6 +229,11 @@ amlp_status amlp_multi_forces_adjoint(const float *d_pos, const float *d_quat, c
                                       const amlp_replica *d_rp, const int *d_pairs, const long long *d_npairs,
                                       long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
                                       float *d_F, float *d_T, double *d_pe, void *stream);
+amlp_status amlp_multi_forces_adjoint_wide(const float *d_pos, const float *d_quat, const int *d_rep,
+                                           const amlp_replica *d_rp, const int *d_pairs, const long long *d_npairs,
+                                           long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
+                                           float *d_F, float *d_T, double *d_pe, void *d_ws, size_t ws_bytes,
+                                           void *stream);
 /* prm supplies dt, tau and moi shared by the systems; the rest is per system. */
 amlp_status amlp_multi_nvt_init(const float *d_vel, const float *d_quat, const float *d_angmom, const float *d_mass,
                                 const int *d_rep, int n, int nrep, const amlp_nvt *prm, amlp_thermostat *d_th,

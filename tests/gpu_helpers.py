@@ -110,6 +110,10 @@ def fused_forces(pos, quat, L, pairs, shape, hypers, layers, act, method="amlp_f
         pr[:P] = torch.tensor(np.asarray(pairs, np.int32).reshape(-1, 2), device=DEV)
     npairs = torch.tensor([P], dtype=torch.int64, device=DEV)
     pos_t, quat_t = t32(pos), t32(quat)
-    call(method, pos_t.data_ptr(), quat_t.data_ptr(), float(L), pr.data_ptr(), npairs.data_ptr(), max(P, 1),
-         ctypes.byref(n), ctypes.byref(net.struct), F.data_ptr(), T.data_ptr(), pe.data_ptr(), stream())
+    args = [pos_t.data_ptr(), quat_t.data_ptr(), float(L), pr.data_ptr(), npairs.data_ptr(), max(P, 1),
+            ctypes.byref(n), ctypes.byref(net.struct), F.data_ptr(), T.data_ptr(), pe.data_ptr()]
+    if method == "amlp_forces_adjoint_wide":
+        ws = torch.empty(size_query("amlp_adjoint_workspace_bytes", max(P, 1)), dtype=torch.uint8, device=DEV)
+        args += [ws.data_ptr(), ws.numel()]
+    call(method, *args, stream())
     return F.cpu().numpy(), T.cpu().numpy(), float(pe.item())

@@ -341,7 +341,7 @@ def test_system_run_graph_rebuilds_and_matches_eager():
 
 
 # ----------------------------------------------------------------------------- adjoint
-def _adjoint_case(shape_name, n, phi, seed, widths, act, pair_limit=None):
+def _adjoint_case(shape_name, n, phi, seed, widths, act, pair_limit=None, method="amlp_forces_adjoint"):
     from amlp.engine import EnergyNet
     from oracle import adjoint
     s = make_state(n, shape_name, phi, seed=seed)
@@ -351,8 +351,7 @@ def _adjoint_case(shape_name, n, phi, seed, widths, act, pair_limit=None):
     if pair_limit:
         pairs = pairs[:pair_limit]
     net = EnergyNet.xavier(47, widths, act, seed=seed + 10, device="cpu")
-    F, T, pe = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, (10, 8, 4), net.layers, act,
-                               method="amlp_forces_adjoint")
+    F, T, pe = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, (10, 8, 4), net.layers, act, method=method)
     from amlp import _lib
     assert _lib.device_error() == 0
     ref = adjoint.exact_pair_forces(s.pos, s.orient, pairs, s.L, shape, (10, 8, 4), net.layers, act)
@@ -379,3 +378,16 @@ def test_adjoint_partial_tile_and_single_pair():
     np.testing.assert_allclose(F, ref["forces"], atol=2e-3 * max(1.0, np.abs(ref["forces"]).max()))
     F, T, pe, ref = _adjoint_case("cube26", 300, 0.45, 3, (64, 64), "tanh", pair_limit=200)
     assert np.linalg.norm(F - ref["forces"]) / np.linalg.norm(ref["forces"]) <= 1e-3
+
+
+@pytest.mark.parametrize("shape_name,phi,widths,act", [("tetra16", 0.40, (128, 128, 128), "silu"),
+                                                       ("cyl24", 0.35, (128, 128), "silu"),
+                                                       ("cube26", 0.45, (64, 64), "tanh")])
+def test_adjoint_wide_nets_vs_fp64_exact(shape_name, phi, widths, act):
+    """The three-kernel path for nets up to 128 wide (the differentiation and
+    precision configurations' nets), same 1e-3 bar."""
+    F, T, pe, ref = _adjoint_case(shape_name, 500, phi, 9, widths, act, method="amlp_forces_adjoint_wide")
+    for got, want in ((F, ref["forces"]), (T, ref["torques"])):
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert err <= 1e-3, err
+    assert abs(pe - ref["E"].sum()) <= 1e-4 * max(1.0, np.abs(ref["E"]).sum())
