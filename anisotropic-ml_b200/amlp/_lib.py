@@ -83,6 +83,7 @@ SIGNATURES = {
     "amlp_pair_filter": [_P, _F, _D, _P, _P, _LL, _P, _P, _P, _SZ, _P],
     "amlp_descriptors": [_P, _P, _F, _P, _LL, ctypes.POINTER(Nep), _P, _P],
     "amlp_mlp_energy": [_P, _LL, ctypes.POINTER(Mlp), _P, _P],
+    "amlp_mlp_loss_grad": [_P, _P, _LL, ctypes.POINTER(Mlp), _P, _P, _P],
     "amlp_fd_scatter": [_P, _LL, _P, ctypes.POINTER(Nep), _P, _P, _P, _P],
     "amlp_forces_fd": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
     "amlp_forces_adjoint": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
@@ -91,6 +92,10 @@ SIGNATURES = {
                                  _P, _SZ, _P],
     "amlp_multi_forces_adjoint_wide": [_P, _P, _P, _P, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp),
                                        _P, _P, _P, _P, _SZ, _P],
+    "amlp_pair_descriptors": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), _P, _I, _P],
+    "amlp_pair_energy_vjp": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _I, _P, _P,
+                             _P, _P, _SZ, _P],
+    "amlp_mlp_backward": [_P, _P, _LL, ctypes.POINTER(Mlp), _P, _P],
     "amlp_device_error": [ctypes.POINTER(ctypes.c_uint), _I],
     "amlp_nvt_workspace_bytes": [_I, _PSZ],
     "amlp_nvt_init": [_P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _I, _P, _P, _SZ, _P],

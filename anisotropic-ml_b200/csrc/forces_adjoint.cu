@@ -724,12 +724,13 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
 constexpr int kWideMax = 128;
 constexpr int kGP = 48;  // padded descriptor width in the workspace rows
 
-// Per-pair force/torque from the two halves' partial sums, scaled, clipped, then
-// scattered with runs of equal i summed in the warp (warps 0..3, lane = pair).
+// Per-pair force/torque from the two halves' partial sums, scaled, clipped
+// (unless clip == 0), then scattered with runs of equal i summed in the warp
+// (warps 0..3, lane = pair).
 template <bool MULTI>
 __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int npts, int valid, float en_min,
                                                 float en_range, const float *y_rows, long long p0, float *F, float *T,
-                                                double *pe, const int *rep, double &pe_acc) {
+                                                double *pe, const int *rep, double &pe_acc, int clip) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nd = 2 * npts;
     if (tid < kAP) {
@@ -765,9 +766,10 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
         Tj[2] = -(Xj[2] - (Qj[0] * Gm[1] - Qj[1] * Gm[0]));
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            S.fd[9 * p + k] = clip100(Fp[k] * en_range);
-            S.fd[9 * p + 3 + k] = clip100(Ti[k] * en_range);
-            S.fd[9 * p + 6 + k] = clip100(Tj[k] * en_range);
+            float f = Fp[k] * en_range, ti = Ti[k] * en_range, tj = Tj[k] * en_range;
+            S.fd[9 * p + k] = clip ? clip100(f) : f;
+            S.fd[9 * p + 3 + k] = clip ? clip100(ti) : ti;
+            S.fd[9 * p + 6 + k] = clip ? clip100(tj) : tj;
         }
         if (!MULTI && p < valid) pe_acc += (double)en_min + (double)en_range * (double)y_rows[p0 + p];
     }
@@ -823,15 +825,19 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
     __syncthreads();
 }
 
-// Descriptor pass of the wide path: BWD = false writes g rows; BWD = true reads
-// dE/dg rows and the net outputs and produces forces, torques and energies.
+// Descriptor pass of the wide path: BWD = false writes g rows (row stride
+// g_ld >= D, zero padded); BWD = true reads dE/dg rows (stride kGP) and the net
+// outputs and produces forces, torques and energies. wt (BWD, may be null)
+// weights pair p's dE/dg by wt[p] (a vector-Jacobian product); clip = 0 turns
+// the +-100 clip of the per-pair forces and torques off.
 template <class Cfg, bool MULTI, bool BWD>
 __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, const float *quat, float L,
                                                           const int *pairs, const long long *d_np, long long cap,
                                                           const float *pts, int npts, float inv_rc, float en_min,
-                                                          float en_range, float *g_rows, const float *dg_rows,
-                                                          const float *y_rows, float *F, float *T, double *pe,
-                                                          const int *rep, const amlp_replica *rp) {
+                                                          float en_range, float *g_rows, int g_ld,
+                                                          const float *dg_rows, const float *y_rows, const float *wt,
+                                                          int clip, float *F, float *T, double *pe, const int *rep,
+                                                          const amlp_replica *rp) {
     constexpr int KC = Half<Cfg>::KC;
     extern __shared__ __align__(128) char smem_raw[];
     __shared__ double pe_s[kAThreads / 32];
@@ -905,22 +911,23 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
         else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGP, A);
         __syncthreads();
         if (!BWD) {
-            for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
-                int q = idx / kGP, d = idx - q * kGP;
-                if (q < valid) g_rows[(p0 + q) * kGP + d] = d < Cfg::D ? S.g0[idx] + S.g1[idx] : 0.f;
+            for (int idx = tid; idx < kAP * g_ld; idx += kAThreads) {
+                int q = idx / g_ld, d = idx - q * g_ld;
+                if (q < valid)
+                    g_rows[(p0 + q) * g_ld + d] = d < Cfg::D ? S.g0[q * kGP + d] + S.g1[q * kGP + d] : 0.f;
             }
             __syncthreads();
             continue;
         }
         for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
             int q = idx / kGP;
-            S.g0[idx] = q < valid ? dg_rows[p0 * kGP + idx] : 0.f;
+            S.g0[idx] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
         }
         __syncthreads();
         if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, S.part + p * 12, A);
         else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, S.part + (kAP + p) * 12, A);
         __syncthreads();
-        adj_finish_tile<MULTI>(S, rs, npts, valid, en_min, en_range, y_rows, p0, F, T, pe, rep, pe_acc);
+        adj_finish_tile<MULTI>(S, rs, npts, valid, en_min, en_range, y_rows, p0, F, T, pe, rep, pe_acc, clip);
     }
     if (BWD && !MULTI && pe) {
         double v = pe_acc;
@@ -1216,17 +1223,31 @@ extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes
     return AMLP_OK;
 }
 
-static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
-                                       const long long *d_npairs, long long cap, const amlp_nep *nep,
-                                       const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe, const int *d_rep,
-                                       const amlp_replica *d_rp, void *d_ws, size_t ws_bytes, void *stream) {
+static size_t wide_desc_smem(int npts) {
+    const int rs = 6 * npts + 1 - ((6 * npts) & 1);
+    return align_up((size_t)kAP * rs * 4, 128) + (size_t)kAP * kGP * 4 * 2 + (size_t)kAP * 3 * 4 +
+           (size_t)2 * kAP * 12 * 4 + (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4;
+}
+
+static amlp_status check_pair_args(const float *d_pos, const float *d_quat, const int *d_pairs,
+                                   const long long *d_npairs, long long cap, const amlp_nep *nep) {
     amlp_status st = check_nep(nep);
     if (st) return st;
-    const int D = nep_D(nep);
-    if ((st = check_mlp(mlp, D))) return st;
-    if (!d_pos || !d_quat || !d_npairs || !d_F || !d_T || cap < 0 || (cap > 0 && !d_pairs)) return AMLP_ERR_INVALID_ARG;
+    if (!d_pos || !d_quat || !d_npairs || cap < 0 || (cap > 0 && !d_pairs)) return AMLP_ERR_INVALID_ARG;
+    if (hyper_kind(nep) != 1 || nep_D(nep) > kGP) return AMLP_ERR_UNSUPPORTED;
+    return AMLP_OK;
+}
+
+static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                       const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                       const amlp_mlp *mlp, const float *d_wt, int clip, float *d_F, float *d_T,
+                                       double *d_pe, const int *d_rep, const amlp_replica *d_rp, void *d_ws,
+                                       size_t ws_bytes, void *stream) {
+    amlp_status st = check_pair_args(d_pos, d_quat, d_pairs, d_npairs, cap, nep);
+    if (st) return st;
+    if ((st = check_mlp(mlp, nep_D(nep)))) return st;
+    if (!d_F || !d_T) return AMLP_ERR_INVALID_ARG;
     if (cap == 0) return AMLP_OK;
-    if (hyper_kind(nep) != 1 || D > kGP) return AMLP_ERR_UNSUPPORTED;
     size_t need;
     amlp_adjoint_workspace_bytes(cap, &need);
     if (!d_ws || ws_bytes < need) return AMLP_ERR_WORKSPACE;
@@ -1237,9 +1258,7 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     float *dg_rows = c.take<float>((size_t)cap * kGP);
     float *y_rows = c.take<float>((size_t)cap);
     const int npts = nep->npts;
-    const int rs = 6 * npts + 1 - ((6 * npts) & 1);
-    const size_t smem_desc = align_up((size_t)kAP * rs * 4, 128) + (size_t)kAP * kGP * 4 * 2 + (size_t)kAP * 3 * 4 +
-                             (size_t)2 * kAP * 12 * 4 + (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4;
+    const size_t smem_desc = wide_desc_smem(npts);
     const size_t smem_mlp = (size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
                             (size_t)(net.par_total + 2 * kAP) * 4;
     if (smem_desc > 220 * 1024 || smem_mlp > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
@@ -1253,10 +1272,12 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mlp));
     fwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
-                                             nep->en_min, rng, g_rows, nullptr, nullptr, d_F, d_T, d_pe, d_rep, d_rp);
+                                             nep->en_min, rng, g_rows, kGP, nullptr, nullptr, nullptr, clip, d_F,
+                                             d_T, d_pe, d_rep, d_rp);
     k_mlp_grad<<<kNumSM, kAThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, y_rows, dg_rows);
     bwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
-                                             nep->en_min, rng, nullptr, dg_rows, y_rows, d_F, d_T, d_pe, d_rep, d_rp);
+                                             nep->en_min, rng, nullptr, kGP, dg_rows, y_rows, d_wt, clip, d_F, d_T,
+                                             d_pe, d_rep, d_rp);
     return check_launch();
 }
 
@@ -1264,8 +1285,8 @@ extern "C" amlp_status amlp_forces_adjoint_wide(const float *d_pos, const float 
                                                 const int *d_pairs, const long long *d_npairs, long long cap,
                                                 const amlp_nep *nep, const amlp_mlp *mlp, float *d_F, float *d_T,
                                                 double *d_pe, void *d_ws, size_t ws_bytes, void *stream) {
-    return launch_adjoint_wide(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, nullptr,
-                               nullptr, d_ws, ws_bytes, stream);
+    return launch_adjoint_wide(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, nullptr, 1, d_F, d_T, d_pe,
+                               nullptr, nullptr, d_ws, ws_bytes, stream);
 }
 
 extern "C" amlp_status amlp_multi_forces_adjoint_wide(const float *d_pos, const float *d_quat, const int *d_rep,
@@ -1274,8 +1295,35 @@ extern "C" amlp_status amlp_multi_forces_adjoint_wide(const float *d_pos, const 
                                                       const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe,
                                                       void *d_ws, size_t ws_bytes, void *stream) {
     if (!d_rep || !d_rp) return AMLP_ERR_INVALID_ARG;
-    return launch_adjoint_wide(d_pos, d_quat, 0.f, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, d_rep, d_rp,
-                               d_ws, ws_bytes, stream);
+    return launch_adjoint_wide(d_pos, d_quat, 0.f, d_pairs, d_npairs, cap, nep, mlp, nullptr, 1, d_F, d_T, d_pe,
+                               d_rep, d_rp, d_ws, ws_bytes, stream);
+}
+
+extern "C" amlp_status amlp_pair_energy_vjp(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                            const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                            const amlp_mlp *mlp, const float *d_wt, int clip, float *d_F,
+                                            float *d_T, double *d_pe, void *d_ws, size_t ws_bytes, void *stream) {
+    return launch_adjoint_wide(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_wt, clip ? 1 : 0, d_F, d_T,
+                               d_pe, nullptr, nullptr, d_ws, ws_bytes, stream);
+}
+
+extern "C" amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                             const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                             float *d_g, int ld_g, void *stream) {
+    amlp_status st = check_pair_args(d_pos, d_quat, d_pairs, d_npairs, cap, nep);
+    if (st) return st;
+    if (!d_g || ld_g < nep_D(nep)) return AMLP_ERR_INVALID_ARG;
+    if (cap == 0) return AMLP_OK;
+    const size_t smem = wide_desc_smem(nep->npts);
+    if (smem > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
+    using Cfg = NepCfg<10, 8, 4, 12>;
+    auto fwd = k_adj_desc<Cfg, false, false>;
+    AMLP_CHECK_CUDA(cudaFuncSetAttribute(fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fwd<<<kNumSM, kAThreads, smem, as_stream(stream)>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts,
+                                                        nep->npts, 1.0f / nep->nep_cutoff, nep->en_min,
+                                                        nep->en_max - nep->en_min, d_g, ld_g, nullptr, nullptr,
+                                                        nullptr, 1, nullptr, nullptr, nullptr, nullptr, nullptr);
+    return check_launch();
 }
 
 extern "C" amlp_status amlp_device_error(unsigned int *flags, int clear) {

@@ -25,6 +25,7 @@
  *   amlp_descriptors      DescriptorGenerator.generate_nep_descriptors  DescriptorGenerator.py:136-161
  *                         (pos_to_pts :163-218, apply_dx_dteta :220-255, pts_to_nep_descriptors :296-442)
  *   amlp_mlp_energy       ForceEvaluator.evaluate_gradients (net forward)  ForceEvaluator.py:80-83
+ *   amlp_mlp_loss_grad    FFNN.train_step loss.backward (MSE on normalised energies)  05/FFNN.py:95-106
  *   amlp_fd_scatter       ForceEvaluator.evaluate_gradients (differences) + evaluate_forces_torques
  *                         ForceEvaluator.py:86-146
  *   amlp_forces_fd        Sim.step lines 261-266 (descriptors + evaluate_interactions), fused
@@ -156,6 +157,15 @@ amlp_status amlp_descriptors(const float *d_pos, const float *d_quat, float box,
 amlp_status amlp_mlp_energy(const float *d_g, long long rows, const amlp_mlp *mlp,
                             float *d_e, void *stream);
 
+/* Gradient of the training loss L = (1/rows) sum_r (net(d_g[r]) - d_y[r])^2
+ * (torch.nn.MSELoss of 05/FFNN.py:95-106; d_y holds the normalised energies of
+ * 05/FFNN.py:59-63) with respect to every weight and bias of the net, in the
+ * packed layout of amlp_mlp.d_w (per layer W (out x in) then b). d_grad is
+ * accumulated into (zero it first); d_loss (may be NULL) accumulates L in FP64.
+ * FP32, layer widths up to 256. */
+amlp_status amlp_mlp_loss_grad(const float *d_g, const float *d_y, long long rows, const amlp_mlp *mlp,
+                               float *d_grad, double *d_loss, void *stream);
+
 /* Finite differences, scaling, clip to [-100,100] and scatter of
  * ForceEvaluator.py:86-146. d_F, d_T (N,3) are accumulated into (zero them
  * first). d_pe (may be NULL) accumulates sum_p (en_min + (en_max-en_min) e0_p). */
@@ -190,6 +200,29 @@ amlp_status amlp_forces_adjoint_wide(const float *d_pos, const float *d_quat, fl
                                      const int *d_pairs, const long long *d_npairs, long long cap,
                                      const amlp_nep *nep, const amlp_mlp *mlp,
                                      float *d_F, float *d_T, double *d_pe, void *d_ws, size_t ws_bytes, void *stream);
+
+/* ------------------------------------------------- differentiation (no reference counterpart)
+ * The pieces of a torch.autograd.Function over the pair energies
+ * E_p = en_min + (en_max - en_min) net(g_p):
+ *   amlp_pair_descriptors  g_p of the unperturbed pair (row p at d_g + p*ld_g,
+ *                          ld_g >= D, columns D..ld_g-1 set to zero);
+ *   amlp_pair_energy_vjp   F = -sum_p w_p dE_p/dx, T = -sum_p w_p dE_p/dtheta
+ *                          (world-frame rotation about each body's centre),
+ *                          accumulated into d_F, d_T; w_p = d_wt[p] (NULL: 1);
+ *                          clip = 1 clips each pair's terms to [-100,100] as the
+ *                          force path does, clip = 0 gives the exact product.
+ *                          Same kernels and workspace as amlp_forces_adjoint_wide;
+ *   amlp_mlp_backward      d_grad += sum_r d_dy[r] d net(d_g[r]) / d theta over
+ *                          every weight and bias (packed like amlp_mlp.d_w). */
+amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                  const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                  float *d_g, int ld_g, void *stream);
+amlp_status amlp_pair_energy_vjp(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                 const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                 const amlp_mlp *mlp, const float *d_wt, int clip, float *d_F, float *d_T,
+                                 double *d_pe, void *d_ws, size_t ws_bytes, void *stream);
+amlp_status amlp_mlp_backward(const float *d_g, const float *d_dy, long long rows, const amlp_mlp *mlp,
+                              float *d_grad, void *stream);
 
 /* Sticky error bits raised by device code since the last clear (1 = a bounded
  * wait for tensor-core completion gave up; the kernel then stops early). */

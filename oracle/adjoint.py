@@ -89,3 +89,78 @@ def exact_pair_forces(pos, quat, pairs, L, shape, hypers, layers, act, chunk=512
     N = len(pos)
     Fn, Tn = nep.scatter(pairs, F, Ti, Tj, N, np.float64)
     return dict(F_pair=F, T_i=Ti, T_j=Tj, forces=Fn, torques=Tn, E=E, pairs=pairs)
+
+
+def _qmul(a, b):
+    w = a[..., 0] * b[..., 0] - np.sum(a[..., 1:] * b[..., 1:], axis=-1)
+    v = a[..., :1] * b[..., 1:] + b[..., :1] * a[..., 1:] + np.cross(a[..., 1:], b[..., 1:])
+    return np.concatenate([w[..., None], v], axis=-1)
+
+
+def _pair_energies64(pos_i, pos_j, q_i, q_j, L, shape, hypers, layers, act, chunk=4096):
+    """FP64 energies E = en_min + en_range * net(g) of pairs given per row by
+    both bodies' centres and orientations (minimum image in a cubic box L)."""
+    nrad, nang, lmax = (int(h) for h in hypers[:3])
+    d = pos_j - pos_i
+    t = d - L * np.round(d / L)
+    R = len(t)
+    pos2 = np.zeros((2 * R, 3))
+    pos2[1::2] = t
+    quat2 = np.empty((2 * R, 4))
+    quat2[0::2], quat2[1::2] = q_i, q_j
+    pr = np.arange(2 * R, dtype=np.int64).reshape(-1, 2)
+    c1, _ = nep.pair_clouds(quat2, pr, t, shape["pts"], np.float64)
+    rng = shape["en_max"] - shape["en_min"]
+    out = []
+    with torch.no_grad():
+        for s in range(0, R, chunk):
+            p = torch.tensor(c1[s:s + chunk], dtype=torch.float64)
+            y = pair_energy_net(descriptor_torch(p, nrad, nang, lmax, float(shape["nep_cutoff"])), layers, act)
+            out.append(shape["en_min"] + rng * y.numpy())
+    return np.concatenate(out) if out else np.zeros(0)
+
+
+def central_difference_forces(pos, quat, pairs, L, shape, hypers, layers, act, bodies, h=1e-4):
+    """Forces and torques on ``bodies`` by FP64 central differences of the summed
+    energy of their pairs: F_k = -(U(x + h e_k) - U(x - h e_k)) / 2h and
+    T_k = -(U(R_k(h) q) - U(R_k(-h) q)) / 2h with R_k(a) the world-frame
+    rotation by angle a about axis k applied on the left of the body's
+    quaternion (rotation about the body's centre). Unclipped. The pair set is
+    held fixed (the filtered list at the unperturbed positions)."""
+    pos = np.asarray(pos, np.float64)
+    quat = np.asarray(quat, np.float64)
+    pairs = np.asarray(pairs, np.int64).reshape(-1, 2)
+    bodies = np.asarray(bodies, np.int64)
+    eye = np.eye(3)
+    dq = []
+    for k in range(3):
+        for sgn in (1.0, -1.0):
+            dq.append(np.concatenate([[np.cos(sgn * h / 2)], np.sin(sgn * h / 2) * eye[k]]))
+    rows_i, rows_j, rows_qi, rows_qj, owner, kind = [], [], [], [], [], []
+    for n, b in enumerate(bodies):
+        sel = np.nonzero((pairs[:, 0] == b) | (pairs[:, 1] == b))[0]
+        for m in range(12):
+            pi, pj = pos[pairs[sel, 0]].copy(), pos[pairs[sel, 1]].copy()
+            qi, qj = quat[pairs[sel, 0]].copy(), quat[pairs[sel, 1]].copy()
+            is_i = pairs[sel, 0] == b
+            if m < 6:
+                delta = (1.0 if m % 2 == 0 else -1.0) * h * eye[m // 2]
+                pi[is_i] += delta
+                pj[~is_i] += delta
+            else:
+                r = dq[m - 6]
+                qi[is_i] = _qmul(r, qi[is_i])
+                qj[~is_i] = _qmul(r, qj[~is_i])
+            rows_i.append(pi)
+            rows_j.append(pj)
+            rows_qi.append(qi)
+            rows_qj.append(qj)
+            owner.append(np.full(len(sel), n))
+            kind.append(np.full(len(sel), m))
+    E = _pair_energies64(np.concatenate(rows_i), np.concatenate(rows_j), np.concatenate(rows_qi),
+                         np.concatenate(rows_qj), L, shape, hypers, layers, act)
+    U = np.zeros((len(bodies), 12))
+    np.add.at(U, (np.concatenate(owner), np.concatenate(kind)), E)
+    F = -(U[:, 0:6:2] - U[:, 1:6:2]) / (2 * h)
+    T = -(U[:, 6:12:2] - U[:, 7:12:2]) / (2 * h)
+    return F, T

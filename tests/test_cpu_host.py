@@ -153,3 +153,24 @@ def test_exact_forces_oracle_matches_fp64_differences():
         fd = np.stack([-(e[base + c] - e[0]) / 1e-5 for c in range(3)], 1) * rng
         scale = max(1.0, np.abs(fd).max())
         assert np.abs(fd - a[k]).max() <= 2e-3 * scale, k  # forward-difference truncation O(dx)
+
+
+def test_central_differences_oracle_matches_exact_derivative():
+    """FP64 central differences (step 1e-4) of the summed pair energy of a body
+    agree with the exact derivative (autograd) to the O(h^2) truncation."""
+    from amlp.configs import make_state
+    from amlp.engine import EnergyNet
+    from oracle import adjoint, nep, nlist
+    from oracle.shapes import SHAPES
+    s = make_state(200, "tetra16", 0.40, seed=2)
+    shape = SHAPES["tetra16"]
+    vp = nlist.sorted_pairs(nlist.reference_pairs(s.pos, s.L, 4.5))
+    _, pairs, _ = nep.min_image_filter(s.pos, vp, s.L, 2.5)
+    bodies = np.array([3, 77, 150])
+    sub = pairs[np.isin(pairs[:, 0], bodies) | np.isin(pairs[:, 1], bodies)]
+    net = EnergyNet.xavier(47, (32, 32), "silu", seed=4, device="cpu")
+    F, T = adjoint.central_difference_forces(s.pos, s.orient, sub, s.L, shape, (10, 8, 4), net.layers, "silu",
+                                             bodies, h=1e-4)
+    a = adjoint.exact_pair_forces(s.pos, s.orient, sub, s.L, shape, (10, 8, 4), net.layers, "silu", clip=False)
+    for got, want in ((F, a["forces"][bodies]), (T, a["torques"][bodies])):
+        assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max())
