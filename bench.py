@@ -394,6 +394,85 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         dist.destroy_process_group()
 
 
+# ----------------------------------------------------------------------------- NVE energy drift
+DRIFT_MODEL = os.path.join(REPO, "tests", "golden", "model_cyl24_soft.npz")
+
+
+def run_drift(args, local_rank: int) -> None:
+    """Energy conservation of the precision workload: 262,144 twisted cylinders
+    (cyl24) at packing fraction 0.35, seed 3, net 47 -> 128 -> 128 -> 1 SiLU
+    fitted to a soft point-point repulsion that vanishes inside the pair cutoff
+    (a random net's energy jumps at the cutoff would swamp the integrator's
+    drift). The lattice start is first equilibrated under the NVT thermostat at
+    kT 1.0 (``--drift-equil`` steps, dt 0.005); from that state each run
+    integrates NVE and reads H = KE_t + KE_r + PE (FP64) every 100 steps.
+    Runs: the tensor-core adjoint forces at dt 0.005 (``--drift-steps``) and at
+    dt 0.0025 (``--drift-half-steps``, to separate time-step error from the
+    rest), and the plain FP32 finite differences at dt 0.005
+    (``--drift-fd-steps``). Prints one JSON line per run."""
+    import numpy as np
+    import torch
+    from amlp.configs import make_state
+    from amlp.engine import EnergyNet, Hypers, System
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    z = np.load(args.drift_model)
+    layers = [(z[f"W{k}"], z[f"b{k}"]) for k in range(len(z.files) // 2)]
+    net = EnergyNet(layers, "silu", dev)
+    n = 262144
+    state = make_state(n, "cyl24", 0.35, kT=1.0, seed=3)
+    equil = {"steps": args.drift_equil}
+    if args.drift_equil > 0:
+        s = System(state, "cyl24", Hypers(), net, kT=1.0, dt=0.005, device=dev)
+        s.run(args.drift_equil, "adjoint")
+        th = s.thermostat()
+        equil.update(ke_per_body=(th["ke_t"] + th["ke_r"]) / n, pe_per_body=th["pe"] / n)
+        state = s.state()
+        del s
+        torch.cuda.empty_cache()
+    for method, dt, steps in (("adjoint", 0.005, args.drift_steps), ("adjoint", 0.0025, args.drift_half_steps),
+                              ("fd_split", 0.005, args.drift_fd_steps)):
+        if steps <= 0:
+            continue
+        s = System(state, "cyl24", Hypers(), net, kT=1.0, dt=dt, device=dev, nve=True)
+        H, t_H = [], []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.run(1, method)  # first force pass: H at t = 0
+        torch.cuda.synchronize()
+        H.append(s.conserved_quantity())
+        t_H.append(0)
+        th = s.thermostat()
+        ke0, pe0 = th["ke_t"] + th["ke_r"], th["pe"]
+        ev0.record()
+        while s.timestep < steps + 1:
+            s.run(min(100, steps + 1 - s.timestep), method)
+            H.append(s.conserved_quantity())
+            t_H.append(s.timestep - 1)
+        ev1.record()
+        torch.cuda.synchronize()
+        H = np.asarray(H)
+        time_units = np.asarray(t_H, np.float64) * dt
+        slope = float(np.polyfit(time_units, H, 1)[0]) if len(H) > 2 else float("nan")
+        th = s.thermostat()
+        line = {"metric": "nve_energy_drift", "method": method, "dt": dt, "steps": steps,
+                "workload": "nve-262144-cyl24-phi0.35-mlp47x128x128x1-silu", "bodies": n,
+                "filtered_pairs": int(s.nf.item()), "equilibration": equil,
+                "H0": float(H[0]), "H_end": float(H[-1]), "ke0": ke0, "pe0": pe0,
+                "ke_end": th["ke_t"] + th["ke_r"], "pe_end": th["pe"],
+                "drift_per_body": float((H[-1] - H[0]) / n),
+                "slope_per_time_unit_per_body": slope / n,
+                "max_abs_dev_per_body": float(np.abs(H - H[0]).max() / n),
+                "rel_drift_vs_ke0": float((H[-1] - H[0]) / ke0),
+                "ms_per_step": ev0.elapsed_time(ev1) / steps,
+                "precision": ("FP32 descriptors, net on tensor cores as bf16x3 splits, FP32 accumulation; "
+                              "FP64 kinetic-energy and pair-energy sums" if method == "adjoint" else
+                              "FP32 finite differences (dx = dteta = 1e-5), the reference's method"),
+                "H_per_body_samples": [float(h / n) for h in H[:: max(1, len(H) // 20)]]}
+        print(json.dumps(line), flush=True)
+        del s
+        torch.cuda.empty_cache()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -405,7 +484,19 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--bodies", type=int, default=N_BODIES,
                     help="system size (the benchmark workload is 131072; smaller sizes are for profiling)")
+    ap.add_argument("--drift", action="store_true",
+                    help="NVE energy drift of the 262,144-cylinder precision workload instead of the benchmark")
+    ap.add_argument("--drift-steps", type=int, default=10000)
+    ap.add_argument("--drift-half-steps", type=int, default=0,
+                    help="also run the adjoint forces at dt 0.0025 for this many NVE steps")
+    ap.add_argument("--drift-fd-steps", type=int, default=0,
+                    help="also run the plain finite-difference forces for this many NVE steps")
+    ap.add_argument("--drift-equil", type=int, default=2000, help="NVT steps before the NVE runs")
+    ap.add_argument("--drift-model", default=DRIFT_MODEL)
     args = ap.parse_args()
+    if args.drift:
+        run_drift(args, int(os.environ.get("LOCAL_RANK", 0)))
+        return
     if args.bodies != N_BODIES:
         globals()["WORKLOAD"] = WORKLOAD.replace(str(N_BODIES), str(args.bodies))
         globals()["N_BODIES"] = args.bodies
