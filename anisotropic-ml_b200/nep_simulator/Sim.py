@@ -137,20 +137,26 @@ class Sim:
 
     # ------------------------------------------------------------------ state
     def move_data_to_device(self):
-        state = State(pos=np.asarray(self.central_pos, np.float32), orient=np.asarray(self.orientations, np.float32),
-                      vel=np.asarray(self.velocities, np.float32), angmom=np.asarray(self.angmom, np.float32),
-                      mass=np.asarray(self.mass, np.float32), moi=np.asarray(self.moi, np.float32),
+        # the fields alias the device state after the first call (a second run continues from it)
+        def host(a):
+            return a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a, np.float32)
+        state = State(pos=host(self.central_pos), orient=host(self.orientations), vel=host(self.velocities),
+                      angmom=host(self.angmom), mass=host(self.mass), moi=np.asarray(self.moi, np.float32),
                       L=float(np.float32(self.Lx)))
         dg = self.descriptor_generator
         hyp = Hypers(dg.nrad, dg.nang, dg.lmax)
         if self.method is None:
             wide = max(self.evaluator.energy_net.dims[:-1]) > 64
             self.method = "fd_split" if wide else "fd"
+        prev = self.system.thermostat() if self.system is not None else None
         self.system = System(state, dg.shape, hyp, self.evaluator.energy_net, self.kT, self.dt, device=self.device,
-                             nve=self.nve, initial_ke_quirk=self.initial_ke_quirk,
+                             nve=self.nve, initial_ke_quirk=self.initial_ke_quirk and prev is None,
                              nlist_every=getattr(self, "Nlist_freq", 100), dx=self.dx, dteta=self.dteta,
                              moi=np.asarray(self.moi, np.float32))
-        if self._resume_thermo is not None:
+        if prev is not None:  # a later run continues the thermostat of the previous one
+            self.system.set_thermostat((prev["xi"], prev["eta"], prev["xi_rot"], prev["eta_rot"]),
+                                       prev["thermo_fac"])
+        elif self._resume_thermo is not None:
             self.system.set_thermostat(self._resume_thermo[0], self._resume_thermo[1])
         s = self.system
         self.central_pos, self.orientations, self.velocities, self.angmom = s.pos, s.quat, s.vel, s.angmom
