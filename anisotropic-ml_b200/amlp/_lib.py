@@ -79,6 +79,8 @@ SIGNATURES = {
     "amlp_nlist_workspace_bytes": [_I, _F, _D, _PSZ],
     "amlp_nlist_build": [_P, _I, _F, _D, _P, _LL, _P, _P, _SZ, _P],
     "amlp_nlist_build_noalloc": [_P, _I, _F, _D, _P, _LL, _P, _P],
+    "amlp_nlist_check_displacement": [_P, _P, _I, _F, _F, _P, _P],
+    "amlp_nlist_build_gated": [_P, _I, _F, _D, _P, _LL, _P, _P, _SZ, _P, _P, _P],
     "amlp_filter_workspace_bytes": [_LL, _PSZ],
     "amlp_pair_filter": [_P, _F, _D, _P, _P, _LL, _P, _P, _P, _SZ, _P],
     "amlp_descriptors": [_P, _P, _F, _P, _LL, ctypes.POINTER(Nep), _P, _P],

@@ -7,6 +7,13 @@ force pass (pair filter, descriptors, net, forces/torques), then
 every ``nlist_every`` steps (100, ``Sim.py:87``). ``run`` replays segments of
 steps as CUDA graphs.
 
+Verlet-list policies: ``"every"`` (the reference's fixed schedule) and
+``"displacement"``: every step checks on the device whether some body has moved
+more than half the skin since the list was built and rebuilds only then (the
+check and the gated build sit inside the graphs). A rebuild that overflows the
+list's capacity is detected after the segment, which is then run again from a
+snapshot with a larger list.
+
 Force methods:
 * ``"fd"``       -- the reference's finite differences, one fused kernel;
 * ``"fd_split"`` -- the same through the three kernels that keep g_all in HBM
@@ -113,7 +120,7 @@ class System:
     def __init__(self, state: State, shape: Shape | str, hypers: Hypers, net: EnergyNet, kT: float, dt: float,
                  device="cuda", nve: bool = False, initial_ke_quirk: bool = False, nlist_every: int = 100,
                  skin: float = 2.0, dx: float = 1e-5, dteta: float = 1e-5, tau: float | None = None,
-                 moi=None):
+                 moi=None, nlist_policy: str = "every"):
         if isinstance(shape, str):
             shape = get_shape(shape)
         if net.n_inputs != hypers.D:
@@ -138,6 +145,13 @@ class System:
         self.nve = bool(nve)
         self.nlist_every = int(nlist_every)
         self.r_verlet = float(shape.cutoff) + float(skin)  # Sim.py:86
+        if nlist_policy not in ("every", "displacement"):
+            raise ValueError(f"unknown Verlet-list policy {nlist_policy!r}")
+        self.nlist_policy = nlist_policy
+        self.max_disp = 0.5 * float(skin)
+        if nlist_policy == "displacement":
+            self.nl_ref = torch.zeros(self.N, 3, **f32)
+            self.nl_gate = torch.zeros(3, dtype=torch.int32, device=self.device)
 
         self.nep = Nep()
         self.nep.nrad, self.nep.nang, self.nep.lmax = hypers.nrad, hypers.nang, hypers.lmax
@@ -207,6 +221,8 @@ class System:
                 return -1
             n = int(self.nv.item())
             if n <= self.cap:
+                if self.nlist_policy == "displacement":
+                    self.nl_ref.copy_(self.pos)
                 return n
             self._alloc_pairs(int(n * 1.25) + 1024)
 
@@ -270,21 +286,60 @@ class System:
              self.quat.data_ptr(), self.angmom.data_ptr(), self.dp.data_ptr(), self.mass.data_ptr(), self.N,
              ctypes.byref(self.nvt), self.th.data_ptr(), self.nvt_ws.data_ptr(), self.nvt_ws.numel(), _stream())
 
+    def _gated_rebuild(self) -> None:
+        call("amlp_nlist_check_displacement", self.pos.data_ptr(), self.nl_ref.data_ptr(), self.N, self.L,
+             self.max_disp, self.nl_gate.data_ptr(), _stream())
+        call("amlp_nlist_build_gated", self.pos.data_ptr(), self.N, self.L, self.r_verlet, self.vpairs.data_ptr(),
+             self.cap, self.nv.data_ptr(), self.nl_ws.data_ptr(), self.nl_ws.numel(), self.nl_gate.data_ptr(),
+             self.nl_ref.data_ptr(), _stream())
+
+    @property
+    def rebuilds(self) -> int:
+        """Gated rebuilds so far (displacement policy)."""
+        return int(self.nl_gate[1].item()) if self.nlist_policy == "displacement" else -1
+
     def _step_kernels(self, method: str) -> None:
+        if self.nlist_policy == "displacement":
+            self._gated_rebuild()
         self.compute_forces(method)
         self.integrate_step_two()
         self.integrate_step_one()
 
     def step(self, method: str = "fd") -> None:
         """One time step, host-driven (``Sim.step``)."""
+        if self.nlist_policy == "displacement":
+            self._run_checked(1, method, graph=False)
+            return
         if self.timestep % self.nlist_every == 0 and self.timestep > 0:
             self.build_nlist()
         self._step_kernels(method)
         self.timestep += 1
 
+    def _run_checked(self, seg: int, method: str, graph: bool) -> None:
+        """``seg`` steps under the displacement policy; rerun from a snapshot
+        with a larger list if a rebuild inside them overflowed."""
+        snap = self.snapshot_tensors()
+        while True:
+            if graph and method != "fd_split":
+                self._graph(method, seg).replay()
+            else:
+                for _ in range(seg):
+                    self._step_kernels(method)
+            if not int(self.nl_gate[2].item()):
+                break
+            self.restore_tensors(snap)
+            self.nl_gate[2] = 0
+            self._alloc_pairs(int(self.cap * 1.5) + 1024)
+            self.build_nlist()
+        self.timestep += seg
+
     def run(self, nsteps: int, method: str = "fd", graph: bool = True) -> None:
         """``nsteps`` steps; between Verlet rebuilds the steps replay as one CUDA graph."""
         end = self.timestep + nsteps
+        if self.nlist_policy == "displacement":
+            while self.timestep < end:
+                self._run_checked(min(end - self.timestep, self.nlist_every), method, graph)
+            return
         while self.timestep < end:
             if self.timestep % self.nlist_every == 0 and self.timestep > 0:
                 self.build_nlist()

@@ -10,6 +10,12 @@
 // the cell lists, (4) one warp per body i counts the j > i within r over the
 // 27 neighbouring cells, (5) scan of the counts, (6) the same traversal
 // collects the j into shared memory, ranks them and writes them in order.
+//
+// Gated builds (displacement-triggered rebuilds): every kernel of the pass
+// takes gate (null = always build); with gate[0] == 0 they return at once, so
+// a CUDA graph can hold the pass in every step and only the flagged steps pay
+// for it. A gated build also stores the positions it was built from, counts
+// itself in gate[1] and sets gate[2] when the list did not fit its capacity.
 #include <mutex>
 
 #include "common.cuh"
@@ -29,9 +35,16 @@ struct Grid {
     float halfL;      // float32(L * 0.5)
 };
 
-__global__ void k_cells(const float *pos, Grid g, double *xd, int *cell_of, int *cell_count) {
+__global__ void k_cells(const float *pos, Grid g, double *xd, int *cell_of, int *cell_count, const int *gate,
+                        float *ref) {
+    if (gate && !*gate) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.n) return;
+    if (ref) {
+        ref[3 * i] = pos[3 * i];
+        ref[3 * i + 1] = pos[3 * i + 1];
+        ref[3 * i + 2] = pos[3 * i + 2];
+    }
     int c[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -45,7 +58,9 @@ __global__ void k_cells(const float *pos, Grid g, double *xd, int *cell_of, int 
     atomicAdd(&cell_count[cid], 1);
 }
 
-__global__ void k_fill(int n, const int *cell_of, const long long *cell_start, int *cell_fill, int *cell_list) {
+__global__ void k_fill(int n, const int *cell_of, const long long *cell_start, int *cell_fill, int *cell_list,
+                       const int *gate) {
+    if (gate && !*gate) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int cid = cell_of[i];
@@ -92,7 +107,8 @@ __device__ __forceinline__ void for_candidates(int i, const Grid &g, const doubl
 }
 
 __global__ void k_count(Grid g, const double *xd, const int *cell_of, const long long *cell_start,
-                        const int *cell_list, long long *counts) {
+                        const int *cell_list, long long *counts, const int *gate) {
+    if (gate && !*gate) return;
     int i = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     if (i >= g.n) return;
     int cnt = 0;
@@ -103,7 +119,8 @@ __global__ void k_count(Grid g, const double *xd, const int *cell_of, const long
 }
 
 __global__ void k_write(Grid g, const double *xd, const int *cell_of, const long long *cell_start,
-                        const int *cell_list, const long long *offsets, int *pairs, long long cap) {
+                        const int *cell_list, const long long *offsets, int *pairs, long long cap, const int *gate) {
+    if (gate && !*gate) return;
     __shared__ int buf[kWarpsPerBlock][kSortCap];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int i = blockIdx.x * kWarpsPerBlock + w;
@@ -149,8 +166,28 @@ __global__ void k_write(Grid g, const double *xd, const int *cell_of, const long
     }
 }
 
-__global__ void k_total(const long long *offsets, int n, long long *d_count) {
+__global__ void k_total(const long long *offsets, int n, long long *d_count, int *gate, long long cap) {
+    if (gate && !gate[0]) return;
     *d_count = offsets[n];
+    if (gate) {
+        gate[1] += 1;
+        if (offsets[n] > cap) gate[2] = 1;
+    }
+}
+
+// gate[0] = 1 when some body has moved more than sqrt(max_d2) from ref
+// (minimum image in the cubic box), else 0 (gate[0] is cleared before).
+__global__ void k_displacement(const float *pos, const float *ref, int n, float box, float max_d2, int *gate) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float d2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float d = pos[3 * i + k] - ref[3 * i + k];
+        d -= box * rintf(d / box);
+        d2 = fmaf(d, d, d2);
+    }
+    if (d2 > max_d2) gate[0] = 1;
 }
 
 Grid make_grid(int n, float box, double r) {
@@ -174,6 +211,9 @@ struct NlistWs {
     int *cell_of, *cell_count, *cell_fill, *cell_list;
     long long *cell_start, *counts, *scan_tmp;
 };
+
+amlp_status launch_build(const float *d_pos, const Grid &g, const NlistWs &w, int *d_pairs, long long cap,
+                         long long *d_count, int *gate, float *ref, cudaStream_t s);
 
 size_t carve(Carver &c, const Grid &g, NlistWs *w) {
     size_t ncell = (size_t)g.nc * g.nc * g.nc;
@@ -213,21 +253,57 @@ extern "C" amlp_status amlp_nlist_build(const float *d_pos, int n, float box, do
     NlistWs w;
     carve(c, g, &w);
     if (!d_ws || !c.ok()) return AMLP_ERR_WORKSPACE;
+    return launch_build(d_pos, g, w, d_pairs, cap, d_count, nullptr, nullptr, s);
+}
+
+namespace amlp {
+namespace {
+
+amlp_status launch_build(const float *d_pos, const Grid &g, const NlistWs &w, int *d_pairs, long long cap,
+                         long long *d_count, int *gate, float *ref, cudaStream_t s) {
+    const int n = g.n;
     size_t ncell = (size_t)g.nc * g.nc * g.nc;
     AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_count, 0, ncell * sizeof(int), s));
     AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_fill, 0, ncell * sizeof(int), s));
     int tb = 256;
-    k_cells<<<(n + tb - 1) / tb, tb, 0, s>>>(d_pos, g, w.xd, w.cell_of, w.cell_count);
-    amlp_status st = exclusive_scan_int(w.cell_count, w.cell_start, (long long)ncell, w.scan_tmp, s);
+    k_cells<<<(n + tb - 1) / tb, tb, 0, s>>>(d_pos, g, w.xd, w.cell_of, w.cell_count, gate, ref);
+    amlp_status st = exclusive_scan_int(w.cell_count, w.cell_start, (long long)ncell, w.scan_tmp, s, gate);
     if (st) return st;
-    k_fill<<<(n + tb - 1) / tb, tb, 0, s>>>(n, w.cell_of, w.cell_start, w.cell_fill, w.cell_list);
+    k_fill<<<(n + tb - 1) / tb, tb, 0, s>>>(n, w.cell_of, w.cell_start, w.cell_fill, w.cell_list, gate);
     int nb = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    k_count<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts);
-    st = exclusive_scan_ll(w.counts, w.counts, n, w.scan_tmp, s);
+    k_count<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, gate);
+    st = exclusive_scan_ll(w.counts, w.counts, n, w.scan_tmp, s, gate);
     if (st) return st;
-    k_write<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap);
-    k_total<<<1, 1, 0, s>>>(w.counts, n, d_count);
+    k_write<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap,
+                                               gate);
+    k_total<<<1, 1, 0, s>>>(w.counts, n, d_count, gate, cap);
     return check_launch();
+}
+
+}  // namespace
+}  // namespace amlp
+
+extern "C" amlp_status amlp_nlist_check_displacement(const float *d_pos, const float *d_ref, int n, float box,
+                                                     float max_disp, int *d_gate, void *stream) {
+    if (n <= 0 || !(box > 0.f) || !(max_disp >= 0.f) || !d_pos || !d_ref || !d_gate) return AMLP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    AMLP_CHECK_CUDA(cudaMemsetAsync(d_gate, 0, sizeof(int), s));
+    k_displacement<<<(n + 255) / 256, 256, 0, s>>>(d_pos, d_ref, n, box, max_disp * max_disp, d_gate);
+    return check_launch();
+}
+
+extern "C" amlp_status amlp_nlist_build_gated(const float *d_pos, int n, float box, double r, int *d_pairs,
+                                              long long cap, long long *d_count, void *d_ws, size_t ws_bytes,
+                                              int *d_gate, float *d_ref, void *stream) {
+    if (n <= 0 || !(box > 0.f) || !(r > 0.0) || !d_pos || !d_count || !d_gate || !d_ref || cap < 0 ||
+        (cap > 0 && !d_pairs))
+        return AMLP_ERR_INVALID_ARG;
+    Grid g = make_grid(n, box, r);
+    Carver c(d_ws, ws_bytes);
+    NlistWs w;
+    carve(c, g, &w);
+    if (!d_ws || !c.ok()) return AMLP_ERR_WORKSPACE;
+    return launch_build(d_pos, g, w, d_pairs, cap, d_count, d_gate, d_ref, as_stream(stream));
 }
 
 // ---------------------------------------------------------------------------
@@ -299,18 +375,5 @@ extern "C" amlp_status amlp_nlist_build_noalloc(const float *d_pos, int n, float
     if (st) return st;
     Carver c(scratch, kNoAllocScratchBytes);
     carve(c, g, &w);
-    cudaStream_t s = as_stream(stream);
-    size_t ncell = (size_t)g.nc * g.nc * g.nc;
-    AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_count, 0, ncell * sizeof(int), s));
-    AMLP_CHECK_CUDA(cudaMemsetAsync(w.cell_fill, 0, ncell * sizeof(int), s));
-    int tb = 256;
-    k_cells<<<(n + tb - 1) / tb, tb, 0, s>>>(d_pos, g, w.xd, w.cell_of, w.cell_count);
-    if ((st = exclusive_scan_int(w.cell_count, w.cell_start, (long long)ncell, w.scan_tmp, s))) return st;
-    k_fill<<<(n + tb - 1) / tb, tb, 0, s>>>(n, w.cell_of, w.cell_start, w.cell_fill, w.cell_list);
-    int nb = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    k_count<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts);
-    if ((st = exclusive_scan_ll(w.counts, w.counts, n, w.scan_tmp, s))) return st;
-    k_write<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap);
-    k_total<<<1, 1, 0, s>>>(w.counts, n, d_count);
-    return check_launch();
+    return launch_build(d_pos, g, w, d_pairs, cap, d_count, nullptr, nullptr, as_stream(stream));
 }

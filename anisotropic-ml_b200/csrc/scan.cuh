@@ -1,7 +1,8 @@
 // Device-wide exclusive prefix sums (three passes: tile sums, scan of the tile
 // sums in one block, tile scans with their offsets). out[0..n] receives n+1
 // values, out[n] being the total; out may alias in (each tile is read before
-// it is written).
+// it is written). With a non-null gate every kernel returns at once when
+// gate[0] == 0 (the scan is part of a pass that only runs when flagged).
 #pragma once
 #include "common.cuh"
 
@@ -40,7 +41,8 @@ __device__ __forceinline__ long long block_exclusive_scan(long long v, long long
 }
 
 template <class T>
-__global__ void k_tile_sums(const T *in, long long n, long long *tsum) {
+__global__ void k_tile_sums(const T *in, long long n, long long *tsum, const int *gate) {
+    if (gate && !*gate) return;
     long long i = (long long)blockIdx.x * kScanTile + threadIdx.x;
     long long v = i < n ? (long long)in[i] : 0;
     long long tot;
@@ -49,7 +51,8 @@ __global__ void k_tile_sums(const T *in, long long n, long long *tsum) {
 }
 
 // Exclusive scan of the tile sums in one block (any number of tiles).
-__global__ void k_scan_tiles(long long *tsum, long long ntiles) {
+__global__ void k_scan_tiles(long long *tsum, long long ntiles, const int *gate) {
+    if (gate && !*gate) return;
     long long carry = 0;
     for (long long base = 0; base < ntiles; base += blockDim.x) {
         long long i = base + threadIdx.x;
@@ -63,7 +66,9 @@ __global__ void k_scan_tiles(long long *tsum, long long ntiles) {
 }
 
 template <class T>
-__global__ void k_tile_scan(const T *in, long long *out, long long n, const long long *tsum, long long ntiles) {
+__global__ void k_tile_scan(const T *in, long long *out, long long n, const long long *tsum, long long ntiles,
+                            const int *gate) {
+    if (gate && !*gate) return;
     long long i = (long long)blockIdx.x * kScanTile + threadIdx.x;
     long long v = i < n ? (long long)in[i] : 0;
     long long tot;
@@ -73,21 +78,23 @@ __global__ void k_tile_scan(const T *in, long long *out, long long n, const long
 }
 
 template <class T>
-inline amlp_status exclusive_scan(const T *in, long long *out, long long n, long long *tmp, cudaStream_t s) {
+inline amlp_status exclusive_scan(const T *in, long long *out, long long n, long long *tmp, cudaStream_t s,
+                                  const int *gate = nullptr) {
     long long ntiles = (n + kScanTile - 1) / kScanTile;
     if (ntiles == 0) ntiles = 1;
-    k_tile_sums<T><<<(unsigned)ntiles, kScanTile, 0, s>>>(in, n, tmp);
-    k_scan_tiles<<<1, kScanTile, 0, s>>>(tmp, ntiles);
-    k_tile_scan<T><<<(unsigned)ntiles, kScanTile, 0, s>>>(in, out, n, tmp, ntiles);
+    k_tile_sums<T><<<(unsigned)ntiles, kScanTile, 0, s>>>(in, n, tmp, gate);
+    k_scan_tiles<<<1, kScanTile, 0, s>>>(tmp, ntiles, gate);
+    k_tile_scan<T><<<(unsigned)ntiles, kScanTile, 0, s>>>(in, out, n, tmp, ntiles, gate);
     return AMLP_OK;
 }
 
-inline amlp_status exclusive_scan_int(const int *in, long long *out, long long n, long long *tmp, cudaStream_t s) {
-    return exclusive_scan<int>(in, out, n, tmp, s);
+inline amlp_status exclusive_scan_int(const int *in, long long *out, long long n, long long *tmp, cudaStream_t s,
+                                      const int *gate = nullptr) {
+    return exclusive_scan<int>(in, out, n, tmp, s, gate);
 }
 inline amlp_status exclusive_scan_ll(const long long *in, long long *out, long long n, long long *tmp,
-                                     cudaStream_t s) {
-    return exclusive_scan<long long>(in, out, n, tmp, s);
+                                     cudaStream_t s, const int *gate = nullptr) {
+    return exclusive_scan<long long>(in, out, n, tmp, s, gate);
 }
 
 }  // namespace amlp

@@ -21,6 +21,9 @@
  *
  * Reference interfaces replaced (paths inside the reference project):
  *   amlp_nlist_build      Sim.setNeighborList / Sim.refreshNList   Sim.py:85-92, :192-198
+ *   amlp_nlist_build_gated, amlp_nlist_check_displacement
+ *                         the rebuild schedule of Sim.run (every 100 steps, Sim.py:218-221)
+ *                         replaced by a displacement criterion (opt-in)
  *   amlp_pair_filter      DescriptorGenerator.pos_to_pts (filter)  DescriptorGenerator.py:168-182
  *   amlp_descriptors      DescriptorGenerator.generate_nep_descriptors  DescriptorGenerator.py:136-161
  *                         (pos_to_pts :163-218, apply_dx_dteta :220-255, pts_to_nep_descriptors :296-442)
@@ -135,6 +138,24 @@ amlp_status amlp_nlist_build(const float *d_pos, int n, float box, double r,
  * Calls share the array, so calls that overlap on the GPU race. */
 amlp_status amlp_nlist_build_noalloc(const float *d_pos, int n, float box, double r,
                                      int *d_pairs, long long cap, long long *d_count, void *stream);
+
+/* Displacement-triggered rebuilds (no reference counterpart: the reference
+ * rebuilds every 100 steps, Sim.py:87, :218-221).
+ *   amlp_nlist_check_displacement: d_gate[0] = 1 when some body has moved
+ *     farther than max_disp (minimum image in the box) from d_ref, else 0.
+ *     With max_disp = skin / 2 no pair within the cutoff can be missing from
+ *     a list built with radius cutoff + skin.
+ *   amlp_nlist_build_gated: amlp_nlist_build when d_gate[0] != 0 (it then also
+ *     copies d_pos to d_ref, adds 1 to d_gate[1] and sets d_gate[2] = 1 if the
+ *     list had more than cap pairs); nothing otherwise. Both take the same
+ *     launches whatever the flag, so a CUDA graph can hold them in every step.
+ *     d_gate: three ints in device memory; d_gate[1] and d_gate[2] are only
+ *     ever raised by the library (the caller clears them). */
+amlp_status amlp_nlist_check_displacement(const float *d_pos, const float *d_ref, int n, float box,
+                                          float max_disp, int *d_gate, void *stream);
+amlp_status amlp_nlist_build_gated(const float *d_pos, int n, float box, double r, int *d_pairs,
+                                   long long cap, long long *d_count, void *d_ws, size_t ws_bytes,
+                                   int *d_gate, float *d_ref, void *stream);
 
 /* --------------------------------------------------------------- pair filter
  * Minimum image (FP32, box L) and |t| < cutoff on the Verlet pairs, kept in
