@@ -33,6 +33,10 @@ constexpr int kAThreads = 256;
 constexpr int kMaxHidden = 3;
 constexpr int kWpad = 64;          // hidden widths padded to 64 in TMEM regions
 constexpr uint32_t kErrMbarTimeout = 1u;
+// Shared-memory row strides of per-pair arrays, odd so that the 32 pairs of a
+// warp (thread = pair) hit 32 different banks.
+constexpr int kGS = 49;           // descriptor partials / dE/dg rows (48 used)
+constexpr int kPartStride = 13;   // gradient partial sums (12 used)
 
 struct AdjNet {
     int nh;                         // hidden layers
@@ -288,14 +292,15 @@ struct AdjShared {
     char *ops;         // MLP operand area (bf16 hi/lo tiles)
     char *wts;         // weights (bf16 hi/lo), resident
     float *par;        // biases + last-layer weights (fp32)
-    float *g0, *g1;    // per-half descriptor partials, kAP x 48 each; g0 later holds dE/dg
+    float *g0, *g1;    // per-half descriptor partials, kAP x kGS each; g0 later holds dE/dg
     float *t;          // translations, kAP x 3
     float *cen;        // centroids, kAP x 3
-    float *part;       // per-half gradient partial sums, 2 x kAP x 12
+    float *part;       // per-half gradient partial sums, 2 x kAP x kPartStride
     float *eps;        // per-half energy partials, 2 x kAP
     float *fd;         // per-pair F, T_i, T_j, kAP x 9
     int *ij;           // pair indices, kAP x 2
     float *pts;        // body points
+    float4 *q;         // orientations of the tile's pairs, kAP x 2 (i, j)
 };
 
 // Activation tile of layer k in the operand area (hi at its base, lo after it).
@@ -331,6 +336,19 @@ __device__ __forceinline__ void store_split8(char *tile_hi, int K, int p, int c0
     *reinterpret_cast<uint4 *>(tile_hi + kAP * K * 2 + off) = *reinterpret_cast<uint4 *>(lo);
 }
 
+// Rotated body points of the tile's pairs into S.R from the orientations in S.q.
+__device__ __forceinline__ void rotate_tile(const AdjShared &S, int npts, int rs) {
+    const int nd = 2 * npts;
+    for (int idx = threadIdx.x; idx < kAP * nd; idx += blockDim.x) {
+        int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
+        float3 r = rotate_ref(S.q[2 * q + body], make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
+        float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
+        dst[0] = r.x;
+        dst[1] = r.y;
+        dst[2] = r.z;
+    }
+}
+
 // MULTI: the pairs come from many systems in one launch; body i's system is
 // rep[i], its box rp[rep[i]].box, and the pair energies are summed per system
 // into pe[rep[i]].
@@ -342,7 +360,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                                                                 float *T, double *pe, const int *rep,
                                                                 const amlp_replica *rp) {
     constexpr int KC = Half<Cfg>::KC;
-    constexpr int DP = 48;  // padded descriptor width in fp32 staging
+    constexpr int DP = kGS;  // row stride of the fp32 descriptor staging
     extern __shared__ __align__(128) char smem_raw[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
@@ -373,7 +391,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     S.cen = reinterpret_cast<float *>(smem_raw + off);
     off += (size_t)kAP * 3 * 4;
     S.part = reinterpret_cast<float *>(smem_raw + off);
-    off += (size_t)2 * kAP * 12 * 4;
+    off += (size_t)2 * kAP * kPartStride * 4;
     S.eps = reinterpret_cast<float *>(smem_raw + off);
     off += (size_t)2 * kAP * 4;
     S.fd = reinterpret_cast<float *>(smem_raw + off);
@@ -381,6 +399,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     S.ij = reinterpret_cast<int *>(smem_raw + off);
     off += (size_t)kAP * 2 * 4;
     S.pts = reinterpret_cast<float *>(smem_raw + off);
+    off = align_up(off + (size_t)3 * npts * 4, 16);
+    S.q = reinterpret_cast<float4 *>(smem_raw + off);
 
     // ---- one-time set-up: weights (bf16 hi/lo, K-major), biases, TMEM, mbarrier
     for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = pts[k];
@@ -442,20 +462,12 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long p0 = tile * kAP;
         const int valid = (int)min((long long)kAP, P - p0);
-        // ---- 1. rotated body points, translations, pair indices
-        for (int idx = tid; idx < kAP * nd; idx += kAThreads) {
-            int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
-            long long pr = min(p0 + q, P - 1);
-            float4 qq = load_quat(quat, pairs[2 * pr + body]);
-            float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
-            float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
-            dst[0] = r.x;
-            dst[1] = r.y;
-            dst[2] = r.z;
-        }
+        // ---- 1. pair indices, orientations, translations, then the rotated body points
         if (tid < kAP) {
             long long pr = min(p0 + tid, P - 1);
             int i = pairs[2 * pr], j = pairs[2 * pr + 1];
+            S.q[2 * tid] = load_quat(quat, i);
+            S.q[2 * tid + 1] = load_quat(quat, j);
             float dd;
             float3 tt = min_image(pos, i, j, MULTI ? rp[rep[i]].box : L, &dd);
             S.t[3 * tid] = tt.x;
@@ -464,6 +476,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             S.ij[2 * tid] = i;
             S.ij[2 * tid + 1] = j;
         }
+        __syncthreads();
+        rotate_tile(S, npts, rs);
         __syncthreads();
         // ---- 2. descriptor forward
         const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
@@ -581,24 +595,15 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         if (!MULTI && h == 0 && p < valid)
             pe_acc += (double)en_min + (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
         // ---- 4. recompute the rotated points (their area held the MLP tiles)
-        for (int idx = tid; idx < kAP * nd; idx += kAThreads) {
-            int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
-            long long pr = min(p0 + q, P - 1);
-            float4 qq = load_quat(quat, pairs[2 * pr + body]);
-            float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
-            float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
-            dst[0] = r.x;
-            dst[1] = r.y;
-            dst[2] = r.z;
-        }
+        rotate_tile(S, npts, rs);
         __syncthreads();
         // ---- descriptor backward
-        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + p * 12, A);
-        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * 12, A);
+        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + p * kPartStride, A);
+        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * kPartStride, A);
         __syncthreads();
         // ---- 5. per-pair forces and torques
         if (tid < kAP) {
-            const float *a0 = S.part + p * 12, *a1 = S.part + (kAP + p) * 12;
+            const float *a0 = S.part + p * kPartStride, *a1 = S.part + (kAP + p) * kPartStride;
             float Si[3], Sa[3], Xi[3], Xj[3], Pi[3] = {0, 0, 0}, Qj[3] = {0, 0, 0};
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -736,7 +741,7 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
     if (tid < kAP) {
         const int p = tid;
         const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
-        const float *a0 = S.part + p * 12, *a1 = S.part + (kAP + p) * 12;
+        const float *a0 = S.part + p * kPartStride, *a1 = S.part + (kAP + p) * kPartStride;
         float Si[3], Sa[3], Xi[3], Xj[3], Pi[3] = {0, 0, 0}, Qj[3] = {0, 0, 0};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -849,18 +854,20 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
     S.R = reinterpret_cast<float *>(smem_raw);
     off = align_up((size_t)kAP * rs * 4, 128);
     S.g0 = reinterpret_cast<float *>(smem_raw + off);
-    off += (size_t)kAP * kGP * 4;
+    off += (size_t)kAP * kGS * 4;
     S.g1 = reinterpret_cast<float *>(smem_raw + off);
-    off += (size_t)kAP * kGP * 4;
+    off += (size_t)kAP * kGS * 4;
     S.t = reinterpret_cast<float *>(smem_raw + off);
     off += (size_t)kAP * 3 * 4;
     S.part = reinterpret_cast<float *>(smem_raw + off);
-    off += (size_t)2 * kAP * 12 * 4;
+    off += (size_t)2 * kAP * kPartStride * 4;
     S.fd = reinterpret_cast<float *>(smem_raw + off);
     off += (size_t)kAP * 9 * 4;
     S.ij = reinterpret_cast<int *>(smem_raw + off);
     off += (size_t)kAP * 2 * 4;
     S.pts = reinterpret_cast<float *>(smem_raw + off);
+    off = align_up(off + (size_t)3 * npts * 4, 16);
+    S.q = reinterpret_cast<float4 *>(smem_raw + off);
     for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = pts[k];
     __syncthreads();
     const long long P = min(*d_np, cap);
@@ -869,19 +876,11 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long p0 = tile * kAP;
         const int valid = (int)min((long long)kAP, P - p0);
-        for (int idx = tid; idx < kAP * nd; idx += kAThreads) {
-            int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
-            long long pr = min(p0 + q, P - 1);
-            float4 qq = load_quat(quat, pairs[2 * pr + body]);
-            float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
-            float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
-            dst[0] = r.x;
-            dst[1] = r.y;
-            dst[2] = r.z;
-        }
         if (tid < kAP) {
             long long pr = min(p0 + tid, P - 1);
             int i = pairs[2 * pr], j = pairs[2 * pr + 1];
+            S.q[2 * tid] = load_quat(quat, i);
+            S.q[2 * tid + 1] = load_quat(quat, j);
             float dd;
             float3 tt = min_image(pos, i, j, MULTI ? rp[rep[i]].box : L, &dd);
             S.t[3 * tid] = tt.x;
@@ -890,6 +889,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             S.ij[2 * tid] = i;
             S.ij[2 * tid + 1] = j;
         }
+        __syncthreads();
+        rotate_tile(S, npts, rs);
         __syncthreads();
         const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
         const float3 t = make_float3(S.t[3 * p], S.t[3 * p + 1], S.t[3 * p + 2]);
@@ -907,25 +908,25 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             c.z *= inv;
         }
         float A[Cfg::NA][KC];
-        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, A);
-        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGP, A);
+        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, A);
+        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGS, A);
         __syncthreads();
         if (!BWD) {
             for (int idx = tid; idx < kAP * g_ld; idx += kAThreads) {
                 int q = idx / g_ld, d = idx - q * g_ld;
                 if (q < valid)
-                    g_rows[(p0 + q) * g_ld + d] = d < Cfg::D ? S.g0[q * kGP + d] + S.g1[q * kGP + d] : 0.f;
+                    g_rows[(p0 + q) * g_ld + d] = d < Cfg::D ? S.g0[q * kGS + d] + S.g1[q * kGS + d] : 0.f;
             }
             __syncthreads();
             continue;
         }
         for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
-            int q = idx / kGP;
-            S.g0[idx] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
+            int q = idx / kGP, d = idx - q * kGP;
+            S.g0[q * kGS + d] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
         }
         __syncthreads();
-        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, S.part + p * 12, A);
-        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGP, S.part + (kAP + p) * 12, A);
+        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, S.part + p * kPartStride, A);
+        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, S.part + (kAP + p) * kPartStride, A);
         __syncthreads();
         adj_finish_tile<MULTI>(S, rs, npts, valid, en_min, en_range, y_rows, p0, F, T, pe, rep, pe_acc, clip);
     }
@@ -1151,8 +1152,8 @@ static amlp_status launch_adjoint(const float *d_pos, const float *d_quat, float
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
     size_t r_bytes = (size_t)kAP * rs * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
     size_t smem = align_up(std::max(r_bytes, ops_bytes), 128) + align_up(wsm, 128) + align_up((size_t)par * 4, 128) +
-                  (size_t)kAP * 48 * 4 * 2 + (size_t)kAP * 3 * 4 * 2 + (size_t)2 * kAP * 12 * 4 + (size_t)2 * kAP * 4 +
-                  (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 + 128;
+                  (size_t)kAP * kGS * 4 * 2 + (size_t)kAP * 3 * 4 * 2 + (size_t)2 * kAP * kPartStride * 4 + (size_t)2 * kAP * 4 +
+                  (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 + (size_t)kAP * 32 + 16 + 128;
     if (smem > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
     cudaStream_t s = as_stream(stream);
@@ -1225,8 +1226,9 @@ extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes
 
 static size_t wide_desc_smem(int npts) {
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
-    return align_up((size_t)kAP * rs * 4, 128) + (size_t)kAP * kGP * 4 * 2 + (size_t)kAP * 3 * 4 +
-           (size_t)2 * kAP * 12 * 4 + (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4;
+    return align_up((size_t)kAP * rs * 4, 128) + (size_t)kAP * kGS * 4 * 2 + (size_t)kAP * 3 * 4 +
+           (size_t)2 * kAP * kPartStride * 4 + (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 +
+           (size_t)kAP * 32 + 16;
 }
 
 static amlp_status check_pair_args(const float *d_pos, const float *d_quat, const int *d_pairs,
