@@ -51,6 +51,31 @@ struct AdjNet {
     int par_total;
 };
 
+// Activation and its derivative from one exponential, for the tensor-core
+// epilogues (the net there is accurate to about 1e-5 relative, so the fast
+// exponential's few-ulp error does not show): tanh(z) = 1 - 2 / (1 + e^(2z)),
+// tanh' = 1 - tanh^2; silu(z) = z s, silu' = s (1 + z (1 - s)), s = 1 / (1 + e^-z).
+__device__ __forceinline__ void act_pair(int act, float z, float &f, float &df) {
+    if (act == AMLP_ACT_RELU) {
+        f = fmaxf(z, 0.0f);
+        df = z > 0.0f ? 1.0f : 0.0f;
+    } else if (act == AMLP_ACT_TANH) {
+        const float t = 1.0f - __fdividef(2.0f, 1.0f + __expf(2.0f * z));
+        f = t;
+        df = fmaf(-t, t, 1.0f);
+    } else {
+        const float sg = __fdividef(1.0f, 1.0f + __expf(-z));
+        f = z * sg;
+        df = sg * fmaf(z, 1.0f - sg, 1.0f);
+    }
+}
+
+__device__ __forceinline__ float act_dfast(int act, float z) {
+    float f, df;
+    act_pair(act, z, f, df);
+    return df;
+}
+
 // Derivative of f_n with respect to the distance d, together with f_n.
 template <int NR>
 __device__ __forceinline__ void radial_basis_grad(float d, float inv_rc, float *f, float *df) {
@@ -301,7 +326,25 @@ struct AdjShared {
     int *ij;           // pair indices, kAP x 2
     float *pts;        // body points
     float4 *q;         // orientations of the tile's pairs, kAP x 2 (i, j)
+    float *psum;       // sum of the body points (body frame), 3
 };
+
+// Sum of the body-frame points into S.psum (one warp; call before a barrier).
+__device__ __forceinline__ void body_point_sum(const AdjShared &S, int npts) {
+    if (threadIdx.x < 32) {
+        float v[3] = {0.f, 0.f, 0.f};
+        for (int a = threadIdx.x; a < npts; a += 32)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) v[k] += S.pts[3 * a + k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) S.psum[k] = v[k];
+    }
+}
 
 // Activation tile of layer k in the operand area (hi at its base, lo after it).
 // Only two are live at a time (the one an MMA reads and the one its epilogue
@@ -366,6 +409,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     __shared__ double pe_s[kAThreads / 32];
+    __shared__ float psum_s[3];
 
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
@@ -401,9 +445,12 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     S.pts = reinterpret_cast<float *>(smem_raw + off);
     off = align_up(off + (size_t)3 * npts * 4, 16);
     S.q = reinterpret_cast<float4 *>(smem_raw + off);
+    S.psum = psum_s;
 
     // ---- one-time set-up: weights (bf16 hi/lo, K-major), biases, TMEM, mbarrier
     for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = pts[k];
+    __syncthreads();
+    body_point_sum(S, npts);
     for (int L2 = 0; L2 < net.nh; ++L2) {
         const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
         const float *W = w + net.woff[L2];
@@ -542,12 +589,13 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 tc::tmem_ld8(tmem + lane_base + zcol(L2) + c0, z);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    float zz = z[k] + bias[c0 + k];
+                    float zz = z[k] + bias[c0 + k], fz, dfz;
+                    act_pair(net.act, zz, fz, dfz);
                     if (last) {
-                        esum = fmaf(wl[c0 + k], act_f(net.act, zz), esum);
-                        v[k] = wl[c0 + k] * act_df(net.act, zz);
+                        esum = fmaf(wl[c0 + k], fz, esum);
+                        v[k] = wl[c0 + k] * dfz;
                     } else {
-                        v[k] = act_f(net.act, zz);
+                        v[k] = fz;
                     }
                 }
                 store_split8(dst, Np, p, c0, v);
@@ -577,7 +625,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                     tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
                     tc::tmem_ld8(tmem + lane_base + zcol(L2 - 1) + c0, z);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_df(net.act, z[k] + bias[c0 + k]);
+                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_dfast(net.act, z[k] + bias[c0 + k]);
                     store_split8(dst, Kp, p, c0, v);
                 }
                 tc::fence_async_smem();
@@ -604,7 +652,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         // ---- 5. per-pair forces and torques
         if (tid < kAP) {
             const float *a0 = S.part + p * kPartStride, *a1 = S.part + (kAP + p) * kPartStride;
-            float Si[3], Sa[3], Xi[3], Xj[3], Pi[3] = {0, 0, 0}, Qj[3] = {0, 0, 0};
+            float Si[3], Sa[3], Xi[3], Xj[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 Si[k] = a0[k] + a1[k];
@@ -612,14 +660,10 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 Xi[k] = a0[6 + k] + a1[6 + k];
                 Xj[k] = a0[9 + k] + a1[9 + k];
             }
-            for (int a = 0; a < npts; ++a) {
-                Pi[0] += Ri[3 * a];
-                Pi[1] += Ri[3 * a + 1];
-                Pi[2] += Ri[3 * a + 2];
-                Qj[0] += Rj[3 * a];
-                Qj[1] += Rj[3 * a + 1];
-                Qj[2] += Rj[3 * a + 2];
-            }
+            // sums of the rotated points of i and of j: the rotation of the point sum
+            const float3 ps = make_float3(S.psum[0], S.psum[1], S.psum[2]);
+            const float3 pi3 = rotate_ref(S.q[2 * p], ps), qj3 = rotate_ref(S.q[2 * p + 1], ps);
+            const float Pi[3] = {pi3.x, pi3.y, pi3.z}, Qj[3] = {qj3.x, qj3.y, qj3.z};
             const float inv_nd = 1.0f / (float)nd;
             float Gm[3] = {Sa[0] * inv_nd, Sa[1] * inv_nd, Sa[2] * inv_nd};  // mean gradient
             float Fp[3], Ti[3], Tj[3];
@@ -740,9 +784,8 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
     const int nd = 2 * npts;
     if (tid < kAP) {
         const int p = tid;
-        const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
         const float *a0 = S.part + p * kPartStride, *a1 = S.part + (kAP + p) * kPartStride;
-        float Si[3], Sa[3], Xi[3], Xj[3], Pi[3] = {0, 0, 0}, Qj[3] = {0, 0, 0};
+        float Si[3], Sa[3], Xi[3], Xj[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             Si[k] = a0[k] + a1[k];
@@ -750,14 +793,9 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
             Xi[k] = a0[6 + k] + a1[6 + k];
             Xj[k] = a0[9 + k] + a1[9 + k];
         }
-        for (int a = 0; a < npts; ++a) {
-            Pi[0] += Ri[3 * a];
-            Pi[1] += Ri[3 * a + 1];
-            Pi[2] += Ri[3 * a + 2];
-            Qj[0] += Rj[3 * a];
-            Qj[1] += Rj[3 * a + 1];
-            Qj[2] += Rj[3 * a + 2];
-        }
+        const float3 ps = make_float3(S.psum[0], S.psum[1], S.psum[2]);
+        const float3 pi3 = rotate_ref(S.q[2 * p], ps), qj3 = rotate_ref(S.q[2 * p + 1], ps);
+        const float Pi[3] = {pi3.x, pi3.y, pi3.z}, Qj[3] = {qj3.x, qj3.y, qj3.z};
         const float inv_nd = 1.0f / (float)nd;
         float Gm[3] = {Sa[0] * inv_nd, Sa[1] * inv_nd, Sa[2] * inv_nd};
         float Fp[3], Ti[3], Tj[3];
@@ -846,10 +884,12 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
     constexpr int KC = Half<Cfg>::KC;
     extern __shared__ __align__(128) char smem_raw[];
     __shared__ double pe_s[kAThreads / 32];
+    __shared__ float psum_s[3];
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
     const int nd = 2 * npts;
     AdjShared S;
+    S.psum = psum_s;
     size_t off = 0;
     S.R = reinterpret_cast<float *>(smem_raw);
     off = align_up((size_t)kAP * rs * 4, 128);
@@ -869,6 +909,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
     off = align_up(off + (size_t)3 * npts * 4, 16);
     S.q = reinterpret_cast<float4 *>(smem_raw + off);
     for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = pts[k];
+    __syncthreads();
+    body_point_sum(S, npts);
     __syncthreads();
     const long long P = min(*d_np, cap);
     const long long ntiles = (P + kAP - 1) / kAP;
@@ -1040,12 +1082,13 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
                 tc::tmem_ld8(tmem + lane_base + (uint32_t)(L2 * kWideMax) + c0, z);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    float zz = z[k] + bias[c0 + k];
+                    float zz = z[k] + bias[c0 + k], fz, dfz;
+                    act_pair(net.act, zz, fz, dfz);
                     if (last) {
-                        esum = fmaf(wl[c0 + k], act_f(net.act, zz), esum);
-                        v[k] = wl[c0 + k] * act_df(net.act, zz);
+                        esum = fmaf(wl[c0 + k], fz, esum);
+                        v[k] = wl[c0 + k] * dfz;
                     } else {
-                        v[k] = act_f(net.act, zz);
+                        v[k] = fz;
                     }
                 }
                 store_split8(tile(L2 + 1), Np, p, c0, v);
@@ -1075,7 +1118,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
                     tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
                     tc::tmem_ld8(tmem + lane_base + (uint32_t)((L2 - 1) * kWideMax) + c0, z);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_df(net.act, z[k] + bias[c0 + k]);
+                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_dfast(net.act, z[k] + bias[c0 + k]);
                     store_split8(tile(L2), Kp, p, c0, v);
                 }
             } else {
