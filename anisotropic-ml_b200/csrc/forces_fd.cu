@@ -31,25 +31,18 @@ __host__ __device__ inline TileGeom tile_geom(int npts) {
 }
 
 // Rotated body points of the pairs [p0, p0 + kPT) (clamped to the last pair),
-// the minimum-image translations and the pair indices.
+// the minimum-image translations and the pair indices. The pairs'
+// orientations are read once into shared memory first. The caller's barrier
+// must separate this from the previous use of R, t and ij.
 __device__ void load_tile(const float *pos, const float *quat, float L, const int *pairs, long long P, long long p0,
                           const float *pts_s, const TileGeom &g, float *R, float *t, int *ij) {
+    __shared__ float4 qs[2 * kPT];
     const int nthr = blockDim.x;
-    for (int idx = threadIdx.x; idx < kPT * g.nd; idx += nthr) {
-        int p = idx / g.nd, rem = idx - p * g.nd;
-        int body = rem / g.npts, a = rem - body * g.npts;
-        long long pr = min(p0 + p, P - 1);
-        int who = pairs[2 * pr + body];
-        float4 q = load_quat(quat, who);
-        float3 r = rotate_ref(q, make_float3(pts_s[3 * a], pts_s[3 * a + 1], pts_s[3 * a + 2]));
-        float *dst = R + p * g.rs + body * 3 * g.npts + 3 * a;
-        dst[0] = r.x;
-        dst[1] = r.y;
-        dst[2] = r.z;
-    }
     for (int p = threadIdx.x; p < kPT; p += nthr) {
         long long pr = min(p0 + p, P - 1);
         int i = pairs[2 * pr], j = pairs[2 * pr + 1];
+        qs[2 * p] = load_quat(quat, i);
+        qs[2 * p + 1] = load_quat(quat, j);
         float d;
         float3 tt = min_image(pos, i, j, L, &d);
         t[3 * p] = tt.x;
@@ -58,12 +51,22 @@ __device__ void load_tile(const float *pos, const float *quat, float L, const in
         ij[2 * p] = i;
         ij[2 * p + 1] = j;
     }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kPT * g.nd; idx += nthr) {
+        int p = idx / g.nd, rem = idx - p * g.nd;
+        int body = rem / g.npts, a = rem - body * g.npts;
+        float3 r = rotate_ref(qs[2 * p + body], make_float3(pts_s[3 * a], pts_s[3 * a + 1], pts_s[3 * a + 2]));
+        float *dst = R + p * g.rs + body * 3 * g.npts + 3 * a;
+        dst[0] = r.x;
+        dst[1] = r.y;
+        dst[2] = r.z;
+    }
 }
 
-// Descriptor of row (v = warp, p = lane) of the staged tile into gT[d*ld + row].
+// Descriptor of row (v = warp, p = lane) of the staged tile into gT[d*ld + col].
 template <class Cfg>
 __device__ __forceinline__ void tile_descriptor_row(const float *R, const float *t, const TileGeom &g, float dx,
-                                                    float dteta, float inv_rc, float *gT, int ld) {
+                                                    float dteta, float inv_rc, float *gT, int ld, int col) {
     const int v = threadIdx.x >> 5, p = threadIdx.x & 31;
     VariantPoints vp;
     vp.Ri = R + p * g.rs;
@@ -75,7 +78,7 @@ __device__ __forceinline__ void tile_descriptor_row(const float *R, const float 
     vp.v = v;
     vp.dx = dx;
     vp.q = variant_quat(v, dteta);
-    nep_descriptor<Cfg>(vp, g.nd, inv_rc, gT + threadIdx.x, ld);
+    nep_descriptor<Cfg>(vp, g.nd, inv_rc, gT + col, ld);
 }
 
 // ---------------------------------------------------------------- g_all to HBM
@@ -98,7 +101,7 @@ __global__ void __launch_bounds__(kTileThreads) k_descriptors(const float *pos, 
         long long p0 = tile * kPT;
         load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
         __syncthreads();
-        tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld);
+        tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld, threadIdx.x);
         __syncthreads();
         int valid = (int)min((long long)kPT, P - p0);
         // rows v*P + p0 .. p0+valid-1 of variant v are contiguous in g_all
@@ -211,13 +214,23 @@ struct FusedNet {
     int wt_total;
 };
 
-// YT[n*kRows + r] = act(b[n] + sum_k XT[k*kRows + r] WT[k*npad + n]) for n < npad;
-// 8x8 register tiles, float4 shared-memory loads.
+// Activations of the fused net are feature-major, YT[n*kRows + col], with the
+// rows permuted: row r = 8 rg + 4 hf + i (i < 4) sits at column
+// hf * kRows/2 + 4 rg + i. A thread owns the 8 rows of one rg; the 8 threads
+// of a quarter warp take consecutive rg, so their float4 loads and stores of
+// activations cover 128 contiguous bytes (no bank conflicts) and they share
+// the weight loads (broadcast).
+static_assert(kRows % 8 == 0, "rows come in groups of 8");
+__host__ __device__ constexpr int act_col(int r) { return ((r >> 2) & 1) * (kRows / 2) + (r >> 3) * 4 + (r & 3); }
+
+// YT[n][r] = act(b[n] + sum_k XT[k][r] WT[k*npad + n]) for n < npad, rows in the
+// permuted layout above; 8x8 register tiles.
 __device__ __forceinline__ void tile_gemm(const float *XT, int K, const float *WT, const float *b, int npad, float *YT,
                                           int act) {
-    const int ncg = npad / 8, items = (kRows / 8) * ncg;
+    constexpr int nrg = kRows / 8, hoff = kRows / 2;
+    const int items = nrg * (npad / 8);
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int cg = it % ncg, rg = it / ncg;
+        const int rg = it % nrg, cg = it / nrg;
         float acc[8][8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -225,11 +238,11 @@ __device__ __forceinline__ void tile_gemm(const float *XT, int K, const float *W
 #pragma unroll
             for (int i = 0; i < 8; ++i) acc[i][j] = bj;
         }
-        const float *xp = XT + rg * 8;
+        const float *xp = XT + rg * 4;
         const float *wp = WT + cg * 8;
         for (int k = 0; k < K; ++k) {
             float4 x0 = *reinterpret_cast<const float4 *>(xp + k * kRows);
-            float4 x1 = *reinterpret_cast<const float4 *>(xp + k * kRows + 4);
+            float4 x1 = *reinterpret_cast<const float4 *>(xp + k * kRows + hoff);
             float4 w0 = *reinterpret_cast<const float4 *>(wp + k * npad);
             float4 w1 = *reinterpret_cast<const float4 *>(wp + k * npad + 4);
             float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
@@ -244,9 +257,9 @@ __device__ __forceinline__ void tile_gemm(const float *XT, int K, const float *W
             float o[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) o[i] = act_f(act, acc[i][j]);
-            float *yp = YT + (cg * 8 + j) * kRows + rg * 8;
+            float *yp = YT + (cg * 8 + j) * kRows + rg * 4;
             *reinterpret_cast<float4 *>(yp) = make_float4(o[0], o[1], o[2], o[3]);
-            *reinterpret_cast<float4 *>(yp + 4) = make_float4(o[4], o[5], o[6], o[7]);
+            *reinterpret_cast<float4 *>(yp + hoff) = make_float4(o[4], o[5], o[6], o[7]);
         }
     }
 }
@@ -340,7 +353,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
         const int valid = (int)min((long long)kPT, P - p0);
         load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
         __syncthreads();
-        tile_descriptor_row<Cfg>(R, t, g, c.dx, c.dteta, inv_rc, bufA, kRows);
+        tile_descriptor_row<Cfg>(R, t, g, c.dx, c.dteta, inv_rc, bufA, kRows, act_col(threadIdx.x));
         __syncthreads();
         float *X = bufA, *Y = bufB;
         for (int L2 = 0; L2 + 1 < net.n_layers; ++L2) {
@@ -354,7 +367,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
             const int Ll = net.n_layers - 1, K = net.dims[Ll];
             const float *wl = wt + net.wt_off[Ll];
             float acc = wt[net.b_off[Ll]];
-            for (int k = 0; k < K; ++k) acc = fmaf(wl[k * net.npad[Ll]], X[k * kRows + threadIdx.x], acc);
+            const int col = act_col(threadIdx.x);
+            for (int k = 0; k < K; ++k) acc = fmaf(wl[k * net.npad[Ll]], X[k * kRows + col], acc);
             e[threadIdx.x] = acc;
         }
         __syncthreads();
