@@ -49,6 +49,13 @@ LAUNCHES = {"amlp_nlist_build": 11, "amlp_pair_filter": 2, "amlp_forces_fd": 1, 
             "amlp_nvt_step_two": 2, "amlp_nvt_step_one": 1}
 
 
+# DRAM bytes (read + written) per filtered pair of one force launch, from an ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum at 32,768 cube26 bodies (436,636 pairs; the kernels'
+# profiles give the command). The traffic grows with the pairs (a capture at 131,072 bodies gave the
+# same bytes per pair), so the roofline's traffic is this figure times the launch's pairs.
+DRAM_BYTES_PER_PAIR = {"adjoint": 5.330432e6 / 436636, "fd": 5.318912e6 / 436636}
+
+
 def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS) -> float:
     """Algorithmic FLOPs per filtered pair: descriptor F_d = 573 Nd + 432 per
     cloud evaluation (spherical-harmonic form), net F_n = 2 (sum of layer
@@ -352,7 +359,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         achieved = fl_pair * r["P"] / (r["force_ms"] / 1e3) / 1e12
         return {"value": world * N_BODIES * args.steps / (r["total_ms"] / 1e3), "ms_per_step": r["total_ms"] / args.steps,
                 "roofline": {"bound": "fp32", "kernel": "k_forces_" + m, "achieved": achieved, "peak": fp32_peak,
-                             "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                             "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                             "traffic": DRAM_BYTES_PER_PAIR[m] * r["P"], "traffic_unit": "bytes per launch (ncu, "
+                             "scaled by pairs from 32,768 bodies)",
                              "flops_per_pair": fl_pair, "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
                              "force_share_of_step": r["force_share"],
                              "peak_source": f"nominal FP32 SIMT 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz (no measured "
