@@ -76,33 +76,58 @@ __device__ __forceinline__ float act_dfast(int act, float z) {
     return df;
 }
 
-// Derivative of f_n with respect to the distance d, together with f_n.
+// Radial basis f_n of the adjoint kernels, with the cutoff function from the
+// hardware sine/cosine (__sincosf: a few 1e-7 absolute error for the
+// arguments here, far below the tensor-core net's 1e-5), used by both their
+// forward and their backward so that the forces stay the exact derivative of
+// the energy they compute.
+template <int NR>
+__device__ __forceinline__ void radial_basis_fast(float d, float inv_rc, float *f) {
+    const float u = d * inv_rc, um1 = u - 1.0f;
+    const float x = fmaf(2.0f * um1, um1, -1.0f);
+    float s, c;
+    __sincosf(3.14159265358979f * u, &s, &c);
+    const float hfc = fmaf(0.25f, c, 0.25f);  // fc / 2
+    float tm1 = 1.0f, t = x;
+    f[0] = 2.0f * hfc;
+    if (NR > 1) f[1] = fmaf(hfc, x, hfc);
+#pragma unroll
+    for (int n = 2; n < NR; ++n) {
+        const float tn = fmaf(2.0f * x, t, -tm1);
+        tm1 = t;
+        t = tn;
+        f[n] = fmaf(hfc, tn, hfc);
+    }
+}
+
+// Derivative of f_n with respect to the distance d, together with f_n (same
+// arithmetic as radial_basis_fast for f_n).
 template <int NR>
 __device__ __forceinline__ void radial_basis_grad(float d, float inv_rc, float *f, float *df) {
-    float u = d * inv_rc;
-    float x = fmaf(2.0f * (u - 1.0f), (u - 1.0f), -1.0f);
-    float dx = 4.0f * (u - 1.0f) * inv_rc;                  // dx/dd
+    const float u = d * inv_rc, um1 = u - 1.0f;
+    const float x = fmaf(2.0f * um1, um1, -1.0f);
     float s, c;
-    sincospif(u, &s, &c);
-    float fc = 0.5f * (1.0f + c);
-    float dfc = -0.5f * 3.14159265358979f * s * inv_rc;     // dfc/dd
-    float tm1 = 1.0f, t = x, dtm1 = 0.0f, dt = 1.0f;        // T_n and dT_n/dx
-    f[0] = fc;
-    df[0] = dfc;
+    __sincosf(3.14159265358979f * u, &s, &c);
+    const float hfc = fmaf(0.25f, c, 0.25f);                        // fc / 2
+    const float hdfc = -0.25f * 3.14159265358979f * s * inv_rc;      // (dfc/dd) / 2
+    const float hdxfc = 4.0f * um1 * inv_rc * hfc;                   // (dx/dd) fc / 2
+    float tm1 = 1.0f, t = x, dtm1 = 0.0f, dt = 1.0f;                // T_n and dT_n/dx
+    f[0] = 2.0f * hfc;
+    df[0] = 2.0f * hdfc;
     if (NR > 1) {
-        f[1] = 0.5f * (1.0f + x) * fc;
-        df[1] = 0.5f * (dx * fc + (1.0f + x) * dfc);
+        f[1] = fmaf(hfc, x, hfc);
+        df[1] = fmaf(hdfc, x, hdfc) + hdxfc;
     }
 #pragma unroll
     for (int n = 2; n < NR; ++n) {
-        float tn = fmaf(2.0f * x, t, -tm1);
-        float dtn = 2.0f * t + fmaf(2.0f * x, dt, -dtm1);
+        const float tn = fmaf(2.0f * x, t, -tm1);
+        const float dtn = fmaf(2.0f * x, dt, fmaf(2.0f, t, -dtm1));
         tm1 = t;
         t = tn;
         dtm1 = dt;
         dt = dtn;
-        f[n] = 0.5f * (1.0f + tn) * fc;
-        df[n] = 0.5f * (dtn * dx * fc + (1.0f + tn) * dfc);
+        f[n] = fmaf(hfc, tn, hfc);
+        df[n] = fmaf(dtn, hdxfc, fmaf(hdfc, tn, hdfc));
     }
 }
 
@@ -184,7 +209,7 @@ __device__ __forceinline__ void accumulate_A(const float *Ri, const float *Rj, f
         float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
         float inv_d = rsqrtf(d2);
         float f[Cfg::NR];
-        radial_basis<Cfg::NR>(d2 * inv_d, inv_rc, f);
+        radial_basis_fast<Cfg::NR>(d2 * inv_d, inv_rc, f);
 #pragma unroll
         for (int n = 0; n < Cfg::NR; ++n) R[n] += f[n];
         float Y[Cfg::K];
