@@ -404,16 +404,20 @@ __device__ __forceinline__ void store_split8(char *tile_hi, int K, int p, int c0
     *reinterpret_cast<uint4 *>(tile_hi + kAP * K * 2 + off) = *reinterpret_cast<uint4 *>(lo);
 }
 
-// Rotated body points of the tile's pairs into S.R from the orientations in S.q.
+// Rotated body points of the tile's pairs into S.R from the orientations in S.q:
+// thread (q, body) = (tid % kAP, tid / kAP) rotates all points of one body of
+// one pair (orientation in registers, body points broadcast from shared
+// memory, rows of odd stride rs: no bank conflicts, no index divisions).
 __device__ __forceinline__ void rotate_tile(const AdjShared &S, int npts, int rs) {
-    const int nd = 2 * npts;
-    for (int idx = threadIdx.x; idx < kAP * nd; idx += blockDim.x) {
-        int q = idx / nd, rem = idx - q * nd, body = rem / npts, a = rem - body * npts;
-        float3 r = rotate_ref(S.q[2 * q + body], make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
-        float *dst = S.R + q * rs + body * 3 * npts + 3 * a;
-        dst[0] = r.x;
-        dst[1] = r.y;
-        dst[2] = r.z;
+    static_assert(kAThreads == 2 * kAP, "one thread per (pair, body)");
+    const int q = threadIdx.x & (kAP - 1), body = threadIdx.x / kAP;
+    const float4 qq = S.q[2 * q + body];
+    float *dst = S.R + q * rs + body * 3 * npts;
+    for (int a = 0; a < npts; ++a) {
+        float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
+        dst[3 * a] = r.x;
+        dst[3 * a + 1] = r.y;
+        dst[3 * a + 2] = r.z;
     }
 }
 

@@ -17,6 +17,7 @@ namespace amlp {
 constexpr int kPT = 32;             // pairs per tile
 constexpr int kRows = 10 * kPT;     // rows (pair-variants) per tile
 constexpr int kTileThreads = kRows;  // one thread per row
+static_assert(kTileThreads % (2 * kPT) == 0, "whole (pair, body) groups per thread stride");
 
 struct TileGeom {
     int npts, nd, rs;  // points per body, points per cloud, floats per pair in R (odd)
@@ -52,14 +53,15 @@ __device__ void load_tile(const float *pos, const float *quat, float L, const in
         ij[2 * p + 1] = j;
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kPT * g.nd; idx += nthr) {
-        int p = idx / g.nd, rem = idx - p * g.nd;
-        int body = rem / g.npts, a = rem - body * g.npts;
-        float3 r = rotate_ref(qs[2 * p + body], make_float3(pts_s[3 * a], pts_s[3 * a + 1], pts_s[3 * a + 2]));
-        float *dst = R + p * g.rs + body * 3 * g.npts + 3 * a;
-        dst[0] = r.x;
-        dst[1] = r.y;
-        dst[2] = r.z;
+    // thread -> (pair, body) = tid % 64 and a stride of points tid / 64 (no index divisions)
+    const int pb = threadIdx.x & (2 * kPT - 1), p = pb >> 1, body = pb & 1;
+    const float4 qq = qs[2 * p + body];
+    float *dst = R + p * g.rs + body * 3 * g.npts;
+    for (int a = threadIdx.x / (2 * kPT); a < g.npts; a += nthr / (2 * kPT)) {
+        float3 r = rotate_ref(qq, make_float3(pts_s[3 * a], pts_s[3 * a + 1], pts_s[3 * a + 2]));
+        dst[3 * a] = r.x;
+        dst[3 * a + 1] = r.y;
+        dst[3 * a + 2] = r.z;
     }
 }
 
