@@ -131,11 +131,11 @@ __device__ __forceinline__ void radial_basis_grad(float d, float inv_rc, float *
     }
 }
 
-// Harmonics and their gradients as polynomials of (x, y, z) (before the
-// projection onto the sphere's tangent plane).
+// The recurrences behind the harmonics: C_m + i S_m = (x + i y)^m (m <= LMAX)
+// and Q[l][m] = d^m P_l / dz^m (m <= l + 1 <= LMAX + 1; 0 above l).
 template <int LMAX>
-__device__ __forceinline__ void sh_eval_grad(float x, float y, float z, float *Y, float (*G)[3]) {
-    float C[LMAX + 1], S[LMAX + 1];
+__device__ __forceinline__ void sh_recurrences(float x, float y, float z, float *C, float *S,
+                                               float (&Q)[LMAX + 2][LMAX + 2]) {
     C[0] = 1.0f;
     S[0] = 0.0f;
 #pragma unroll
@@ -143,7 +143,6 @@ __device__ __forceinline__ void sh_eval_grad(float x, float y, float z, float *Y
         C[m] = fmaf(x, C[m - 1], -y * S[m - 1]);
         S[m] = fmaf(x, S[m - 1], y * C[m - 1]);
     }
-    float Q[LMAX + 2][LMAX + 2];  // Q[l][m] = d^m P_l / dz^m (0 for m > l)
 #pragma unroll
     for (int l = 0; l <= LMAX + 1; ++l)
 #pragma unroll
@@ -157,27 +156,13 @@ __device__ __forceinline__ void sh_eval_grad(float x, float y, float z, float *Y
             else Q[l][m] = ((float)(2 * l - 1) * z * Q[l - 1][m] - (float)(l + m - 1) * Q[l - 2][m]) * (1.0f / (float)(l - m));
         }
     }
-#pragma unroll
-    for (int l = 1; l <= LMAX; ++l) {
-        const int base = l * l - 1;
-        Y[base] = Q[l][0];
-        G[base][0] = 0.0f;
-        G[base][1] = 0.0f;
-        G[base][2] = Q[l][1];
-#pragma unroll
-        for (int m = 1; m <= l; ++m) {
-            const float nm = c_shnorm[l][m];
-            const float q = nm * Q[l][m], q1 = nm * Q[l][m + 1], mq = (float)m * q;
-            Y[base + 2 * m - 1] = q * C[m];
-            Y[base + 2 * m] = q * S[m];
-            G[base + 2 * m - 1][0] = mq * C[m - 1];
-            G[base + 2 * m - 1][1] = -mq * S[m - 1];
-            G[base + 2 * m - 1][2] = q1 * C[m];
-            G[base + 2 * m][0] = mq * S[m - 1];
-            G[base + 2 * m][1] = mq * C[m - 1];
-            G[base + 2 * m][2] = q1 * S[m];
-        }
-    }
+}
+
+__host__ __device__ constexpr int sh_m_of(int k) {  // m of harmonic index k (order m = 0, (cos, sin) m = 1..l)
+    return (k + 1 - sh_l_of(k) * sh_l_of(k) + 1) / 2;
+}
+__host__ __device__ constexpr bool sh_is_sin(int k) {
+    return sh_m_of(k) > 0 && ((k + 1 - sh_l_of(k) * sh_l_of(k)) % 2 == 0);
 }
 
 // Point a of cloud 1 (body i at the origin, body j moved by t).
@@ -282,29 +267,66 @@ __device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, 
         float ux = rx * inv_d, uy = ry * inv_d, uz = rz * inv_d;
         float f[Cfg::NR], df[Cfg::NR];
         radial_basis_grad<Cfg::NR>(d, inv_rc, f, df);
-        float Y[Cfg::K], GY[Cfg::K][3];
-        sh_eval_grad<Cfg::LMAX>(ux, uy, uz, Y, GY);
-        float gr = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+        constexpr int LM = Cfg::LMAX;
+        float C[LM + 1], Sn[LM + 1], Q[LM + 2][LM + 2];
+        sh_recurrences<LM>(ux, uy, uz, C, Sn, Q);
+        // this half's harmonics: Y_k = N Q_l^m {C_m, S_m}
+        float Y[KC];
+#pragma unroll
+        for (int kk = 0; kk < KC; ++kk) {
+            const int k = H * KC + kk;
+            if (k < Cfg::K) {
+                const int l = sh_l_of(k), m = sh_m_of(k);
+                const float q = m == 0 ? Q[l][0] : c_shnorm[l][m] * Q[l][m];
+                Y[kk] = m == 0 ? q : q * (sh_is_sin(k) ? Sn[m] : C[m]);
+            } else {
+                Y[kk] = 0.f;
+            }
+        }
+        float gr = 0.f;
 #pragma unroll
         for (int n = 0; n < Cfg::NR; ++n) {
             float s = grad_rad[n];
             if (n < Cfg::NA) {
 #pragma unroll
                 for (int kk = 0; kk < KC; ++kk)
-                    if (H * KC + kk < Cfg::K) s = fmaf(A[n][kk], Y[H * KC + kk], s);
+                    if (H * KC + kk < Cfg::K) s = fmaf(A[n][kk], Y[kk], s);
             }
             gr = fmaf(s, df[n], gr);
         }
+        // gradient of sum_k s_k Y_k grouped by m: with U_m, V_m the sums of
+        // s N m Q_l^m over the cos / sin harmonics of order m and Wc_m, Ws_m those
+        // of s N Q_l^(m+1),
+        //   gx = sum_m U_m C_(m-1) + V_m S_(m-1), gy = sum_m V_m C_(m-1) - U_m S_(m-1),
+        //   gz = sum_m Wc_m C_m + Ws_m S_m.
+        float U[LM + 1], V[LM + 1], Wc[LM + 1], Ws[LM + 1];
+#pragma unroll
+        for (int m = 0; m <= LM; ++m) U[m] = V[m] = Wc[m] = Ws[m] = 0.f;
 #pragma unroll
         for (int kk = 0; kk < KC; ++kk) {
-            if (H * KC + kk < Cfg::K) {
+            const int k = H * KC + kk;
+            if (k < Cfg::K) {
                 float s = 0.f;
 #pragma unroll
                 for (int n = 0; n < Cfg::NA; ++n) s = fmaf(A[n][kk], f[n], s);
-                gx = fmaf(s, GY[H * KC + kk][0], gx);
-                gy = fmaf(s, GY[H * KC + kk][1], gy);
-                gz = fmaf(s, GY[H * KC + kk][2], gz);
+                const int l = sh_l_of(k), m = sh_m_of(k);
+                const float nrm = m == 0 ? 1.0f : c_shnorm[l][m];
+                const float wq = nrm * Q[l][m + 1];
+                if (sh_is_sin(k)) {
+                    V[m] = fmaf(s, (float)m * nrm * Q[l][m], V[m]);
+                    Ws[m] = fmaf(s, wq, Ws[m]);
+                } else {
+                    if (m > 0) U[m] = fmaf(s, (float)m * nrm * Q[l][m], U[m]);
+                    Wc[m] = fmaf(s, wq, Wc[m]);
+                }
             }
+        }
+        float gx = 0.f, gy = 0.f, gz = Wc[0];
+#pragma unroll
+        for (int m = 1; m <= LM; ++m) {
+            gx = fmaf(U[m], C[m - 1], fmaf(V[m], Sn[m - 1], gx));
+            gy = fmaf(V[m], C[m - 1], fmaf(-U[m], Sn[m - 1], gy));
+            gz = fmaf(Wc[m], C[m], fmaf(Ws[m], Sn[m], gz));
         }
         // dE/dr = gr rhat + (g - rhat (rhat . g)) / d
         float dot = ux * gx + uy * gy + uz * gz;

@@ -43,6 +43,20 @@ DT = 0.005
 KT = 1.0
 METRIC = "particle-steps/s"
 WORKLOAD = "nvt-step-131072-cube26-phi0.45-mlp47x64x64x1-tanh"
+SHAPE = "cube26"
+NET = "xavier"
+
+# The other large configurations, measured with --workload (the default is the cube workload above):
+# 65,536 regular tetrahedra of 16 points (differentiation workload, Xavier net with its output layer
+# scaled by 0.05) and 262,144 twisted cylinders (precision workload, the trained net of
+# tests/golden/make_cyl24_potential.py). Their nets are 128 wide, so the tuned path is the
+# three-kernel adjoint and the fused plain kernel (widths <= 64) does not apply.
+WORKLOADS = {
+    "cube26": dict(n=131072, shape="cube26", phi=0.45, seed=1, widths=(64, 64), act="tanh", net="xavier"),
+    "tetra16": dict(n=65536, shape="tetra16", phi=0.40, seed=2, widths=(128, 128, 128), act="silu",
+                    net="xavier_out0.05"),
+    "cyl24": dict(n=262144, shape="cyl24", phi=0.35, seed=3, widths=(128, 128), act="silu", net="trained"),
+}
 
 # kernels launched by each libamlp entry point (for the gpu_launches count)
 LAUNCHES = {"amlp_nlist_build": 11, "amlp_pair_filter": 2, "amlp_forces_fd": 1, "amlp_forces_adjoint": 1,
@@ -167,6 +181,9 @@ def cpu_step_sample(state, steps: int = 3):
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
+    if SHAPE != "cube26":
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU arm is timed on the cube26 benchmark workload"}))
+        return
     from amlp.configs import make_state
     state = make_state(N_BODIES, "cube26", PHI, kT=KT, seed=SEED)
     ref = CpuReferenceStep(state)
@@ -198,6 +215,9 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
     launches = [0]
     entry = "amlp_forces_" + ("fd" if method == "fd" else "adjoint")
+    wide = method != "fd" and system.adj_ws is not None  # nets wider than 64: the three-kernel adjoint
+    if wide:
+        entry = "amlp_forces_adjoint_wide"
 
     def one_step(ev_force=None):
         if system.timestep % system.nlist_every == 0 and system.timestep > 0:
@@ -209,15 +229,19 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
         system.filter_pairs()
         if ev_force is not None:
             ev_force[0].record(stream)
-        _lib.call(entry, system.pos.data_ptr(), system.quat.data_ptr(), system.L, system.fpairs.data_ptr(),
-                  system.nf.data_ptr(), system.cap, ctypes.byref(system.nep), ctypes.byref(system.net.struct),
-                  system.F.data_ptr(), system.T.data_ptr(), system._pe_ptr(), stream.cuda_stream)
+        args = [system.pos.data_ptr(), system.quat.data_ptr(), system.L, system.fpairs.data_ptr(),
+                system.nf.data_ptr(), system.cap, ctypes.byref(system.nep), ctypes.byref(system.net.struct),
+                system.F.data_ptr(), system.T.data_ptr(), system._pe_ptr()]
+        if wide:
+            args += [system.adj_ws.data_ptr(), system.adj_ws.numel()]
+        _lib.call(entry, *args, stream.cuda_stream)
         if ev_force is not None:
             ev_force[1].record(stream)
         system.integrate_step_two()
         system.integrate_step_one()
         system.timestep += 1
-        launches[0] += LAUNCHES["amlp_pair_filter"] + 1 + LAUNCHES["amlp_nvt_step_two"] + LAUNCHES["amlp_nvt_step_one"]
+        launches[0] += (LAUNCHES["amlp_pair_filter"] + (3 if wide else 1) + LAUNCHES["amlp_nvt_step_two"] +
+                        LAUNCHES["amlp_nvt_step_one"])
 
     for _ in range(warmup):
         one_step()
@@ -322,6 +346,22 @@ def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) 
             "served_over_sequential_plain": stats["particle_steps_per_s"] / seq_rate}
 
 
+def make_net(dev):
+    """The workload's net: seeded Xavier weights, the same with the output layer scaled by 0.05, or the
+    trained cylinder net."""
+    import numpy as np
+    from amlp.engine import EnergyNet
+    if NET == "trained":
+        z = np.load(DRIFT_MODEL)
+        return EnergyNet([(z[f"W{k}"], z[f"b{k}"]) for k in range(len(z.files) // 2)], ACT, dev)
+    net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device="cpu")
+    layers = list(net.layers)
+    if NET == "xavier_out0.05":
+        W, b = layers[-1]
+        layers[-1] = (W * np.float32(0.05), b)
+    return EnergyNet(layers, ACT, dev)
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     import torch
     from amlp.configs import make_state
@@ -334,16 +374,18 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    state = make_state(N_BODIES, "cube26", PHI, kT=KT, seed=SEED)
-    net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device=dev)
+    state = make_state(N_BODIES, SHAPE, PHI, kT=KT, seed=SEED)
+    net = make_net(dev)
     methods = ["adjoint", "fd"] if args.method == "both" else [args.method]
+    if max(WIDTHS) > 64:
+        methods = ["adjoint"]  # the fused plain kernel takes widths up to 64
     peaks = measured_peaks()
     clk_mhz = peaks["sm_max_mhz"] or 1965.0
     fp32_peak = 148 * 128 * 2 * clk_mhz * 1e6 / 1e12
     results = {}
     clocks = ClockSampler(local_rank)
     for m in methods:
-        system = System(state, "cube26", Hypers(), net, kT=KT, dt=DT, device=dev)
+        system = System(state, SHAPE, Hypers(), net, kT=KT, dt=DT, device=dev)
         r = _measure(system, m, args.steps, args.warmup, dist, dev)
         e2e_steps = max(3, min(args.steps, 20))
         r["e2e_ms"], r["e2e_bytes"] = _e2e(system, m, e2e_steps, dist, dev)
@@ -355,12 +397,14 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
 
     def summary(m):
         r = results[m]
-        fl_pair = algorithmic_flops_per_pair(m)
+        from amlp.shapes import get_shape
+        fl_pair = algorithmic_flops_per_pair(m, nd=get_shape(SHAPE).nd, widths=WIDTHS)
         achieved = fl_pair * r["P"] / (r["force_ms"] / 1e3) / 1e12
         return {"value": world * N_BODIES * args.steps / (r["total_ms"] / 1e3), "ms_per_step": r["total_ms"] / args.steps,
-                "roofline": {"bound": "fp32", "kernel": "k_forces_" + m, "achieved": achieved, "peak": fp32_peak,
+                "roofline": {"bound": "fp32",
+                             "kernel": "k_forces_" + m if max(WIDTHS) <= 64 else "k_adj_desc x2 + k_mlp_grad", "achieved": achieved, "peak": fp32_peak,
                              "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                             "traffic": DRAM_BYTES_PER_PAIR[m] * r["P"], "traffic_unit": "bytes per launch (ncu, "
+                             "traffic": DRAM_BYTES_PER_PAIR[m] * r["P"] if SHAPE == "cube26" else None, "traffic_unit": "bytes per launch (ncu, "
                              "scaled by pairs from 32,768 bodies)",
                              "flops_per_pair": fl_pair, "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
                              "force_share_of_step": r["force_share"],
@@ -389,9 +433,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                          "roofline": ps["roofline"], "e2e": ps["e2e"]}
         line["tuned_over_plain"] = hs["value"] / ps["value"]
         line["gpu_launches"] += ps["gpu_launches"]
-    if rank == 0 and world == 1 and not args.no_serving:
+    if rank == 0 and world == 1 and not args.no_serving and SHAPE == "cube26":
         line["serving"] = run_serving(dev)
-    if rank == 0 and not args.no_cpu_baseline and world == 1:
+    if rank == 0 and not args.no_cpu_baseline and world == 1 and SHAPE == "cube26":
         from amlp.configs import make_state as _ms
         t_cpu, sample, _ = cpu_step_sample(_ms(N_BODIES, "cube26", PHI, kT=KT, seed=SEED))
         line["cpu_baseline"] = {"value": N_BODIES / t_cpu, "unit": "particle-steps/s", "cores": os.cpu_count() or 1,
@@ -493,6 +537,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--bodies", type=int, default=N_BODIES,
                     help="system size (the benchmark workload is 131072; smaller sizes are for profiling)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cube26",
+                    help="cube26 is the benchmark; tetra16 and cyl24 are the differentiation and precision workloads")
     ap.add_argument("--drift", action="store_true",
                     help="NVE energy drift of the 262,144-cylinder precision workload instead of the benchmark")
     ap.add_argument("--drift-steps", type=int, default=10000)
@@ -503,6 +549,15 @@ def main():
     ap.add_argument("--drift-equil", type=int, default=2000, help="NVT steps before the NVE runs")
     ap.add_argument("--drift-model", default=DRIFT_MODEL)
     args = ap.parse_args()
+    if args.workload != "cube26":
+        w = WORKLOADS[args.workload]
+        g = globals()
+        g.update(N_BODIES=w["n"], SHAPE=w["shape"], PHI=w["phi"], SEED=w["seed"], WIDTHS=w["widths"],
+                 ACT=w["act"], NET=w["net"])
+        g["WORKLOAD"] = (f"nvt-step-{w['n']}-{w['shape']}-phi{w['phi']:.2f}-mlp47x" +
+                         "x".join(str(x) for x in w["widths"]) + f"x1-{w['act']}")
+        if args.bodies == 131072:
+            args.bodies = w["n"]
     if args.drift:
         run_drift(args, int(os.environ.get("LOCAL_RANK", 0)))
         return
