@@ -45,7 +45,8 @@ struct AdjNet {
     int nout[kMaxHidden + 1];       // padded output width of hidden layer k (multiple of 16)
     int dims[kMaxHidden + 2];       // true dims: D, h1, .., h_nh, 1
     long long woff[kMaxHidden + 1];  // offset of W_k in the packed global weights (k = 0..nh)
-    int wsm_off[kMaxHidden];        // byte offset of W_k (hi) in the weight area; lo follows
+    int wsm_off[kMaxHidden];        // byte offset of W_k (hi) in the weight area; lo follows (the wide
+                                    // path: in the pre-split global copy of the weights)
     int wsm_total;                  // bytes of the weight area
     int bias_off[kMaxHidden + 1];   // float offsets of b_k in the fp32 parameter area; last = w_last
     int par_total;
@@ -823,6 +824,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
 // ============================================================================
 constexpr int kWideMax = 128;
 constexpr int kGP = 48;  // padded descriptor width in the workspace rows
+constexpr size_t kWeightSplitBytes = (size_t)kMaxHidden * kWideMax * kWideMax * 4;  // bf16 hi/lo of every layer
 
 // Per-pair force/torque from the two halves' partial sums, scaled, clipped
 // (unless clip == 0), then scattered with runs of equal i summed in the warp
@@ -1037,13 +1039,38 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
     }
 }
 
+// The hidden layers' weights split into bf16 hi/lo once per launch, in the
+// K-major layout of the shared-memory operand (per layer: hi, then lo), so that
+// k_mlp_grad loads a layer with one bulk copy.
+__global__ void k_split_weights(AdjNet net, const float *w, char *dst) {
+    for (int L2 = 0; L2 < net.nh; ++L2) {
+        const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
+        const float *W = w + net.woff[L2];
+        char *hi = dst + net.wsm_off[L2], *lo = hi + (size_t)Np * Kp * 2;
+        for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < Np * Kp; idx += gridDim.x * blockDim.x) {
+            int n = idx / Kp, k = idx - n * Kp;
+            float v = (n < N && k < K) ? W[(size_t)n * K + k] : 0.f;
+            __nv_bfloat16 a, bb;
+            tc::split_bf16(v, a, bb);
+            uint32_t o = tc::kmajor_offset(n, k, Kp);
+            *reinterpret_cast<__nv_bfloat16 *>(hi + o) = a;
+            *reinterpret_cast<__nv_bfloat16 *>(lo + o) = bb;
+        }
+    }
+}
+
 // Net forward and backward over rows of g on the tensor cores (bf16x3 splits,
-// fp32 TMEM accumulators). Weights are staged into shared memory one layer at
-// a time. Outputs per row: y = net(g) and dE/dg (kGP floats).
+// fp32 TMEM accumulators). One layer's weights at a time sit in shared memory,
+// brought in by a bulk copy from the pre-split copy (k_split_weights) that
+// thread 0 starts as soon as the previous layer's MMAs are done, so it overlaps
+// the epilogue; the layer order fwd 0..nh-1, bwd nh-1..0 reuses the last
+// forward layer and, across tiles, layer 0. Outputs per row: y = net(g) and
+// dE/dg (kGP floats).
 __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
-                                                          AdjNet net, const float *w, float *y_rows, float *dg_rows) {
+                                                          AdjNet net, const float *w, const char *wsplit,
+                                                          float *y_rows, float *dg_rows) {
     extern __shared__ __align__(128) char smem_raw[];
-    __shared__ uint64_t mbar;
+    __shared__ uint64_t mbar, wbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5;
@@ -1067,6 +1094,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
     if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);
     if (tid == 0) {
         tc::mbar_init(&mbar, 1);
+        tc::mbar_init(&wbar, 1);
         abort_flag = 0;
     }
     tc::fence_before();
@@ -1084,22 +1112,33 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
         phase ^= 1u;
         tc::fence_after();
     };
-    // stage layer L's weights, bf16 hi/lo, K-major (rows = outputs)
-    auto stage = [&](int L2) {
-        const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
-        const float *W = w + net.woff[L2];
-        char *lo = wbuf + (size_t)Np * Kp * 2;
-        for (int idx = tid; idx < Np * Kp; idx += kAThreads) {
-            int n = idx / Kp, k = idx - n * Kp;
-            float v = (n < N && k < K) ? __ldg(W + (size_t)n * K + k) : 0.f;
-            __nv_bfloat16 a, bb;
-            tc::split_bf16(v, a, bb);
-            uint32_t o = tc::kmajor_offset(n, k, Kp);
-            *reinterpret_cast<__nv_bfloat16 *>(wbuf + o) = a;
-            *reinterpret_cast<__nv_bfloat16 *>(lo + o) = bb;
+    // weights: `in_buf` (tracked identically by every thread) is the layer whose
+    // weights are in wbuf or on their way; thread 0 starts the copies and waits
+    // for them before its MMAs.
+    int in_buf = -1;
+    bool w_pending = false;
+    uint32_t wphase = 0;
+    const uint32_t wb_u32 = tc::smem_u32(wbuf), wbar_u32 = tc::smem_u32(&wbar);
+    auto request = [&](int L2) {
+        if (L2 == in_buf) return;
+        in_buf = L2;
+        if (tid == 0 && !abort_flag) {
+            const uint32_t bytes = (uint32_t)(4 * net.nout[L2] * net.kin[L2]);
+            tc::mbar_arrive_expect_tx(wbar_u32, bytes);
+            tc::bulk_g2s(wb_u32, wsplit + net.wsm_off[L2], bytes, wbar_u32);
+            w_pending = true;
         }
-        tc::fence_async_smem();
     };
+    auto ensure = [&]() {  // thread 0 only
+        if (!w_pending) return;
+        if (!tc::mbar_wait(wbar_u32, wphase)) {
+            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
+            abort_flag = 1;
+        }
+        wphase ^= 1u;
+        w_pending = false;
+    };
+    request(0);
     const long long P = min(*d_np, cap);
     const long long ntiles = (P + kAP - 1) / kAP;
     const int Kg = net.kin[0];
@@ -1114,9 +1153,10 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
         }
         for (int L2 = 0; L2 < net.nh; ++L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
-            stage(L2);
+            request(L2);
             tc::fence_async_smem();
             __syncthreads();
+            if (tid == 0) ensure();
             if (tid == 0 && !abort_flag) {
                 tc::fence_after();
                 mma3(tmem + (uint32_t)(L2 * kWideMax), tile(L2), Kp, wbuf, (size_t)Np * Kp * 2, Np, false, 256, 128,
@@ -1124,6 +1164,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
                 tc::commit(bar);
             }
             wait_mma();
+            if (L2 + 1 < net.nh) request(L2 + 1);  // overlaps this layer's epilogue
             const bool last = L2 == net.nh - 1;
             const float *bias = par + net.bias_off[L2];
             const float *wl = par + net.bias_off[net.nh];
@@ -1152,9 +1193,10 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
         if (tid < kAP && p < valid) y_rows[r0 + p] = eps[p] + eps[kAP + p] + par[net.bias_off[net.nh] + kWideMax];
         for (int L2 = net.nh - 1; L2 >= 0; --L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
-            stage(L2);
+            request(L2);
             tc::fence_async_smem();
             __syncthreads();
+            if (tid == 0) ensure();
             if (tid == 0 && !abort_flag) {
                 tc::fence_after();
                 mma3(tmem + bcol, tile(L2 + 1), Np, wbuf, (size_t)Np * Kp * 2, Kp, true, 2 * Kp * 16,
@@ -1162,6 +1204,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
                 tc::commit(bar);
             }
             wait_mma();
+            request(L2 > 0 ? L2 - 1 : 0);  // the next layer needed (layer 0 again for the next tile)
             if (L2 > 0) {
                 const float *bias = par + net.bias_off[L2 - 1];
                 for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
@@ -1188,6 +1231,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
         if (abort_flag) break;
     }
     if (abort_flag && tid == 0) tc::mbar_wait(bar, phase);
+    if (tid == 0) ensure();  // no copy may still be writing shared memory at exit
     __syncthreads();
     if (warp == 0) {
         tc::fence_after();
@@ -1305,6 +1349,8 @@ static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
         net->nout[k] = (mlp->dims[k + 1] + 15) / 16 * 16;
         net->bias_off[k] = par;
         par += net->nout[k];
+        net->wsm_off[k] = net->wsm_total;  // pre-split weights of layer k: hi then lo
+        net->wsm_total += 4 * net->nout[k] * net->kin[k];
     }
     net->bias_off[nh] = par;
     par += kWideMax + 4;
@@ -1314,7 +1360,7 @@ static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
 
 extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes) {
     if (cap < 0 || !bytes) return AMLP_ERR_INVALID_ARG;
-    *bytes = align_up((size_t)cap * kGP * 4) * 2 + align_up((size_t)cap * 4) + 256;
+    *bytes = align_up((size_t)cap * kGP * 4) * 2 + align_up((size_t)cap * 4) + align_up(kWeightSplitBytes) + 256;
     return AMLP_OK;
 }
 
@@ -1353,6 +1399,7 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     float *g_rows = c.take<float>((size_t)cap * kGP);
     float *dg_rows = c.take<float>((size_t)cap * kGP);
     float *y_rows = c.take<float>((size_t)cap);
+    char *wsplit = c.take<char>(kWeightSplitBytes);
     const int npts = nep->npts;
     const size_t smem_desc = wide_desc_smem(npts);
     const size_t smem_mlp = (size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
@@ -1370,7 +1417,8 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     fwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, g_rows, kGP, nullptr, nullptr, nullptr, clip, d_F,
                                              d_T, d_pe, d_rep, d_rp);
-    k_mlp_grad<<<kNumSM, kAThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, y_rows, dg_rows);
+    k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
+    k_mlp_grad<<<kNumSM, kAThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
     bwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, nullptr, kGP, dg_rows, y_rows, d_wt, clip, d_F, d_T,
                                              d_pe, d_rep, d_rp);

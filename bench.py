@@ -240,7 +240,7 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
         system.integrate_step_two()
         system.integrate_step_one()
         system.timestep += 1
-        launches[0] += (LAUNCHES["amlp_pair_filter"] + (3 if wide else 1) + LAUNCHES["amlp_nvt_step_two"] +
+        launches[0] += (LAUNCHES["amlp_pair_filter"] + (4 if wide else 1) + LAUNCHES["amlp_nvt_step_two"] +
                         LAUNCHES["amlp_nvt_step_one"])
 
     for _ in range(warmup):
