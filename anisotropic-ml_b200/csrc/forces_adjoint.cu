@@ -825,6 +825,11 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
 constexpr int kWideMax = 128;
 constexpr int kGP = 48;  // padded descriptor width in the workspace rows
 constexpr size_t kWeightSplitBytes = (size_t)kMaxHidden * kWideMax * kWideMax * 4;  // bf16 hi/lo of every layer
+constexpr size_t kAdjAFloats = 2 * 9 * 12;  // harmonic sums per pair kept between the passes (two halves of 9 x 12)
+
+__host__ __device__ inline size_t adj_a_bytes(long long cap) {
+    return (size_t)((cap + 127) / 128) * 128 * kAdjAFloats * 4;
+}
 
 // Per-pair force/torque from the two halves' partial sums, scaled, clipped
 // (unless clip == 0), then scattered with runs of equal i summed in the warp
@@ -933,8 +938,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
                                                           float en_range, float *g_rows, int g_ld,
                                                           const float *dg_rows, const float *y_rows, const float *wt,
                                                           int clip, float *F, float *T, double *pe, const int *rep,
-                                                          const amlp_replica *rp) {
+                                                          const amlp_replica *rp, float *a_rows) {
     constexpr int KC = Half<Cfg>::KC;
+    static_assert(2 * Cfg::NA * KC == kAdjAFloats, "harmonic sums per pair in the workspace");
     extern __shared__ __align__(128) char smem_raw[];
     __shared__ double pe_s[kAThreads / 32];
     __shared__ float psum_s[3];
@@ -1002,9 +1008,26 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             c.y *= inv;
             c.z *= inv;
         }
+        // this thread's harmonic sums: computed by the forward pass (and stored
+        // for the backward pass when a_rows is given), read back by the backward
+        // pass; layout [tile][half][n][kk][pair] so that a warp's accesses coalesce
         float A[Cfg::NA][KC];
-        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, A);
-        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGS, A);
+        float *a_tile = a_rows ? a_rows + ((size_t)tile * 2 + h) * (Cfg::NA * KC) * kAP + p : nullptr;
+        if (!BWD || !a_rows) {
+            if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, A);
+            else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGS, A);
+            if (!BWD && a_tile) {
+#pragma unroll
+                for (int n = 0; n < Cfg::NA; ++n)
+#pragma unroll
+                    for (int kk = 0; kk < KC; ++kk) a_tile[(n * KC + kk) * kAP] = A[n][kk];
+            }
+        } else {
+#pragma unroll
+            for (int n = 0; n < Cfg::NA; ++n)
+#pragma unroll
+                for (int kk = 0; kk < KC; ++kk) A[n][kk] = a_tile[(n * KC + kk) * kAP];
+        }
         __syncthreads();
         if (!BWD) {
             for (int idx = tid; idx < kAP * g_ld; idx += kAThreads) {
@@ -1360,7 +1383,8 @@ static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
 
 extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes) {
     if (cap < 0 || !bytes) return AMLP_ERR_INVALID_ARG;
-    *bytes = align_up((size_t)cap * kGP * 4) * 2 + align_up((size_t)cap * 4) + align_up(kWeightSplitBytes) + 256;
+    *bytes = align_up((size_t)cap * kGP * 4) * 2 + align_up((size_t)cap * 4) + align_up(kWeightSplitBytes) +
+             align_up(adj_a_bytes(cap)) + 256;
     return AMLP_OK;
 }
 
@@ -1400,6 +1424,7 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     float *dg_rows = c.take<float>((size_t)cap * kGP);
     float *y_rows = c.take<float>((size_t)cap);
     char *wsplit = c.take<char>(kWeightSplitBytes);
+    float *a_rows = c.take<float>(adj_a_bytes(cap) / 4);
     const int npts = nep->npts;
     const size_t smem_desc = wide_desc_smem(npts);
     const size_t smem_mlp = (size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
@@ -1416,12 +1441,12 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mlp));
     fwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, g_rows, kGP, nullptr, nullptr, nullptr, clip, d_F,
-                                             d_T, d_pe, d_rep, d_rp);
+                                             d_T, d_pe, d_rep, d_rp, a_rows);
     k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
     k_mlp_grad<<<kNumSM, kAThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
     bwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, nullptr, kGP, dg_rows, y_rows, d_wt, clip, d_F, d_T,
-                                             d_pe, d_rep, d_rp);
+                                             d_pe, d_rep, d_rp, a_rows);
     return check_launch();
 }
 
@@ -1466,7 +1491,8 @@ extern "C" amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_
     fwd<<<kNumSM, kAThreads, smem, as_stream(stream)>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts,
                                                         nep->npts, 1.0f / nep->nep_cutoff, nep->en_min,
                                                         nep->en_max - nep->en_min, d_g, ld_g, nullptr, nullptr,
-                                                        nullptr, 1, nullptr, nullptr, nullptr, nullptr, nullptr);
+                                                        nullptr, 1, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                        nullptr);
     return check_launch();
 }
 
