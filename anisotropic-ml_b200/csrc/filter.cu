@@ -17,18 +17,50 @@ struct BoxOf {
     float L;
     const int *rep;
     const amlp_replica *rp;
+    int vec;  // the pair list is 16-byte aligned: vector loads allowed
     __device__ __forceinline__ float operator()(int i) const { return rep ? rp[rep[i]].box : L; }
 };
 
-__device__ __forceinline__ bool keep_pair(const float *pos, const int *vp, long long k, BoxOf box, double cutoff) {
+__device__ __forceinline__ bool keep_ij(const float *pos, int i, int j, BoxOf box, double cutoff) {
     float d;
-    int i = vp[2 * k];
-    min_image(pos, i, vp[2 * k + 1], box(i), &d);
+    min_image(pos, i, j, box(i), &d);
     return (double)d < cutoff;
 }
 
+// Each thread takes kFilterItems consecutive pairs per round (two 16-byte loads
+// when the four lie inside the chunk), so a block covers 1024 pairs per round
+// and every thread has four independent position gathers in flight.
+constexpr int kFilterItems = 4;
+constexpr int kFilterRound = kFilterThreads * kFilterItems;
+
+// Bit u set when pair k0 + u (< e) is kept.
+__device__ __forceinline__ unsigned keep_mask(const float *pos, const int *vp, long long k0, long long e, BoxOf box,
+                                              double cutoff, int (&ij)[2 * kFilterItems]) {
+    if (box.vec && k0 + kFilterItems <= e) {
+        const int4 a = *reinterpret_cast<const int4 *>(vp + 2 * k0);
+        const int4 b = *reinterpret_cast<const int4 *>(vp + 2 * k0 + 4);
+        ij[0] = a.x; ij[1] = a.y; ij[2] = a.z; ij[3] = a.w;
+        ij[4] = b.x; ij[5] = b.y; ij[6] = b.z; ij[7] = b.w;
+    } else {
+#pragma unroll
+        for (int u = 0; u < kFilterItems; ++u) {
+            const bool in = k0 + u < e;
+            ij[2 * u] = in ? vp[2 * (k0 + u)] : 0;
+            ij[2 * u + 1] = in ? vp[2 * (k0 + u) + 1] : 0;
+        }
+    }
+    unsigned m = 0;
+#pragma unroll
+    for (int u = 0; u < kFilterItems; ++u)
+        if (k0 + u < e && keep_ij(pos, ij[2 * u], ij[2 * u + 1], box, cutoff)) m |= 1u << u;
+    return m;
+}
+
+// Chunks of whole rounds' alignment (multiples of kFilterItems pairs, so the
+// 16-byte loads are aligned).
 __device__ __forceinline__ void chunk_range(long long nv, long long *s, long long *e) {
     long long chunk = (nv + gridDim.x - 1) / gridDim.x;
+    chunk = (chunk + kFilterItems - 1) / kFilterItems * kFilterItems;
     *s = min(nv, (long long)blockIdx.x * chunk);
     *e = min(nv, *s + chunk);
 }
@@ -38,7 +70,9 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *po
     long long nv = min(*d_nv, cap), s, e;
     chunk_range(nv, &s, &e);
     int c = 0;
-    for (long long k = s + threadIdx.x; k < e; k += blockDim.x) c += keep_pair(pos, vp, k, L, cutoff);
+    int ij[2 * kFilterItems];
+    for (long long k0 = s + (long long)threadIdx.x * kFilterItems; k0 < e; k0 += kFilterRound)
+        c += __popc(keep_mask(pos, vp, k0, e, L, cutoff, ij));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     __shared__ int ws[kFilterThreads / 32];
@@ -69,21 +103,34 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_write(const float *po
     long long base = base_s;
     long long nv = min(*d_nv, cap), s, e;
     chunk_range(nv, &s, &e);
-    for (long long t0 = s; t0 < e; t0 += blockDim.x) {
-        long long k = t0 + threadIdx.x;
-        bool keep = k < e && keep_pair(pos, vp, k, L, cutoff);
-        unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) wsum[w] = __popc(m);
+    int ij[2 * kFilterItems];
+    for (long long r0 = s; r0 < e; r0 += kFilterRound) {
+        const long long k0 = r0 + (long long)threadIdx.x * kFilterItems;
+        const unsigned m = k0 < e ? keep_mask(pos, vp, k0, e, L, cutoff, ij) : 0u;
+        // block-wide exclusive scan of the kept counts (thread order = pair order)
+        const int cnt = __popc(m);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[w] = incl;
         __syncthreads();
-        int before = 0, total = 0;
+        int before = incl - cnt, total = 0;
+#pragma unroll
         for (int q = 0; q < kFilterThreads / 32; ++q) {
             before += q < w ? wsum[q] : 0;
             total += wsum[q];
         }
-        if (keep) {
-            long long o = base + before + __popc(m & ((1u << lane) - 1u));
-            out[2 * o] = vp[2 * k];
-            out[2 * o + 1] = vp[2 * k + 1];
+        long long o = base + before;
+#pragma unroll
+        for (int u = 0; u < kFilterItems; ++u) {
+            if (m & (1u << u)) {
+                out[2 * o] = ij[2 * u];
+                out[2 * o + 1] = ij[2 * u + 1];
+                ++o;
+            }
         }
         base += total;
         __syncthreads();
@@ -110,7 +157,7 @@ extern "C" amlp_status amlp_pair_filter(const float *d_pos, float box, double cu
     cudaStream_t s = as_stream(stream);
     int *counts = static_cast<int *>(d_ws);
     double c = cutoff;
-    BoxOf b{box, nullptr, nullptr};
+    BoxOf b{box, nullptr, nullptr, ((uintptr_t)d_vpairs & 15) == 0};
     k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, c, d_vpairs, d_nverlet, cap_verlet, counts);
     k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, c, d_vpairs, d_nverlet, cap_verlet, counts,
                                                             d_pairs, d_npairs);
@@ -125,7 +172,7 @@ extern "C" amlp_status amlp_multi_pair_filter(const float *d_pos, const int *d_r
     if (!d_ws || ws_bytes < kFilterBlocks * sizeof(int)) return AMLP_ERR_WORKSPACE;
     cudaStream_t s = as_stream(stream);
     int *counts = static_cast<int *>(d_ws);
-    BoxOf b{0.f, d_rep, d_rp};
+    BoxOf b{0.f, d_rep, d_rp, ((uintptr_t)d_vpairs & 15) == 0};
     k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, cutoff, d_vpairs, d_nverlet, cap_verlet, counts);
     k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, cutoff, d_vpairs, d_nverlet, cap_verlet, counts,
                                                             d_pairs, d_npairs);
