@@ -25,7 +25,8 @@ namespace amlp {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
-constexpr int kSortCap = 1024;  // neighbours per body ranked in shared memory
+constexpr int kSortCap = 1024;   // neighbours per body ranked in a warp's shared buffer
+constexpr int kBigCap = 8192;    // up to this many: written unordered, then ranked by one block (k_sort_big)
 
 struct Grid {
     int n, nc;        // bodies, cells per side (1 = one cell holding all bodies)
@@ -127,7 +128,7 @@ __global__ void k_write(Grid g, const double *xd, const int *cell_of, const long
     if (i >= g.n) return;
     long long off = offsets[i];
     int cnt = (int)(offsets[i + 1] - off);
-    if (cnt == 0) return;
+    if (cnt == 0 || off >= cap) return;  // nothing of this body's list fits
     int *b = buf[w];
     if (cnt <= kSortCap) {
         int fill = 0;
@@ -148,8 +149,20 @@ __global__ void k_write(Grid g, const double *xd, const int *cell_of, const long
         }
         return;
     }
-    // More neighbours than the shared buffer holds: emit them in increasing
-    // order by repeated warp-wide minimum (slow, only for pathological inputs).
+    if (cnt <= kBigCap && off + cnt > cap) return;  // crossing cap: k_sort_big writes the part that fits
+    if (cnt <= kBigCap) {
+        // written in candidate order here; k_sort_big ranks the segment afterwards
+        int fill = 0;
+        for_candidates(i, g, xd, cell_of, cell_start, cell_list, [&](int j, bool ok) {
+            unsigned m = __ballot_sync(0xffffffffu, ok);
+            long long o = off + fill + __popc(m & ((1u << lane) - 1u));
+            if (ok && o < cap) pairs[2 * o + 1] = j;
+            fill += __popc(m);
+        });
+        return;
+    }
+    // More neighbours than one block ranks: emit them in increasing order by
+    // repeated warp-wide minimum (slow, only for pathological inputs).
     int prev = i;
     for (int k = 0; k < cnt; ++k) {
         int best = 0x7fffffff;
@@ -163,6 +176,48 @@ __global__ void k_write(Grid g, const double *xd, const int *cell_of, const long
             pairs[2 * (off + k) + 1] = best;
         }
         prev = best;
+    }
+}
+
+// Sorts the segments of bodies with kSortCap < count <= kBigCap: one block per
+// body, every j ranked by counting the smaller ones (the j of a body are
+// distinct), written back with i. k_write left such a segment in candidate
+// order when it fits below cap; the one segment that crosses cap is gathered
+// here (warp 0 walks the neighbouring cells) and only its first cap - off
+// pairs are written, so the pairs that fit are always the head of the list.
+__global__ void __launch_bounds__(256) k_sort_big(Grid g, const double *xd, const int *cell_of,
+                                                  const long long *cell_start, const int *cell_list,
+                                                  const long long *offsets, int *pairs, long long cap,
+                                                  const int *gate) {
+    if (gate && !*gate) return;
+    __shared__ int buf[kBigCap];
+    for (int i = blockIdx.x; i < g.n; i += gridDim.x) {
+        const long long off = offsets[i];
+        const int cnt = (int)(offsets[i + 1] - off);
+        if (cnt <= kSortCap || cnt > kBigCap || off >= cap) continue;
+        const bool crossing = off + cnt > cap;
+        if (!crossing) {
+            for (int e = threadIdx.x; e < cnt; e += blockDim.x) buf[e] = pairs[2 * (off + e) + 1];
+        } else if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            int fill = 0;
+            for_candidates(i, g, xd, cell_of, cell_start, cell_list, [&](int j, bool ok) {
+                unsigned m = __ballot_sync(0xffffffffu, ok);
+                if (ok) buf[fill + __popc(m & ((1u << lane) - 1u))] = j;
+                fill += __popc(m);
+            });
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+            const int j = buf[e];
+            int rank = 0;
+            for (int k = 0; k < cnt; ++k) rank += buf[k] < j;
+            if (off + rank < cap) {
+                pairs[2 * (off + rank)] = i;
+                pairs[2 * (off + rank) + 1] = j;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -276,6 +331,7 @@ amlp_status launch_build(const float *d_pos, const Grid &g, const NlistWs &w, in
     if (st) return st;
     k_write<<<nb, 32 * kWarpsPerBlock, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap,
                                                gate);
+    k_sort_big<<<kNumSM, 256, 0, s>>>(g, w.xd, w.cell_of, w.cell_start, w.cell_list, w.counts, d_pairs, cap, gate);
     k_total<<<1, 1, 0, s>>>(w.counts, n, d_count, gate, cap);
     return check_launch();
 }

@@ -45,16 +45,19 @@ METRIC = "particle-steps/s"
 WORKLOAD = "nvt-step-131072-cube26-phi0.45-mlp47x64x64x1-tanh"
 SHAPE = "cube26"
 NET = "xavier"
+IS_BENCHMARK = True  # the default workload (serving leg, CPU baseline and ncu traffic belong to it)
 
-# The other large configurations, measured with --workload (the default is the cube workload above):
-# 65,536 regular tetrahedra of 16 points (differentiation workload, Xavier net with its output layer
-# scaled by 0.05) and 262,144 twisted cylinders (precision workload, the trained net of
-# tests/golden/make_cyl24_potential.py). Their nets are 128 wide, so the tuned path is the
-# three-kernel adjoint and the fused plain kernel (widths <= 64) does not apply.
+# The other configurations, measured with --workload (the default is the cube workload above): the
+# small 1,000-cube system (packing fraction 0.30, seed 0),
+# 65,536 regular tetrahedra of 16 points (differentiation workload) and 262,144 twisted cylinders
+# (precision workload), both with the soft-repulsion nets trained by
+# tests/golden/make_soft_potential.py (random nets make the dynamics blow up at these sizes). The
+# last two have 128-wide nets, so their tuned path is the wide adjoint and the fused plain kernel
+# (widths <= 64) does not apply.
 WORKLOADS = {
     "cube26": dict(n=131072, shape="cube26", phi=0.45, seed=1, widths=(64, 64), act="tanh", net="xavier"),
-    "tetra16": dict(n=65536, shape="tetra16", phi=0.40, seed=2, widths=(128, 128, 128), act="silu",
-                    net="xavier_out0.05"),
+    "cube1000": dict(n=1000, shape="cube26", phi=0.30, seed=0, widths=(64, 64), act="tanh", net="xavier"),
+    "tetra16": dict(n=65536, shape="tetra16", phi=0.40, seed=2, widths=(128, 128, 128), act="silu", net="trained"),
     "cyl24": dict(n=262144, shape="cyl24", phi=0.35, seed=3, widths=(128, 128), act="silu", net="trained"),
 }
 
@@ -70,17 +73,18 @@ LAUNCHES = {"amlp_nlist_build": 11, "amlp_pair_filter": 2, "amlp_forces_fd": 1, 
 DRAM_BYTES_PER_PAIR = {"adjoint": 5.330432e6 / 436636, "fd": 5.318912e6 / 436636}
 
 
-def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS) -> float:
-    """Algorithmic FLOPs per filtered pair: descriptor F_d = 573 Nd + 432 per
-    cloud evaluation (spherical-harmonic form), net F_n = 2 (sum of layer
-    in x out); the plain method evaluates 10 clouds and 10 nets per pair, the
-    adjoint one cloud + its backward (2 F_d) and the net forward + backward (2 F_n)."""
+def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS):
+    """Algorithmic FLOPs per filtered pair as (FP32 SIMT part, tensor-core part):
+    descriptor F_d = 573 Nd + 432 per cloud evaluation (spherical-harmonic form),
+    net F_n = 2 (sum of layer in x out). The plain method evaluates 10 clouds and
+    10 nets per pair, all in FP32 SIMT; the adjoint one cloud + its backward
+    (3 F_d, FP32 SIMT) and the net forward + backward (2 F_n) on the tensor cores."""
     dims = [D] + list(widths) + [1]
     fn = 2.0 * sum(dims[k] * dims[k + 1] for k in range(len(dims) - 1))
     fd = 573.0 * nd + 432.0
     if method == "fd":
-        return 10.0 * (fd + fn)
-    return 3.0 * fd + 2.0 * fn
+        return 10.0 * (fd + fn), 0.0
+    return 3.0 * fd, 2.0 * fn
 
 
 class ClockSampler:
@@ -268,8 +272,9 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total = float(t.item())
     assert _lib.device_error() == 0, "a bounded device wait gave up"
+    finite = bool(torch.isfinite(system.pos).all() and torch.isfinite(system.vel).all())
     return {"total_ms": total, "force_ms": statistics.mean(force_ms), "force_share": sum(force_ms) / sum(step_ms),
-            "P": P, "NV": NV, "launches": launches[0]}
+            "P": P, "NV": NV, "launches": launches[0], "P_end": int(system.nf.item()), "finite": finite}
 
 
 def _e2e(system, method, steps, dist, dev):
@@ -348,11 +353,11 @@ def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) 
 
 def make_net(dev):
     """The workload's net: seeded Xavier weights, the same with the output layer scaled by 0.05, or the
-    trained cylinder net."""
+    shape's trained soft-repulsion net."""
     import numpy as np
     from amlp.engine import EnergyNet
     if NET == "trained":
-        z = np.load(DRIFT_MODEL)
+        z = np.load(os.path.join(REPO, "tests", "golden", f"model_{SHAPE}_soft.npz"))
         return EnergyNet([(z[f"W{k}"], z[f"b{k}"]) for k in range(len(z.files) // 2)], ACT, dev)
     net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device="cpu")
     layers = list(net.layers)
@@ -398,18 +403,29 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     def summary(m):
         r = results[m]
         from amlp.shapes import get_shape
-        fl_pair = algorithmic_flops_per_pair(m, nd=get_shape(SHAPE).nd, widths=WIDTHS)
+        fl_pair, tc_pair = algorithmic_flops_per_pair(m, nd=get_shape(SHAPE).nd, widths=WIDTHS)
         achieved = fl_pair * r["P"] / (r["force_ms"] / 1e3) / 1e12
+        tensor = None
+        if tc_pair:
+            tc_alg = tc_pair * r["P"] / (r["force_ms"] / 1e3) / 1e12
+            tensor = {"algorithmic_tflops": tc_alg, "executed_tflops": 3.0 * tc_alg,
+                      "peak": peaks["bf16_tflops"], "frac_executed": 3.0 * tc_alg / peaks["bf16_tflops"],
+                      "note": "net on the tensor cores as three bf16 products per multiply-add (bf16x3)"}
         return {"value": world * N_BODIES * args.steps / (r["total_ms"] / 1e3), "ms_per_step": r["total_ms"] / args.steps,
                 "roofline": {"bound": "fp32",
                              "kernel": "k_forces_" + m if max(WIDTHS) <= 64 else "k_adj_desc x2 + k_mlp_grad", "achieved": achieved, "peak": fp32_peak,
                              "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                             "traffic": DRAM_BYTES_PER_PAIR[m] * r["P"] if SHAPE == "cube26" else None, "traffic_unit": "bytes per launch (ncu, "
+                             "traffic": DRAM_BYTES_PER_PAIR[m] * r["P"] if IS_BENCHMARK else None, "traffic_unit": "bytes per launch (ncu, "
                              "scaled by pairs from 32,768 bodies)",
-                             "flops_per_pair": fl_pair, "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
+                             "flops_per_pair": fl_pair, "tensor_flops_per_pair": tc_pair, "tensor": tensor,
+                             "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
                              "force_share_of_step": r["force_share"],
                              "peak_source": f"nominal FP32 SIMT 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz (no measured "
-                                            f"FP32 peak; HBM {peaks['hbm_gbs']} GB/s {peaks['source']})"},
+                                            f"FP32 peak; HBM {peaks['hbm_gbs']} GB/s, bf16 {peaks['bf16_tflops']} TFLOP/s "
+                                            f"{peaks['source']})",
+                             "work": ("achieved counts the FP32 SIMT work only (descriptor forward and backward); "
+                                      "the net's tensor-core work is reported under 'tensor'") if tc_pair else
+                                     "achieved counts all the work (descriptors and net, FP32 SIMT)"},
                 "e2e": {"value": world * N_BODIES * r["e2e_steps"] / (r["e2e_ms"] / 1e3), "unit": "particle-steps/s",
                         "h2d_bytes_per_step": r["e2e_bytes"], "d2h_bytes_per_step": r["e2e_bytes"],
                         "steps": r["e2e_steps"]},
@@ -421,7 +437,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             "warmup": args.warmup, "ms_per_step": hs["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, Xavier weights)",
             "config": {"workload": WORKLOAD, "method": head, "bodies": N_BODIES,
-                       "verlet_pairs": results[head]["NV"], "filtered_pairs": results[head]["P"], "nlist_every": 100,
+                       "verlet_pairs": results[head]["NV"], "filtered_pairs": results[head]["P"],
+                       "filtered_pairs_last_step": results[head]["P_end"], "state_finite": results[head]["finite"],
+                       "nlist_every": 100,
                        "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": "replicas" if world > 1 else "single",
                        "precision": ("FP32 descriptors; net on tensor cores as bf16x3 splits with FP32 accumulation"
@@ -433,7 +451,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                          "roofline": ps["roofline"], "e2e": ps["e2e"]}
         line["tuned_over_plain"] = hs["value"] / ps["value"]
         line["gpu_launches"] += ps["gpu_launches"]
-    if rank == 0 and world == 1 and not args.no_serving and SHAPE == "cube26":
+    if rank == 0 and world == 1 and not args.no_serving and IS_BENCHMARK:
         line["serving"] = run_serving(dev)
     if rank == 0 and not args.no_cpu_baseline and world == 1 and SHAPE == "cube26":
         from amlp.configs import make_state as _ms
@@ -553,7 +571,7 @@ def main():
         w = WORKLOADS[args.workload]
         g = globals()
         g.update(N_BODIES=w["n"], SHAPE=w["shape"], PHI=w["phi"], SEED=w["seed"], WIDTHS=w["widths"],
-                 ACT=w["act"], NET=w["net"])
+                 ACT=w["act"], NET=w["net"], IS_BENCHMARK=False)
         g["WORKLOAD"] = (f"nvt-step-{w['n']}-{w['shape']}-phi{w['phi']:.2f}-mlp47x" +
                          "x".join(str(x) for x in w["widths"]) + f"x1-{w['act']}")
         if args.bodies == 131072:

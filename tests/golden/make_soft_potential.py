@@ -1,5 +1,6 @@
-"""Train the 47->128->128->1 SiLU pair-energy net of the twisted-cylinder
-(``cyl24``) workload and write it to ``model_cyl24_soft.npz`` in this directory.
+"""Train the SiLU pair-energy nets of the twisted-cylinder (``cyl24``,
+47->128->128->1) and tetrahedron (``tetra16``, 47->128->128->128->1) workloads and
+write them to ``model_<shape>_soft.npz`` in this directory.
 
 A random net has no meaning as a potential: its pair energy at the 2.5 pair
 cutoff is far from zero, so every pair that crosses the cutoff changes the
@@ -8,28 +9,30 @@ ground truth, so that it can drive NVE runs whose energy drift means something:
 
     E_ij = sum_{a in i, b in j} eps (1 - r_ab / r_c)^3   for r_ab < r_c,
 
-the soft repulsion of the two bodies' interaction points, eps = 10, r_c = 0.34.
-With points at most sqrt(1 + 0.4^2) = 1.077 from a cylinder's centre, E_ij is
-exactly 0 beyond a centre distance of 2 * 1.077 + 0.34 = 2.494, inside the 2.5
-cutoff.
+the soft repulsion of the two bodies' interaction points, eps = 10. For the
+cylinders r_c = 0.34: with points at most sqrt(1 + 0.4^2) = 1.077 from a
+cylinder's centre, E_ij is exactly 0 beyond a centre distance of
+2 * 1.077 + 0.34 = 2.494, inside the 2.5 cutoff. For the tetrahedra (points at
+most sqrt(3/8) = 0.612 from the centre) r_c = 0.5, so E_ij vanishes beyond 1.72.
 
 Training data: 262,144 pairs, three quarters with the centre distance uniform
-in [0.4, 3.0] and one quarter uniform in [2.2, 3.0] (where the label is 0 or
-nearly so), uniform random orientations (seed 0); labels in FP64 from the
+in [0.4, 3.0] and one quarter uniform in [zero_from - 0.3, 3.0] (where the label
+is 0 or nearly so; zero_from is the distance beyond which E_ij vanishes),
+uniform random orientations (seed 0); labels in FP64 from the
 formula above, normalised as the reference's training code does
 (``05/FFNN.py:59-63``); descriptors from ``amlp_pair_descriptors`` on the GPU.
 The net sees standardised descriptors during training; the standardisation is
 folded into the first layer before saving, so the saved net takes raw
 descriptors like the reference's. Loss: mean squared error as in
-``05/FFNN.py:95-106``, with pairs beyond a centre distance of 2.3 weighted 20x
-so that the fitted energy is close to zero where pairs cross the cutoff (a
-jump there breaks energy conservation); forward by ``amlp_mlp_energy``, the
+``05/FFNN.py:95-106``, with pairs beyond zero_from - 0.2 weighted 20x so that
+the fitted energy is close to zero where pairs cross the cutoff (a jump there
+breaks energy conservation); forward by ``amlp_mlp_energy``, the
 weighted output gradient formed in torch, weight gradient by
 ``amlp_mlp_backward``. Adam (lr 2e-3, cosine decay), batch 4,096, 120 epochs.
 A held-out set of 16,384 pairs gives the fit error and the net's energy at the
-cutoff (centre distances 2.45-2.55), written to ``model_cyl24_soft.json``.
+cutoff (centre distances 2.45-2.55), written to ``model_<shape>_soft.json``.
 
-Usage (needs a CUDA device): ``python tests/golden/make_cyl24_potential.py [out.npz]``.
+Usage (needs a CUDA device): ``python tests/golden/make_soft_potential.py [cyl24|tetra16] [out.npz]``.
 """
 from __future__ import annotations
 
@@ -44,8 +47,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "anisotropic-ml_b200"))
 
-EPS, RC = 10.0, 0.34
-WIDTHS = (128, 128)
+EPS = 10.0
+# per shape: hidden widths, point-point interaction range r_c, centre distance beyond which E_ij = 0
+SHAPE_CFG = {
+    "cyl24": dict(widths=(128, 128), rc=0.34, zero_from=2.494),
+    "tetra16": dict(widths=(128, 128, 128), rc=0.5, zero_from=1.72),
+}
+RC = SHAPE_CFG["cyl24"]["rc"]
+WIDTHS = SHAPE_CFG["cyl24"]["widths"]
 
 
 def _rotate(q, p):
@@ -55,20 +64,21 @@ def _rotate(q, p):
     return p[None] + w * t + np.cross(u, t)
 
 
-def soft_energy(pts, d_vec, qi, qj, chunk=16384):
+def soft_energy(pts, d_vec, qi, qj, chunk=16384, rc=None):
     """Ground-truth pair energy in FP64 (formula in the module docstring)."""
+    rc = RC if rc is None else rc
     out = np.empty(len(d_vec))
     pts = np.asarray(pts, np.float64)
     for s in range(0, len(d_vec), chunk):
         pi = _rotate(qi[s:s + chunk], pts)
         pj = _rotate(qj[s:s + chunk], pts) + d_vec[s:s + chunk, None, :]
         r = np.linalg.norm(pi[:, :, None, :] - pj[:, None, :, :], axis=-1)
-        x = np.clip(1.0 - r / RC, 0.0, None)
+        x = np.clip(1.0 - r / rc, 0.0, None)
         out[s:s + chunk] = EPS * (x ** 3).sum((1, 2))
     return out
 
 
-def sample_pairs(n, seed, far_fraction=0.25):
+def sample_pairs(n, seed, far_fraction=0.25, far_from=2.2):
     """Pair k = bodies (2k, 2k+1): 2k on a lattice of spacing 8, 2k+1 at a
     random centre distance in a random direction (distribution in the module
     docstring)."""
@@ -78,7 +88,7 @@ def sample_pairs(n, seed, far_fraction=0.25):
     L = float(np.float32(8.0 * m))
     grid = np.stack(np.meshgrid(*[np.arange(m)] * 3, indexing="ij"), -1).reshape(-1, 3)[:n]
     a = grid * 8.0 - L / 2 + 4.0
-    d = np.where(rng.random(n) < far_fraction, rng.uniform(2.2, 3.0, n), rng.uniform(0.4, 3.0, n))
+    d = np.where(rng.random(n) < far_fraction, rng.uniform(far_from, 3.0, n), rng.uniform(0.4, 3.0, n))
     u = rng.normal(size=(n, 3))
     u /= np.linalg.norm(u, axis=1, keepdims=True)
     pos = np.empty((2 * n, 3), np.float32)
@@ -91,7 +101,7 @@ def sample_pairs(n, seed, far_fraction=0.25):
     return pos, quat, pairs, L, d, d_vec, q64[0::2], q64[1::2]
 
 
-def main(out_path: str) -> None:
+def main(shape_name: str, out_path: str) -> None:
     import ctypes
 
     import torch
@@ -101,12 +111,14 @@ def main(out_path: str) -> None:
     from amlp.shapes import get_shape
 
     dev = torch.device("cuda:0")
-    shape = get_shape("cyl24")
-    model = PairModel(shape, Hypers(), [47, *WIDTHS, 1], "silu", dev)
+    cfg = SHAPE_CFG[shape_name]
+    widths = cfg["widths"]
+    shape = get_shape(shape_name)
+    model = PairModel(shape, Hypers(), [47, *widths, 1], "silu", dev)
 
     def dataset(n, seed):
-        pos, quat, pairs, L, d, d_vec, qi, qj = sample_pairs(n, seed)
-        E = soft_energy(shape.pts, d_vec, qi, qj)
+        pos, quat, pairs, L, d, d_vec, qi, qj = sample_pairs(n, seed, far_from=cfg["zero_from"] - 0.3)
+        E = soft_energy(shape.pts, d_vec, qi, qj, rc=cfg["rc"])
         g = model.descriptors(torch.tensor(pos, device=dev), torch.tensor(quat, device=dev),
                               torch.tensor(pairs, device=dev), L).clone()
         y = normalised_energies(torch.tensor(E), shape.en_min, shape.en_max).to(dev, torch.float32)
@@ -118,9 +130,9 @@ def main(out_path: str) -> None:
     sd = g.std(0).clamp_min(1e-6)
     gs, gvs = ((g - mu) / sd).contiguous(), ((gv - mu) / sd).contiguous()
 
-    net0 = EnergyNet.xavier(47, WIDTHS, "silu", seed=0, device="cpu")
+    net0 = EnergyNet.xavier(47, widths, "silu", seed=0, device="cpu")
     w = torch.cat([torch.cat([torch.tensor(W).reshape(-1), torch.tensor(b)]) for W, b in net0.layers]).to(dev)
-    wt = torch.where(torch.tensor(d) > 2.3, 20.0, 1.0).to(dev, torch.float32)
+    wt = torch.where(torch.tensor(d) > cfg["zero_from"] - 0.2, 20.0, 1.0).to(dev, torch.float32)
     opt = torch.optim.Adam([w], lr=2e-3)
     B, epochs = 4096, 120
     steps = epochs * (len(gs) // B)
@@ -147,7 +159,7 @@ def main(out_path: str) -> None:
             print(f"epoch {ep + 1}: train {tl.item():.3e} held-out {vl.item():.3e} (unweighted)", flush=True)
 
     # fold the standardisation into the first layer: W0 (g - mu)/sd + b0 = (W0/sd) g + (b0 - W0 mu/sd)
-    dims = [47, *WIDTHS, 1]
+    dims = [47, *widths, 1]
     layers, off = [], 0
     for k in range(len(dims) - 1):
         n_w = dims[k + 1] * dims[k]
@@ -178,4 +190,5 @@ def main(out_path: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "model_cyl24_soft.npz"))
+    name = sys.argv[1] if len(sys.argv) > 1 else "cyl24"
+    main(name, sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, f"model_{name}_soft.npz"))

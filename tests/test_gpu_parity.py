@@ -53,6 +53,9 @@ def _nlist_cases():
     out.append(("cube26-4096-phi045", s.pos, s.L, 4.5))
     s = make_state(2000, "cyl24", 0.35, seed=3)
     out.append(("cyl24-2000", s.pos, s.L, 4.5))
+    # dense: more than a warp's shared buffer (1,024) of neighbours j > i for many bodies
+    s = make_state(8000, "tetra16", 0.40, seed=2)
+    out.append(("tetra16-8000-phi040-dense", s.pos, s.L, 4.5))
     L = np.float32(8.0)
     out.append(("small-box-brute-force", (rng.random((60, 3)) * L - L / 2).astype(np.float32), float(L), 4.5))
     out.append(("one-body", np.zeros((1, 3), np.float32), 10.0, 4.5))
@@ -79,6 +82,15 @@ def test_nlist_capacity_reports_count():
     full, k = gh.nlist(s.pos, s.L, 4.5)
     part, k2 = gh.nlist(s.pos, s.L, 4.5, cap=100)
     assert k2 == k and np.array_equal(part, full[:100])
+    # a capacity that cuts through a body with more than 1,024 neighbours j > i
+    s = make_state(8000, "tetra16", 0.40, seed=2)
+    full, k = gh.nlist(s.pos, s.L, 4.5)
+    counts = np.bincount(full[:, 0], minlength=8000)
+    big = int(np.argmax(counts > 1024))
+    assert counts[big] > 1024
+    cut = int(counts[:big].sum()) + 500
+    part, k2 = gh.nlist(s.pos, s.L, 4.5, cap=cut)
+    assert k2 == k and np.array_equal(part, full[:cut])
 
 
 # ----------------------------------------------------------------------------- pair filter

@@ -1,7 +1,7 @@
 """Precision of the tensor-core path against the FP64 oracle on the precision
 workload: 262,144 twisted cylinders (cyl24) at packing fraction 0.35, seed 3
 (about 3 M filtered pairs), net 47->128->128->1 SiLU (the soft-repulsion fit of
-``golden/make_cyl24_potential.py``).
+``golden/make_soft_potential.py``).
 
 The force pass (``System.compute_forces('adjoint')``: FP32 descriptors, net on
 the tensor cores as bf16x3 splits with FP32 accumulation, FP64 energy sum) is
