@@ -977,6 +977,22 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long p0 = tile * kAP;
         const int valid = (int)min((long long)kAP, P - p0);
+        // this thread's harmonic sums: computed by the forward pass (and stored
+        // for the backward pass when a_rows is given), read back by the backward
+        // pass; layout [tile][half][n][kk][pair] so that a warp's accesses coalesce
+        float A[Cfg::NA][KC];
+        float *a_tile = a_rows ? a_rows + ((size_t)tile * 2 + h) * (Cfg::NA * KC) * kAP + p : nullptr;
+        if (BWD && a_rows) {
+            // the backward's inputs first, so that their loads overlap the rotation pass
+#pragma unroll
+            for (int n = 0; n < Cfg::NA; ++n)
+#pragma unroll
+                for (int kk = 0; kk < KC; ++kk) A[n][kk] = a_tile[(n * KC + kk) * kAP];
+            for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
+                int q = idx / kGP, d = idx - q * kGP;
+                S.g0[q * kGS + d] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
+            }
+        }
         if (tid < kAP) {
             long long pr = min(p0 + tid, P - 1);
             int i = pairs[2 * pr], j = pairs[2 * pr + 1];
@@ -1008,11 +1024,6 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             c.y *= inv;
             c.z *= inv;
         }
-        // this thread's harmonic sums: computed by the forward pass (and stored
-        // for the backward pass when a_rows is given), read back by the backward
-        // pass; layout [tile][half][n][kk][pair] so that a warp's accesses coalesce
-        float A[Cfg::NA][KC];
-        float *a_tile = a_rows ? a_rows + ((size_t)tile * 2 + h) * (Cfg::NA * KC) * kAP + p : nullptr;
         if (!BWD || !a_rows) {
             if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, A);
             else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGS, A);
@@ -1022,11 +1033,6 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
 #pragma unroll
                     for (int kk = 0; kk < KC; ++kk) a_tile[(n * KC + kk) * kAP] = A[n][kk];
             }
-        } else {
-#pragma unroll
-            for (int n = 0; n < Cfg::NA; ++n)
-#pragma unroll
-                for (int kk = 0; kk < KC; ++kk) A[n][kk] = a_tile[(n * KC + kk) * kAP];
         }
         __syncthreads();
         if (!BWD) {
@@ -1038,9 +1044,11 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             __syncthreads();
             continue;
         }
-        for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
-            int q = idx / kGP, d = idx - q * kGP;
-            S.g0[q * kGS + d] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
+        if (!a_rows) {  // the forward partials held S.g0 until now
+            for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
+                int q = idx / kGP, d = idx - q * kGP;
+                S.g0[q * kGS + d] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
+            }
         }
         __syncthreads();
         if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, S.part + p * kPartStride, A);
@@ -1093,7 +1101,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
                                                           AdjNet net, const float *w, const char *wsplit,
                                                           float *y_rows, float *dg_rows) {
     extern __shared__ __align__(128) char smem_raw[];
-    __shared__ uint64_t mbar, wbar;
+    __shared__ uint64_t mbar, wbar, gbar;
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5;
@@ -1102,6 +1110,10 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
     char *wbuf = smem_raw + 2 * tile_bytes;                       // one layer's weights, hi + lo
     float *par = reinterpret_cast<float *>(wbuf + (size_t)2 * kWideMax * kWideMax * 2);
     float *eps = par + net.par_total;
+    // the next tile's descriptor rows, brought in by a bulk copy during this tile's net
+    float *gbuf = reinterpret_cast<float *>(
+        smem_raw + align_up(2 * tile_bytes + (size_t)2 * kWideMax * kWideMax * 2 + (size_t)(net.par_total + 2 * kAP) * 4,
+                            128));
     auto tile = [&](int k) { return ops + (k & 1) * tile_bytes; };
     for (int L2 = 0; L2 < net.nh; ++L2) {
         const int N = net.dims[L2 + 1], Np = net.nout[L2];
@@ -1118,6 +1130,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
     if (tid == 0) {
         tc::mbar_init(&mbar, 1);
         tc::mbar_init(&wbar, 1);
+        tc::mbar_init(&gbar, 1);
         abort_flag = 0;
     }
     tc::fence_before();
@@ -1165,13 +1178,32 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
     const long long P = min(*d_np, cap);
     const long long ntiles = (P + kAP - 1) / kAP;
     const int Kg = net.kin[0];
+    // descriptor rows of tile tl into gbuf (thread 0; rows r0 .. r0 + valid are contiguous)
+    bool g_pending = false;
+    uint32_t gphase = 0;
+    const uint32_t gbuf_u32 = tc::smem_u32(gbuf), gbar_u32 = tc::smem_u32(&gbar);
+    auto request_g = [&](long long tl) {
+        if (tid != 0 || abort_flag || tl >= ntiles) return;
+        const long long r0 = tl * kAP;
+        const uint32_t bytes = (uint32_t)(min((long long)kAP, P - r0) * kGP * 4);
+        tc::mbar_arrive_expect_tx(gbar_u32, bytes);
+        tc::bulk_g2s(gbuf_u32, g_rows + r0 * kGP, bytes, gbar_u32);
+        g_pending = true;
+    };
+    request_g(blockIdx.x);
     for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
         const long long r0 = tl * kAP;
         const int valid = (int)min((long long)kAP, P - r0);
+        if (!tc::mbar_wait(gbar_u32, gphase)) {  // every thread reads gbuf
+            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
+            abort_flag = 1;
+        }
+        gphase ^= 1u;
+        if (tid == 0) g_pending = false;
         for (int c0 = h * (Kg / 2); c0 < (h + 1) * (Kg / 2); c0 += 8) {
             float v[8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = p < valid ? g_rows[(r0 + p) * kGP + c0 + k] : 0.f;
+            for (int k = 0; k < 8; ++k) v[k] = p < valid ? gbuf[p * kGP + c0 + k] : 0.f;
             store_split8(tile(0), Kg, p, c0, v);
         }
         for (int L2 = 0; L2 < net.nh; ++L2) {
@@ -1179,6 +1211,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
             request(L2);
             tc::fence_async_smem();
             __syncthreads();
+            if (L2 == 0) request_g(tl + gridDim.x);  // gbuf has been read: prefetch the next tile
             if (tid == 0) ensure();
             if (tid == 0 && !abort_flag) {
                 tc::fence_after();
@@ -1255,6 +1288,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
     }
     if (abort_flag && tid == 0) tc::mbar_wait(bar, phase);
     if (tid == 0) ensure();  // no copy may still be writing shared memory at exit
+    if (tid == 0 && g_pending) tc::mbar_wait(gbar_u32, gphase);
     __syncthreads();
     if (warp == 0) {
         tc::fence_after();
@@ -1427,8 +1461,9 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     float *a_rows = c.take<float>(adj_a_bytes(cap) / 4);
     const int npts = nep->npts;
     const size_t smem_desc = wide_desc_smem(npts);
-    const size_t smem_mlp = (size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
-                            (size_t)(net.par_total + 2 * kAP) * 4;
+    const size_t smem_mlp = align_up((size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
+                                     (size_t)(net.par_total + 2 * kAP) * 4, 128) +
+                            (size_t)kAP * kGP * 4;
     if (smem_desc > 220 * 1024 || smem_mlp > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
     cudaStream_t s = as_stream(stream);
