@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                                                                 const float *pts, int npts, float inv_rc, float en_min,
                                                                 float en_range, AdjNet net, const float *w, float *F,
                                                                 float *T, double *pe, const int *rep,
-                                                                const amlp_replica *rp) {
+                                                                const amlp_replica *rp, int keep_r) {
     constexpr int KC = Half<Cfg>::KC;
     constexpr int DP = kGS;  // row stride of the fp32 descriptor staging
     extern __shared__ __align__(128) char smem_raw[];
@@ -470,18 +470,35 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     // ---- shared memory carve-up (offsets are multiples of 128 bytes)
     AdjShared S;
     size_t off = 0;
+    // Two layouts. keep_r: the rotated points R have their own area and the
+    // descriptor partials g0, g1 live in the two operand tiles (free whenever
+    // the partials are), so R survives the net and is rotated once per tile.
+    // Otherwise (when that does not fit) R shares its area with the operand
+    // tiles and is rotated again after the net.
     const size_t r_bytes = (size_t)kAP * rs * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
-    S.ops = smem_raw;
-    S.R = reinterpret_cast<float *>(smem_raw);
-    off = align_up(r_bytes > ops_bytes ? r_bytes : ops_bytes, 128);
+    if (keep_r) {
+        S.R = reinterpret_cast<float *>(smem_raw);
+        off = align_up(r_bytes, 128);
+        S.ops = smem_raw + off;
+        off += align_up(ops_bytes, 128);
+    } else {
+        S.ops = smem_raw;
+        S.R = reinterpret_cast<float *>(smem_raw);
+        off = align_up(r_bytes > ops_bytes ? r_bytes : ops_bytes, 128);
+    }
     S.wts = smem_raw + off;
     off += align_up(net.wsm_total, 128);
     S.par = reinterpret_cast<float *>(smem_raw + off);
     off += align_up((size_t)net.par_total * 4, 128);
-    S.g0 = reinterpret_cast<float *>(smem_raw + off);
-    off += (size_t)kAP * DP * 4;
-    S.g1 = reinterpret_cast<float *>(smem_raw + off);
-    off += (size_t)kAP * DP * 4;
+    if (keep_r) {
+        S.g0 = reinterpret_cast<float *>(op_tile(S.ops, 0));
+        S.g1 = reinterpret_cast<float *>(op_tile(S.ops, 1));
+    } else {
+        S.g0 = reinterpret_cast<float *>(smem_raw + off);
+        off += (size_t)kAP * DP * 4;
+        S.g1 = reinterpret_cast<float *>(smem_raw + off);
+        off += (size_t)kAP * DP * 4;
+    }
     S.t = reinterpret_cast<float *>(smem_raw + off);
     off += (size_t)kAP * 3 * 4;
     S.cen = reinterpret_cast<float *>(smem_raw + off);
@@ -606,15 +623,18 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         // ---- 3. net forward + backward on the tensor cores
         {
             char *tG = op_tile(S.ops, 0);
-            for (int c0 = h * (Kg / 2); c0 < (h + 1) * (Kg / 2); c0 += 8) {
-                float v[8];
+            // this thread's half of its row of g (kin[0] = 48 columns, set by the
+            // launcher, 24 per half), read completely before the tile is written:
+            // with keep_r, g0 and g1 occupy the operand tiles
+            float v[24];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    int d = c0 + k;
-                    v[k] = d < Cfg::D ? S.g0[p * DP + d] + S.g1[p * DP + d] : 0.f;
-                }
-                store_split8(tG, Kg, p, c0, v);
+            for (int k = 0; k < 24; ++k) {
+                int d = h * 24 + k;
+                v[k] = d < Cfg::D ? S.g0[p * DP + d] + S.g1[p * DP + d] : 0.f;
             }
+            __syncthreads();
+#pragma unroll
+            for (int c = 0; c < 3; ++c) store_split8(tG, Kg, p, h * 24 + 8 * c, v + 8 * c);
         }
         tc::fence_async_smem();
         __syncthreads();
@@ -695,8 +715,10 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         if (!MULTI && h == 0 && p < valid)
             pe_acc += (double)en_min + (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
         // ---- 4. recompute the rotated points (their area held the MLP tiles)
-        rotate_tile(S, npts, rs);
-        __syncthreads();
+        if (!keep_r) {
+            rotate_tile(S, npts, rs);
+            __syncthreads();
+        }
         // ---- descriptor backward
         if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + p * kPartStride, A);
         else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * kPartStride, A);
@@ -1346,9 +1368,16 @@ static amlp_status launch_adjoint(const float *d_pos, const float *d_quat, float
     const int npts = nep->npts;
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
     size_t r_bytes = (size_t)kAP * rs * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
-    size_t smem = align_up(std::max(r_bytes, ops_bytes), 128) + align_up(wsm, 128) + align_up((size_t)par * 4, 128) +
-                  (size_t)kAP * kGS * 4 * 2 + (size_t)kAP * 3 * 4 * 2 + (size_t)2 * kAP * kPartStride * 4 + (size_t)2 * kAP * 4 +
-                  (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 + (size_t)kAP * 32 + 16 + 128;
+    static_assert((size_t)kAP * kGS * 4 <= (size_t)2 * kAP * kWpad * 2, "descriptor partials fit an operand tile");
+    const size_t tail = (size_t)kAP * 3 * 4 * 2 + (size_t)2 * kAP * kPartStride * 4 + (size_t)2 * kAP * 4 +
+                        (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 + (size_t)kAP * 32 + 16 + 128;
+    // R kept apart from the operand tiles (one rotation pass per tile) when it fits
+    const size_t smem_keep = align_up(r_bytes, 128) + align_up(ops_bytes, 128) + align_up(wsm, 128) +
+                             align_up((size_t)par * 4, 128) + tail;
+    const size_t smem_shared = align_up(std::max(r_bytes, ops_bytes), 128) + align_up(wsm, 128) +
+                               align_up((size_t)par * 4, 128) + (size_t)kAP * kGS * 4 * 2 + tail;
+    const int keep_r = smem_keep <= 220 * 1024 ? 1 : 0;
+    const size_t smem = keep_r ? smem_keep : smem_shared;
     if (smem > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
     cudaStream_t s = as_stream(stream);
@@ -1358,13 +1387,14 @@ static amlp_status launch_adjoint(const float *d_pos, const float *d_quat, float
                                              (int)smem));
         k_forces_adjoint<Cfg, true><<<kNumSM, kAThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap,
                                                                     nep->d_pts, npts, inv_rc, nep->en_min, rng, net,
-                                                                    mlp->d_w, d_F, d_T, d_pe, d_rep, d_rp);
+                                                                    mlp->d_w, d_F, d_T, d_pe, d_rep, d_rp, keep_r);
     } else {
         AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_forces_adjoint<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem));
         k_forces_adjoint<Cfg, false><<<kNumSM, kAThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap,
                                                                      nep->d_pts, npts, inv_rc, nep->en_min, rng, net,
-                                                                     mlp->d_w, d_F, d_T, d_pe, nullptr, nullptr);
+                                                                     mlp->d_w, d_F, d_T, d_pe, nullptr, nullptr,
+                                                                     keep_r);
     }
     return check_launch();
 }

@@ -71,6 +71,12 @@ LAUNCHES = {"amlp_nlist_build": 11, "amlp_pair_filter": 2, "amlp_forces_fd": 1, 
 # profiles give the command). The traffic grows with the pairs (a capture at 131,072 bodies gave the
 # same bytes per pair), so the roofline's traffic is this figure times the launch's pairs.
 DRAM_BYTES_PER_PAIR = {"adjoint": 5.330432e6 / 436636, "fd": 5.318912e6 / 436636}
+# The wide path (nets wider than 64) stores each pair's descriptor row, harmonic sums and dE/dg in
+# HBM between its three launches: the sum over k_adj_desc forward, k_mlp_grad and k_adj_desc backward
+# captured at 32,768 cyl24 bodies (381,342 pairs). The per-pair rows do not depend on the shape or the
+# net, so the figure serves every wide workload.
+DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.041216e6 + 343.165184e6 + 73.378048e6 + 25.07904e6 + 409.904128e6
+                                       + 4.889344e6) / 381342
 
 
 def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS):
@@ -415,8 +421,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                 "roofline": {"bound": "fp32",
                              "kernel": "k_forces_" + m if max(WIDTHS) <= 64 else "k_adj_desc x2 + k_mlp_grad", "achieved": achieved, "peak": fp32_peak,
                              "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                             "traffic": DRAM_BYTES_PER_PAIR[m] * r["P"] if IS_BENCHMARK else None, "traffic_unit": "bytes per launch (ncu, "
-                             "scaled by pairs from 32,768 bodies)",
+                             "traffic": DRAM_BYTES_PER_PAIR[m if max(WIDTHS) <= 64 else "adjoint_wide"] * r["P"],
+                             "traffic_unit": "bytes per force pass (ncu, scaled by pairs from 32,768 bodies)",
                              "flops_per_pair": fl_pair, "tensor_flops_per_pair": tc_pair, "tensor": tensor,
                              "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
                              "force_share_of_step": r["force_share"],
@@ -435,7 +441,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     hs = summary(head)
     line = {"metric": METRIC, "value": hs["value"], "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": hs["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, Xavier weights)",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, " + ("Xavier weights)" if NET != "trained" else
+                                                                 "net fitted to a soft repulsion, committed fixture)"),
             "config": {"workload": WORKLOAD, "method": head, "bodies": N_BODIES,
                        "verlet_pairs": results[head]["NV"], "filtered_pairs": results[head]["P"],
                        "filtered_pairs_last_step": results[head]["P_end"], "state_finite": results[head]["finite"],
