@@ -846,6 +846,10 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
 // ============================================================================
 constexpr int kWideMax = 128;
 constexpr int kGP = 48;  // padded descriptor width in the workspace rows
+// Row stride of the descriptor rows in the workspace and in k_mlp_grad's shared
+// copy: 52 floats, 13 units of 16 bytes, odd, so that the 16-byte reads of 32
+// consecutive rows by a warp fall in distinct bank groups.
+constexpr int kGRow = 52;
 constexpr size_t kWeightSplitBytes = (size_t)kMaxHidden * kWideMax * kWideMax * 4;  // bf16 hi/lo of every layer
 constexpr size_t kAdjAFloats = 2 * 9 * 12;  // harmonic sums per pair kept between the passes (two halves of 9 x 12)
 
@@ -948,6 +952,17 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
     __syncthreads();
 }
 
+// dE/dg rows of the tile's pairs into S.g0 (row stride kGS), weighted by wt
+// when given; rows past `valid` are zero. One row per warp, lanes over columns.
+__device__ __forceinline__ void load_dg_rows(const AdjShared &S, const float *dg_rows, const float *wt, long long p0,
+                                             int valid) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = warp; q < kAP; q += kAThreads / 32) {
+        const float w = q < valid ? (wt ? wt[p0 + q] : 1.0f) : 0.f;
+        for (int d = lane; d < kGP; d += 32) S.g0[q * kGS + d] = q < valid ? w * dg_rows[(p0 + q) * kGP + d] : 0.f;
+    }
+}
+
 // Descriptor pass of the wide path: BWD = false writes g rows (row stride
 // g_ld >= D, zero padded); BWD = true reads dE/dg rows (stride kGP) and the net
 // outputs and produces forces, torques and energies. wt (BWD, may be null)
@@ -1010,10 +1025,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             for (int n = 0; n < Cfg::NA; ++n)
 #pragma unroll
                 for (int kk = 0; kk < KC; ++kk) A[n][kk] = a_tile[(n * KC + kk) * kAP];
-            for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
-                int q = idx / kGP, d = idx - q * kGP;
-                S.g0[q * kGS + d] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
-            }
+            load_dg_rows(S, dg_rows, wt, p0, valid);
         }
         if (tid < kAP) {
             long long pr = min(p0 + tid, P - 1);
@@ -1058,19 +1070,14 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
         }
         __syncthreads();
         if (!BWD) {
-            for (int idx = tid; idx < kAP * g_ld; idx += kAThreads) {
-                int q = idx / g_ld, d = idx - q * g_ld;
-                if (q < valid)
+            for (int q = warp; q < valid; q += kAThreads / 32)  // one row per warp: coalesced
+                for (int d = lane; d < g_ld; d += 32)
                     g_rows[(p0 + q) * g_ld + d] = d < Cfg::D ? S.g0[q * kGS + d] + S.g1[q * kGS + d] : 0.f;
-            }
             __syncthreads();
             continue;
         }
         if (!a_rows) {  // the forward partials held S.g0 until now
-            for (int idx = tid; idx < kAP * kGP; idx += kAThreads) {
-                int q = idx / kGP, d = idx - q * kGP;
-                S.g0[q * kGS + d] = q < valid ? (wt ? wt[p0 + q] : 1.0f) * dg_rows[p0 * kGP + idx] : 0.f;
-            }
+            load_dg_rows(S, dg_rows, wt, p0, valid);
         }
         __syncthreads();
         if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, S.part + p * kPartStride, A);
@@ -1113,13 +1120,17 @@ __global__ void k_split_weights(AdjNet net, const float *w, char *dst) {
 }
 
 // Net forward and backward over rows of g on the tensor cores (bf16x3 splits,
-// fp32 TMEM accumulators). One layer's weights at a time sit in shared memory,
+// fp32 TMEM accumulators). 16 warps: warp w reads TMEM lanes 32 (w % 4) ..
+// 32 (w % 4) + 31 (its pairs) and, of every layer's columns, the 8-column
+// chunks c with c % 4 == w / 4, so that four warps share each epilogue's rows. One layer's weights at a time sit in shared memory,
 // brought in by a bulk copy from the pre-split copy (k_split_weights) that
 // thread 0 starts as soon as the previous layer's MMAs are done, so it overlaps
 // the epilogue; the layer order fwd 0..nh-1, bwd nh-1..0 reuses the last
 // forward layer and, across tiles, layer 0. Outputs per row: y = net(g) and
 // dE/dg (kGP floats).
-__global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
+constexpr int kMQ = 4;                  // column groups of the k_mlp_grad epilogues
+constexpr int kMThreads = kMQ * kAP;    // 512
+__global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
                                                           AdjNet net, const float *w, const char *wsplit,
                                                           float *y_rows, float *dg_rows) {
     extern __shared__ __align__(128) char smem_raw[];
@@ -1134,18 +1145,18 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
     float *eps = par + net.par_total;
     // the next tile's descriptor rows, brought in by a bulk copy during this tile's net
     float *gbuf = reinterpret_cast<float *>(
-        smem_raw + align_up(2 * tile_bytes + (size_t)2 * kWideMax * kWideMax * 2 + (size_t)(net.par_total + 2 * kAP) * 4,
+        smem_raw + align_up(2 * tile_bytes + (size_t)2 * kWideMax * kWideMax * 2 + (size_t)(net.par_total + kMQ * kAP) * 4,
                             128));
     auto tile = [&](int k) { return ops + (k & 1) * tile_bytes; };
     for (int L2 = 0; L2 < net.nh; ++L2) {
         const int N = net.dims[L2 + 1], Np = net.nout[L2];
         const float *b = w + net.woff[L2] + (size_t)N * net.dims[L2];
-        for (int n = tid; n < Np; n += kAThreads) par[net.bias_off[L2] + n] = n < N ? b[n] : 0.f;
+        for (int n = tid; n < Np; n += kMThreads) par[net.bias_off[L2] + n] = n < N ? b[n] : 0.f;
     }
     {
         const int K = net.dims[net.nh];
         const float *Wl = w + net.woff[net.nh];
-        for (int k = tid; k < kWideMax; k += kAThreads) par[net.bias_off[net.nh] + k] = k < K ? Wl[k] : 0.f;
+        for (int k = tid; k < kWideMax; k += kMThreads) par[net.bias_off[net.nh] + k] = k < K ? Wl[k] : 0.f;
         if (tid == 0) par[net.bias_off[net.nh] + kWideMax] = Wl[K];
     }
     if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);
@@ -1207,9 +1218,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
     auto request_g = [&](long long tl) {
         if (tid != 0 || abort_flag || tl >= ntiles) return;
         const long long r0 = tl * kAP;
-        const uint32_t bytes = (uint32_t)(min((long long)kAP, P - r0) * kGP * 4);
+        const uint32_t bytes = (uint32_t)(min((long long)kAP, P - r0) * kGRow * 4);
         tc::mbar_arrive_expect_tx(gbar_u32, bytes);
-        tc::bulk_g2s(gbuf_u32, g_rows + r0 * kGP, bytes, gbar_u32);
+        tc::bulk_g2s(gbuf_u32, g_rows + r0 * kGRow, bytes, gbar_u32);
         g_pending = true;
     };
     request_g(blockIdx.x);
@@ -1222,10 +1233,13 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
         }
         gphase ^= 1u;
         if (tid == 0) g_pending = false;
-        for (int c0 = h * (Kg / 2); c0 < (h + 1) * (Kg / 2); c0 += 8) {
+        for (int c0 = 8 * h; c0 < Kg; c0 += 8 * kMQ) {
             float v[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = p < valid ? gbuf[p * kGP + c0 + k] : 0.f;
+            const float4 *src = reinterpret_cast<const float4 *>(gbuf + p * kGRow + c0);
+            const float4 lo4 = p < valid ? src[0] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 hi4 = p < valid ? src[1] : make_float4(0.f, 0.f, 0.f, 0.f);
+            v[0] = lo4.x, v[1] = lo4.y, v[2] = lo4.z, v[3] = lo4.w;
+            v[4] = hi4.x, v[5] = hi4.y, v[6] = hi4.z, v[7] = hi4.w;
             store_split8(tile(0), Kg, p, c0, v);
         }
         for (int L2 = 0; L2 < net.nh; ++L2) {
@@ -1247,7 +1261,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
             const float *bias = par + net.bias_off[L2];
             const float *wl = par + net.bias_off[net.nh];
             float esum = 0.f;
-            for (int c0 = h * (Np / 2); c0 < (h + 1) * (Np / 2); c0 += 8) {
+            for (int c0 = 8 * h; c0 < Np; c0 += 8 * kMQ) {
                 float z[8], v[8];
                 tc::tmem_ld8(tmem + lane_base + (uint32_t)(L2 * kWideMax) + c0, z);
 #pragma unroll
@@ -1268,7 +1282,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
             tc::fence_async_smem();
             __syncthreads();
         }
-        if (tid < kAP && p < valid) y_rows[r0 + p] = eps[p] + eps[kAP + p] + par[net.bias_off[net.nh] + kWideMax];
+        if (tid < kAP && p < valid)
+            y_rows[r0 + p] = (eps[p] + eps[kAP + p]) + (eps[2 * kAP + p] + eps[3 * kAP + p]) +
+                             par[net.bias_off[net.nh] + kWideMax];
         for (int L2 = net.nh - 1; L2 >= 0; --L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
             request(L2);
@@ -1285,7 +1301,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
             request(L2 > 0 ? L2 - 1 : 0);  // the next layer needed (layer 0 again for the next tile)
             if (L2 > 0) {
                 const float *bias = par + net.bias_off[L2 - 1];
-                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
+                for (int c0 = 8 * h; c0 < Kp; c0 += 8 * kMQ) {
                     float dz[8], z[8], v[8];
                     tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
                     tc::tmem_ld8(tmem + lane_base + (uint32_t)((L2 - 1) * kWideMax) + c0, z);
@@ -1294,12 +1310,14 @@ __global__ void __launch_bounds__(kAThreads, 1) k_mlp_grad(const float *g_rows, 
                     store_split8(tile(L2), Kp, p, c0, v);
                 }
             } else {
-                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
+                for (int c0 = 8 * h; c0 < Kp; c0 += 8 * kMQ) {
                     float dg[8];
                     tc::tmem_ld8(tmem + lane_base + bcol + c0, dg);
-                    if (p < valid)
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) dg_rows[(r0 + p) * kGP + c0 + k] = dg[k];
+                    if (p < valid) {
+                        float4 *dst = reinterpret_cast<float4 *>(dg_rows + (r0 + p) * kGP + c0);
+                        dst[0] = make_float4(dg[0], dg[1], dg[2], dg[3]);
+                        dst[1] = make_float4(dg[4], dg[5], dg[6], dg[7]);
+                    }
                 }
             }
             tc::fence_before();
@@ -1447,7 +1465,7 @@ static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
 
 extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes) {
     if (cap < 0 || !bytes) return AMLP_ERR_INVALID_ARG;
-    *bytes = align_up((size_t)cap * kGP * 4) * 2 + align_up((size_t)cap * 4) + align_up(kWeightSplitBytes) +
+    *bytes = align_up((size_t)cap * kGRow * 4) + align_up((size_t)cap * kGP * 4) + align_up((size_t)cap * 4) + align_up(kWeightSplitBytes) +
              align_up(adj_a_bytes(cap)) + 256;
     return AMLP_OK;
 }
@@ -1484,7 +1502,7 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     AdjNet net;
     if ((st = wide_net(mlp, &net))) return st;
     Carver c(d_ws, ws_bytes);
-    float *g_rows = c.take<float>((size_t)cap * kGP);
+    float *g_rows = c.take<float>((size_t)cap * kGRow);
     float *dg_rows = c.take<float>((size_t)cap * kGP);
     float *y_rows = c.take<float>((size_t)cap);
     char *wsplit = c.take<char>(kWeightSplitBytes);
@@ -1492,9 +1510,9 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     const int npts = nep->npts;
     const size_t smem_desc = wide_desc_smem(npts);
     const size_t smem_mlp = align_up((size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
-                                     (size_t)(net.par_total + 2 * kAP) * 4, 128) +
-                            (size_t)kAP * kGP * 4;
-    if (smem_desc > 220 * 1024 || smem_mlp > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
+                                     (size_t)(net.par_total + kMQ * kAP) * 4, 128) +
+                            (size_t)kAP * kGRow * 4;
+    if (smem_desc > 220 * 1024 || smem_mlp > 226 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
     cudaStream_t s = as_stream(stream);
     const float inv_rc = 1.0f / nep->nep_cutoff, rng = nep->en_max - nep->en_min;
@@ -1505,10 +1523,10 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mlp));
     fwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
-                                             nep->en_min, rng, g_rows, kGP, nullptr, nullptr, nullptr, clip, d_F,
+                                             nep->en_min, rng, g_rows, kGRow, nullptr, nullptr, nullptr, clip, d_F,
                                              d_T, d_pe, d_rep, d_rp, a_rows);
     k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
-    k_mlp_grad<<<kNumSM, kAThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
+    k_mlp_grad<<<kNumSM, kMThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
     bwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, nullptr, kGP, dg_rows, y_rows, d_wt, clip, d_F, d_T,
                                              d_pe, d_rep, d_rp, a_rows);
