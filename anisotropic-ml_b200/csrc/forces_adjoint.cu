@@ -166,11 +166,33 @@ __host__ __device__ constexpr bool sh_is_sin(int k) {
     return sh_m_of(k) > 0 && ((k + 1 - sh_l_of(k) * sh_l_of(k)) % 2 == 0);
 }
 
-// Point a of cloud 1 (body i at the origin, body j moved by t).
-__device__ __forceinline__ float3 cloud1_point(const float *Ri, const float *Rj, float3 t, int h, int a) {
-    if (a < h) return make_float3(Ri[3 * a], Ri[3 * a + 1], Ri[3 * a + 2]);
-    int b = a - h;
-    return make_float3(__fadd_rn(Rj[3 * b], t.x), __fadd_rn(Rj[3 * b + 1], t.y), __fadd_rn(Rj[3 * b + 2], t.z));
+// Weight of harmonic k in the angular descriptor when the harmonics are kept
+// unnormalised (Q_l^m {C_m, S_m}): N_lm^2 = 2 (l-m)! / (l+m)! for m >= 1, 1 for
+// m = 0, so that g[n][l] = sum_m N_lm^2 (sum_a f_n Q_l^m {C_m, S_m})^2.
+__host__ __device__ constexpr float sh_weight(int k) {
+    const int l = sh_l_of(k), m = sh_m_of(k);
+    if (m == 0) return 1.0f;
+    double num = 2.0, den = 1.0;
+    for (int v = 2; v <= l - m; ++v) num *= v;
+    for (int v = 2; v <= l + m; ++v) den *= v;
+    return (float)(num / den);
+}
+
+// The unnormalised harmonics Q_l^m {C_m, S_m} (m > 0) and Q_l^0 of this half
+// (indices k0 .. k0 + KC - 1, zero past K) from the recurrences.
+template <class Cfg, int KC, int k0>
+__device__ __forceinline__ void sh_half_u(const float *C, const float *Sn, const float (&Q)[Cfg::LMAX + 2][Cfg::LMAX + 2],
+                                          float *Y) {
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk) {
+        const int k = k0 + kk;
+        if (k < Cfg::K) {
+            const int l = sh_l_of(k), m = sh_m_of(k);
+            Y[kk] = m == 0 ? Q[l][0] : Q[l][m] * (sh_is_sin(k) ? Sn[m] : C[m]);
+        } else {
+            Y[kk] = 0.f;
+        }
+    }
 }
 
 template <class Cfg>
@@ -178,47 +200,47 @@ struct Half {
     static constexpr int KC = (Cfg::K + 1) / 2;  // harmonics per half
 };
 
-// sum_a f_n(a) Y_k(a) for this half's harmonics k0..k0+KC-1 (and the radial sums).
+// sum_a f_n(a) Y_k(a) for this half's harmonics k0..k0+KC-1, unnormalised (and
+// the radial sums). r holds the pair's nd centred points (x, y, z each).
 template <class Cfg, int KC, int k0>
-__device__ __forceinline__ void accumulate_A(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
-                                             float inv_rc, float (*A)[KC], float *R) {
+__device__ __forceinline__ void accumulate_A(const float *r, int nd, float inv_rc, float (*A)[KC], float *R) {
 #pragma unroll
     for (int n = 0; n < Cfg::NA; ++n)
 #pragma unroll
         for (int kk = 0; kk < KC; ++kk) A[n][kk] = 0.f;
 #pragma unroll
     for (int n = 0; n < Cfg::NR; ++n) R[n] = 0.f;
-    const int nd = 2 * npts;
     for (int a = 0; a < nd; ++a) {
-        float3 p = cloud1_point(Ri, Rj, t, npts, a);
-        float rx = p.x - c.x, ry = p.y - c.y, rz = p.z - c.z;
+        const float rx = r[3 * a], ry = r[3 * a + 1], rz = r[3 * a + 2];
         float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
         float inv_d = rsqrtf(d2);
         float f[Cfg::NR];
         radial_basis_fast<Cfg::NR>(d2 * inv_d, inv_rc, f);
 #pragma unroll
         for (int n = 0; n < Cfg::NR; ++n) R[n] += f[n];
-        float Y[Cfg::K];
-        sh_eval<Cfg::LMAX>(rx * inv_d, ry * inv_d, rz * inv_d, Y);
+        constexpr int LM = Cfg::LMAX;
+        float C[LM + 1], Sn[LM + 1], Q[LM + 2][LM + 2];
+        sh_recurrences<LM>(rx * inv_d, ry * inv_d, rz * inv_d, C, Sn, Q);
+        float Y[KC];
+        sh_half_u<Cfg, KC, k0>(C, Sn, Q, Y);
 #pragma unroll
         for (int n = 0; n < Cfg::NA; ++n)
 #pragma unroll
             for (int kk = 0; kk < KC; ++kk)
-                if (k0 + kk < Cfg::K) A[n][kk] = fmaf(f[n], Y[k0 + kk], A[n][kk]);
+                if (k0 + kk < Cfg::K) A[n][kk] = fmaf(f[n], Y[kk], A[n][kk]);
     }
 }
 
-
 // Forward of one half of the harmonics: radial sums (half 0) and the partial
-// sums of squares of this half's harmonics, written to gp[0..47] (zeros
-// elsewhere). The sums A of this half stay in the caller's registers for the
-// backward.
+// sums of weighted squares of this half's harmonics, written to gp[0..47]
+// (zeros elsewhere). The unnormalised sums A of this half stay in the caller's
+// registers for the backward.
 template <class Cfg, int H>
-__device__ __forceinline__ void half_forward(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
-                                             float inv_rc, float *gp, float (&A)[Cfg::NA][Half<Cfg>::KC]) {
+__device__ __forceinline__ void half_forward(const float *r, int nd, float inv_rc, float *gp,
+                                             float (&A)[Cfg::NA][Half<Cfg>::KC]) {
     constexpr int KC = Half<Cfg>::KC;
     float Rr[Cfg::NR];
-    accumulate_A<Cfg, KC, H * KC>(Ri, Rj, t, npts, c, inv_rc, A, Rr);
+    accumulate_A<Cfg, KC, H * KC>(r, nd, inv_rc, A, Rr);
     for (int k = 0; k < 48; ++k) gp[k] = 0.f;
     if (H == 0) {
 #pragma unroll
@@ -228,27 +250,30 @@ __device__ __forceinline__ void half_forward(const float *Ri, const float *Rj, f
     for (int kk = 0; kk < KC; ++kk) {
         if (H * KC + kk < Cfg::K) {
             const int l = sh_l_of(H * KC + kk);
+            const float w = sh_weight(H * KC + kk);
 #pragma unroll
-            for (int n = 0; n < Cfg::NA; ++n) gp[Cfg::NR + n * Cfg::LMAX + l - 1] += A[n][kk] * A[n][kk];
+            for (int n = 0; n < Cfg::NA; ++n)
+                gp[Cfg::NR + n * Cfg::LMAX + l - 1] = fmaf(w * A[n][kk], A[n][kk], gp[Cfg::NR + n * Cfg::LMAX + l - 1]);
         }
     }
 }
 
 // Backward of one half: given dE/dg (dg) and the forward sums A of this half
-// (overwritten), the partial sums over points of
-// dE/dr_a needed for the pair force and torques: sum_{a in i} G_a, sum_a G_a,
-// sum_{a in i} p_a x G_a, sum_{a in j} (p_a - t) x G_a -> out[12].
+// (overwritten), the partial sums over the centred points r_a of dE/dr_a
+// needed for the pair force and torques: sum_{a in i} G_a, sum_a G_a,
+// sum_{a in i} r_a x G_a, sum_{a in j} r_a x G_a -> out[12] (the caller adds
+// the centroid terms).
 template <class Cfg, int H>
-__device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, float3 t, int npts, float3 c,
-                                              float inv_rc, const float *dg, float *out,
+__device__ __forceinline__ void half_backward(const float *r, int npts, float inv_rc, const float *dg, float *out,
                                               float (&A)[Cfg::NA][Half<Cfg>::KC]) {
     constexpr int KC = Half<Cfg>::KC;
 #pragma unroll
     for (int kk = 0; kk < KC; ++kk) {
         if (H * KC + kk < Cfg::K) {
             const int l = sh_l_of(H * KC + kk);
+            const float w2 = 2.0f * sh_weight(H * KC + kk);
 #pragma unroll
-            for (int n = 0; n < Cfg::NA; ++n) A[n][kk] *= 2.0f * dg[Cfg::NR + n * Cfg::LMAX + l - 1];
+            for (int n = 0; n < Cfg::NA; ++n) A[n][kk] *= w2 * dg[Cfg::NR + n * Cfg::LMAX + l - 1];
         } else {
 #pragma unroll
             for (int n = 0; n < Cfg::NA; ++n) A[n][kk] = 0.f;
@@ -260,8 +285,7 @@ __device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, 
     float Si[3] = {0, 0, 0}, Sa[3] = {0, 0, 0}, Xi[3] = {0, 0, 0}, Xj[3] = {0, 0, 0};
     const int nd = 2 * npts;
     for (int a = 0; a < nd; ++a) {
-        float3 q = cloud1_point(Ri, Rj, t, npts, a);
-        float rx = q.x - c.x, ry = q.y - c.y, rz = q.z - c.z;
+        const float rx = r[3 * a], ry = r[3 * a + 1], rz = r[3 * a + 2];
         float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
         float inv_d = rsqrtf(d2);
         float d = d2 * inv_d;
@@ -271,19 +295,8 @@ __device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, 
         constexpr int LM = Cfg::LMAX;
         float C[LM + 1], Sn[LM + 1], Q[LM + 2][LM + 2];
         sh_recurrences<LM>(ux, uy, uz, C, Sn, Q);
-        // this half's harmonics: Y_k = N Q_l^m {C_m, S_m}
         float Y[KC];
-#pragma unroll
-        for (int kk = 0; kk < KC; ++kk) {
-            const int k = H * KC + kk;
-            if (k < Cfg::K) {
-                const int l = sh_l_of(k), m = sh_m_of(k);
-                const float q = m == 0 ? Q[l][0] : c_shnorm[l][m] * Q[l][m];
-                Y[kk] = m == 0 ? q : q * (sh_is_sin(k) ? Sn[m] : C[m]);
-            } else {
-                Y[kk] = 0.f;
-            }
-        }
+        sh_half_u<Cfg, KC, H * KC>(C, Sn, Q, Y);
         float gr = 0.f;
 #pragma unroll
         for (int n = 0; n < Cfg::NR; ++n) {
@@ -296,8 +309,8 @@ __device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, 
             gr = fmaf(s, df[n], gr);
         }
         // gradient of sum_k s_k Y_k grouped by m: with U_m, V_m the sums of
-        // s N m Q_l^m over the cos / sin harmonics of order m and Wc_m, Ws_m those
-        // of s N Q_l^(m+1),
+        // s m Q_l^m over the cos / sin harmonics of order m and Wc_m, Ws_m those
+        // of s Q_l^(m+1),
         //   gx = sum_m U_m C_(m-1) + V_m S_(m-1), gy = sum_m V_m C_(m-1) - U_m S_(m-1),
         //   gz = sum_m Wc_m C_m + Ws_m S_m.
         float U[LM + 1], V[LM + 1], Wc[LM + 1], Ws[LM + 1];
@@ -311,14 +324,12 @@ __device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, 
 #pragma unroll
                 for (int n = 0; n < Cfg::NA; ++n) s = fmaf(A[n][kk], f[n], s);
                 const int l = sh_l_of(k), m = sh_m_of(k);
-                const float nrm = m == 0 ? 1.0f : c_shnorm[l][m];
-                const float wq = nrm * Q[l][m + 1];
                 if (sh_is_sin(k)) {
-                    V[m] = fmaf(s, (float)m * nrm * Q[l][m], V[m]);
-                    Ws[m] = fmaf(s, wq, Ws[m]);
+                    V[m] = fmaf(s, m == 1 ? Q[l][m] : (float)m * Q[l][m], V[m]);
+                    Ws[m] = fmaf(s, Q[l][m + 1], Ws[m]);
                 } else {
-                    if (m > 0) U[m] = fmaf(s, (float)m * nrm * Q[l][m], U[m]);
-                    Wc[m] = fmaf(s, wq, Wc[m]);
+                    if (m > 0) U[m] = fmaf(s, m == 1 ? Q[l][m] : (float)m * Q[l][m], U[m]);
+                    Wc[m] = fmaf(s, Q[l][m + 1], Wc[m]);
                 }
             }
         }
@@ -341,14 +352,13 @@ __device__ __forceinline__ void half_backward(const float *Ri, const float *Rj, 
             Si[0] += Gx;
             Si[1] += Gy;
             Si[2] += Gz;
-            Xi[0] += q.y * Gz - q.z * Gy;
-            Xi[1] += q.z * Gx - q.x * Gz;
-            Xi[2] += q.x * Gy - q.y * Gx;
+            Xi[0] += ry * Gz - rz * Gy;
+            Xi[1] += rz * Gx - rx * Gz;
+            Xi[2] += rx * Gy - ry * Gx;
         } else {
-            float bx = q.x - t.x, by = q.y - t.y, bz = q.z - t.z;
-            Xj[0] += by * Gz - bz * Gy;
-            Xj[1] += bz * Gx - bx * Gz;
-            Xj[2] += bx * Gy - by * Gx;
+            Xj[0] += ry * Gz - rz * Gy;
+            Xj[1] += rz * Gx - rx * Gz;
+            Xj[2] += rx * Gy - ry * Gx;
         }
     }
 #pragma unroll
@@ -427,21 +437,53 @@ __device__ __forceinline__ void store_split8(char *tile_hi, int K, int p, int c0
     *reinterpret_cast<uint4 *>(tile_hi + kAP * K * 2 + off) = *reinterpret_cast<uint4 *>(lo);
 }
 
-// Rotated body points of the tile's pairs into S.R from the orientations in S.q:
-// thread (q, body) = (tid % kAP, tid / kAP) rotates all points of one body of
-// one pair (orientation in registers, body points broadcast from shared
-// memory, rows of odd stride rs: no bank conflicts, no index divisions).
+// Centroid of pair q's cloud into S.cen from its orientations and translation
+// (S.q, S.t): c = (R_i s + R_j s + npts t) / (2 npts), s the sum of the
+// body-frame points. Called by the thread that wrote pair q's S.q and S.t.
+__device__ __forceinline__ void store_centroid(const AdjShared &S, int q, int npts) {
+    const float3 ps = make_float3(S.psum[0], S.psum[1], S.psum[2]);
+    const float3 a = rotate_ref(S.q[2 * q], ps), b = rotate_ref(S.q[2 * q + 1], ps);
+    const float inv = 1.0f / (float)(2 * npts), n = (float)npts;
+    S.cen[3 * q] = fmaf(n, S.t[3 * q], a.x + b.x) * inv;
+    S.cen[3 * q + 1] = fmaf(n, S.t[3 * q + 1], a.y + b.y) * inv;
+    S.cen[3 * q + 2] = fmaf(n, S.t[3 * q + 2], a.z + b.z) * inv;
+}
+
+// Centred cloud points of the tile's pairs into S.R: row q holds body i's
+// points R_i b_a - c, then body j's R_j b_a + t - c (c = S.cen). Thread
+// (q, body) = (tid % kAP, tid / kAP) rotates all points of one body of one pair
+// (orientation in registers, body points broadcast from shared memory, rows of
+// odd stride rs: no bank conflicts, no index divisions).
 __device__ __forceinline__ void rotate_tile(const AdjShared &S, int npts, int rs) {
     static_assert(kAThreads == 2 * kAP, "one thread per (pair, body)");
     const int q = threadIdx.x & (kAP - 1), body = threadIdx.x / kAP;
     const float4 qq = S.q[2 * q + body];
+    const float ox = body ? S.t[3 * q] - S.cen[3 * q] : -S.cen[3 * q];
+    const float oy = body ? S.t[3 * q + 1] - S.cen[3 * q + 1] : -S.cen[3 * q + 1];
+    const float oz = body ? S.t[3 * q + 2] - S.cen[3 * q + 2] : -S.cen[3 * q + 2];
     float *dst = S.R + q * rs + body * 3 * npts;
     for (int a = 0; a < npts; ++a) {
         float3 r = rotate_ref(qq, make_float3(S.pts[3 * a], S.pts[3 * a + 1], S.pts[3 * a + 2]));
-        dst[3 * a] = r.x;
-        dst[3 * a + 1] = r.y;
-        dst[3 * a + 2] = r.z;
+        dst[3 * a] = r.x + ox;
+        dst[3 * a + 1] = r.y + oy;
+        dst[3 * a + 2] = r.z + oz;
     }
+}
+
+// Torque sums about the body origins from those about the centroid:
+// sum_{a in i} (r_a + c) x G_a = Xi + c x Si and
+// sum_{a in j} (r_a + c - t) x G_a = Xj + (c - t) x (Sa - Si).
+__device__ __forceinline__ void add_centroid_terms(const AdjShared &S, int q, const float *Si, const float *Sa,
+                                                   float *Xi, float *Xj) {
+    const float c[3] = {S.cen[3 * q], S.cen[3 * q + 1], S.cen[3 * q + 2]};
+    const float e[3] = {c[0] - S.t[3 * q], c[1] - S.t[3 * q + 1], c[2] - S.t[3 * q + 2]};
+    const float Sj[3] = {Sa[0] - Si[0], Sa[1] - Si[1], Sa[2] - Si[2]};
+    Xi[0] += c[1] * Si[2] - c[2] * Si[1];
+    Xi[1] += c[2] * Si[0] - c[0] * Si[2];
+    Xi[2] += c[0] * Si[1] - c[1] * Si[0];
+    Xj[0] += e[1] * Sj[2] - e[2] * Sj[1];
+    Xj[1] += e[2] * Sj[0] - e[0] * Sj[2];
+    Xj[2] += e[0] * Sj[1] - e[1] * Sj[0];
 }
 
 // MULTI: the pairs come from many systems in one launch; body i's system is
@@ -591,34 +633,16 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             S.t[3 * tid + 2] = tt.z;
             S.ij[2 * tid] = i;
             S.ij[2 * tid + 1] = j;
+            store_centroid(S, tid, npts);
         }
         __syncthreads();
         rotate_tile(S, npts, rs);
         __syncthreads();
         // ---- 2. descriptor forward
-        const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
-        const float3 t = make_float3(S.t[3 * p], S.t[3 * p + 1], S.t[3 * p + 2]);
-        float3 c = make_float3(0.f, 0.f, 0.f);
-        for (int a = 0; a < nd; ++a) {
-            float3 q = cloud1_point(Ri, Rj, t, npts, a);
-            c.x += q.x;
-            c.y += q.y;
-            c.z += q.z;
-        }
-        {
-            float inv = 1.0f / (float)nd;
-            c.x *= inv;
-            c.y *= inv;
-            c.z *= inv;
-        }
-        if (h == 0) {
-            S.cen[3 * p] = c.x;
-            S.cen[3 * p + 1] = c.y;
-            S.cen[3 * p + 2] = c.z;
-        }
+        const float *Rp = S.R + p * rs;  // the pair's centred points
         float A[Cfg::NA][KC];  // this half's sum_a f_n Y_k, kept in registers for the backward
-        if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, A);
-        else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * DP, A);
+        if (h == 0) half_forward<Cfg, 0>(Rp, nd, inv_rc, S.g0 + p * DP, A);
+        else half_forward<Cfg, 1>(Rp, nd, inv_rc, S.g1 + p * DP, A);
         __syncthreads();
         // ---- 3. net forward + backward on the tensor cores
         {
@@ -656,21 +680,30 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             const float *wl = S.par + net.bias_off[net.nh];
             char *dst = op_tile(S.ops, L2 + 1);
             float esum = 0.f;
-            for (int c0 = h * (Np / 2); c0 < (h + 1) * (Np / 2); c0 += 8) {
-                float z[8], v[8];
-                tc::tmem_ld8(tmem + lane_base + zcol(L2) + c0, z);
+            // this thread's Np / 2 columns from cb: nch chunks of 8, two per TMEM wait
+            const int cb = h * (Np / 2), nch = Np / 16;
+            for (int g = 0; g < nch; g += 2) {
+                float z[2 * 8];
+                tc::tmem_ld8_many<2>(tmem + lane_base + zcol(L2) + cb + 8 * g, min(2, nch - g), z);
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    float zz = z[k] + bias[c0 + k], fz, dfz;
-                    act_pair(net.act, zz, fz, dfz);
-                    if (last) {
-                        esum = fmaf(wl[c0 + k], fz, esum);
-                        v[k] = wl[c0 + k] * dfz;
-                    } else {
-                        v[k] = fz;
+                for (int ch = 0; ch < 2; ++ch) {
+                    if (g + ch < nch) {
+                        const int c0 = cb + 8 * (g + ch);
+                        float v[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            float zz = z[8 * ch + k] + bias[c0 + k], fz, dfz;
+                            act_pair(net.act, zz, fz, dfz);
+                            if (last) {
+                                esum = fmaf(wl[c0 + k], fz, esum);
+                                v[k] = wl[c0 + k] * dfz;
+                            } else {
+                                v[k] = fz;
+                            }
+                        }
+                        store_split8(dst, Np, p, c0, v);
                     }
                 }
-                store_split8(dst, Np, p, c0, v);
             }
             if (last) S.eps[h * kAP + p] = esum;
             tc::fence_before();
@@ -692,21 +725,30 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             if (L2 > 0) {
                 const float *bias = S.par + net.bias_off[L2 - 1];
                 char *dst = op_tile(S.ops, L2);
-                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
-                    float dz[8], z[8], v[8];
-                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
-                    tc::tmem_ld8(tmem + lane_base + zcol(L2 - 1) + c0, z);
+                const int cb = h * (Kp / 2), nch = Kp / 16;
+                for (int ch = 0; ch < nch; ++ch) {  // a chunk of dz and of z per TMEM wait
+                    const int c0 = cb + 8 * ch;
+                    uint32_t r[16];
+                    float x[16];
+                    tc::tmem_ld8_issue(tmem + lane_base + bcol + c0, r);
+                    tc::tmem_ld8_issue(tmem + lane_base + zcol(L2 - 1) + c0, r + 8);
+                    tc::tmem_wait_ld<16>(r, x);
+                    float v[8];
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_dfast(net.act, z[k] + bias[c0 + k]);
+                    for (int k = 0; k < 8; ++k) v[k] = x[k] * act_dfast(net.act, x[8 + k] + bias[c0 + k]);
                     store_split8(dst, Kp, p, c0, v);
                 }
                 tc::fence_async_smem();
             } else {
-                for (int c0 = h * (Kp / 2); c0 < (h + 1) * (Kp / 2); c0 += 8) {
-                    float dg[8];
-                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dg);
+                const int cb = h * (Kp / 2), nch = Kp / 16;
+                for (int g = 0; g < nch; g += 2) {
+                    float dg[2 * 8];
+                    tc::tmem_ld8_many<2>(tmem + lane_base + bcol + cb + 8 * g, min(2, nch - g), dg);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) S.g0[p * DP + c0 + k] = dg[k];
+                    for (int ch = 0; ch < 2; ++ch)
+                        if (g + ch < nch)
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) S.g0[p * DP + cb + 8 * (g + ch) + k] = dg[8 * ch + k];
                 }
             }
             tc::fence_before();
@@ -720,8 +762,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             __syncthreads();
         }
         // ---- descriptor backward
-        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + p * kPartStride, A);
-        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * kPartStride, A);
+        if (h == 0) half_backward<Cfg, 0>(Rp, npts, inv_rc, S.g0 + p * DP, S.part + p * kPartStride, A);
+        else half_backward<Cfg, 1>(Rp, npts, inv_rc, S.g0 + p * DP, S.part + (kAP + p) * kPartStride, A);
         __syncthreads();
         // ---- 5. per-pair forces and torques
         if (tid < kAP) {
@@ -734,6 +776,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 Xi[k] = a0[6 + k] + a1[6 + k];
                 Xj[k] = a0[9 + k] + a1[9 + k];
             }
+            add_centroid_terms(S, p, Si, Sa, Xi, Xj);
             // sums of the rotated points of i and of j: the rotation of the point sum
             const float3 ps = make_float3(S.psum[0], S.psum[1], S.psum[2]);
             const float3 pi3 = rotate_ref(S.q[2 * p], ps), qj3 = rotate_ref(S.q[2 * p + 1], ps);
@@ -877,6 +920,7 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
             Xi[k] = a0[6 + k] + a1[6 + k];
             Xj[k] = a0[9 + k] + a1[9 + k];
         }
+        add_centroid_terms(S, p, Si, Sa, Xi, Xj);
         const float3 ps = make_float3(S.psum[0], S.psum[1], S.psum[2]);
         const float3 pi3 = rotate_ref(S.q[2 * p], ps), qj3 = rotate_ref(S.q[2 * p + 1], ps);
         const float Pi[3] = {pi3.x, pi3.y, pi3.z}, Qj[3] = {qj3.x, qj3.y, qj3.z};
@@ -995,6 +1039,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
     off += (size_t)kAP * kGS * 4;
     S.t = reinterpret_cast<float *>(smem_raw + off);
     off += (size_t)kAP * 3 * 4;
+    S.cen = reinterpret_cast<float *>(smem_raw + off);
+    off += (size_t)kAP * 3 * 4;
     S.part = reinterpret_cast<float *>(smem_raw + off);
     off += (size_t)2 * kAP * kPartStride * 4;
     S.fd = reinterpret_cast<float *>(smem_raw + off);
@@ -1039,28 +1085,15 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             S.t[3 * tid + 2] = tt.z;
             S.ij[2 * tid] = i;
             S.ij[2 * tid + 1] = j;
+            store_centroid(S, tid, npts);
         }
         __syncthreads();
         rotate_tile(S, npts, rs);
         __syncthreads();
-        const float *Ri = S.R + p * rs, *Rj = Ri + 3 * npts;
-        const float3 t = make_float3(S.t[3 * p], S.t[3 * p + 1], S.t[3 * p + 2]);
-        float3 c = make_float3(0.f, 0.f, 0.f);
-        for (int a = 0; a < nd; ++a) {
-            float3 q = cloud1_point(Ri, Rj, t, npts, a);
-            c.x += q.x;
-            c.y += q.y;
-            c.z += q.z;
-        }
-        {
-            float inv = 1.0f / (float)nd;
-            c.x *= inv;
-            c.y *= inv;
-            c.z *= inv;
-        }
+        const float *Rp = S.R + p * rs;  // the pair's centred points
         if (!BWD || !a_rows) {
-            if (h == 0) half_forward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, A);
-            else half_forward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g1 + p * kGS, A);
+            if (h == 0) half_forward<Cfg, 0>(Rp, nd, inv_rc, S.g0 + p * kGS, A);
+            else half_forward<Cfg, 1>(Rp, nd, inv_rc, S.g1 + p * kGS, A);
             if (!BWD && a_tile) {
 #pragma unroll
                 for (int n = 0; n < Cfg::NA; ++n)
@@ -1080,8 +1113,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
             load_dg_rows(S, dg_rows, wt, p0, valid);
         }
         __syncthreads();
-        if (h == 0) half_backward<Cfg, 0>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, S.part + p * kPartStride, A);
-        else half_backward<Cfg, 1>(Ri, Rj, t, npts, c, inv_rc, S.g0 + p * kGS, S.part + (kAP + p) * kPartStride, A);
+        if (h == 0) half_backward<Cfg, 0>(Rp, npts, inv_rc, S.g0 + p * kGS, S.part + p * kPartStride, A);
+        else half_backward<Cfg, 1>(Rp, npts, inv_rc, S.g0 + p * kGS, S.part + (kAP + p) * kPartStride, A);
         __syncthreads();
         adj_finish_tile<MULTI>(S, rs, npts, valid, en_min, en_range, y_rows, p0, F, T, pe, rep, pe_acc, clip);
     }
@@ -1472,7 +1505,7 @@ extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes
 
 static size_t wide_desc_smem(int npts) {
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
-    return align_up((size_t)kAP * rs * 4, 128) + (size_t)kAP * kGS * 4 * 2 + (size_t)kAP * 3 * 4 +
+    return align_up((size_t)kAP * rs * 4, 128) + (size_t)kAP * kGS * 4 * 2 + (size_t)kAP * 3 * 4 * 2 +
            (size_t)2 * kAP * kPartStride * 4 + (size_t)kAP * 9 * 4 + (size_t)kAP * 2 * 4 + (size_t)3 * npts * 4 +
            (size_t)kAP * 32 + 16;
 }

@@ -65,15 +65,40 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
 }
 
-// 8 consecutive 32-bit columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
-    uint32_t r[8];
+__device__ __forceinline__ void tmem_ld8_issue(uint32_t taddr, uint32_t *r) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(taddr));
+}
+
+// After tcgen05.wait::ld: the empty statements redefine the loaded registers,
+// so that no use of them can be scheduled above the wait.
+template <int N>
+__device__ __forceinline__ void tmem_wait_ld(uint32_t *r, float *v) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = __uint_as_float(r[k]);
+    for (int k = 0; k < N; ++k) {
+        asm volatile("" : "+r"(r[k]));
+        v[k] = __uint_as_float(r[k]);
+    }
+}
+
+// 8 consecutive 32-bit columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
+    uint32_t r[8];
+    tmem_ld8_issue(taddr, r);
+    tmem_wait_ld<8>(r, v);
+}
+
+// n (<= NMAX, warp-uniform) chunks of 8 columns at taddr, taddr + 8, ... with
+// one wait for all of them; v[8 c + k] is column 8 c + k.
+template <int NMAX>
+__device__ __forceinline__ void tmem_ld8_many(uint32_t taddr, int n, float *v) {
+    uint32_t r[8 * NMAX];
+#pragma unroll
+    for (int c = 0; c < NMAX; ++c)
+        if (c < n) tmem_ld8_issue(taddr + 8 * c, r + 8 * c);
+    tmem_wait_ld<8 * NMAX>(r, v);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
