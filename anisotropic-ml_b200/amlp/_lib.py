@@ -66,6 +66,33 @@ class Replica(ctypes.Structure):
                 ("box", ctypes.c_float), ("nve", ctypes.c_int), ("pad", ctypes.c_int * 3)]
 
 
+class SimConfig(ctypes.Structure):
+    """``amlp_sim_config``: parameters of a simulation handle."""
+    _fields_ = [("n", ctypes.c_int), ("nrad", ctypes.c_int), ("nang", ctypes.c_int), ("lmax", ctypes.c_int),
+                ("kT", ctypes.c_float), ("dt", ctypes.c_float), ("tau", ctypes.c_float), ("nve", ctypes.c_int),
+                ("initial_ke_quirk", ctypes.c_int), ("nlist_every", ctypes.c_int), ("skin", ctypes.c_double),
+                ("dx", ctypes.c_float), ("dteta", ctypes.c_float)]
+
+
+class PoolConfig(ctypes.Structure):
+    """``amlp_pool_config``: shape, net and integrator of a serving pool."""
+    _fields_ = [("nrad", ctypes.c_int), ("nang", ctypes.c_int), ("lmax", ctypes.c_int), ("dt", ctypes.c_float),
+                ("tau", ctypes.c_float), ("h_pts", ctypes.c_void_p), ("npts", ctypes.c_int),
+                ("en_min", ctypes.c_float), ("en_max", ctypes.c_float), ("cutoff", ctypes.c_double),
+                ("nep_cutoff", ctypes.c_float), ("skin", ctypes.c_double), ("h_moi", ctypes.c_void_p),
+                ("mlp", ctypes.POINTER(Mlp))]
+
+
+class PoolSystem(ctypes.Structure):
+    """``amlp_pool_system``: one system admitted to a pool (host arrays)."""
+    _fields_ = [("n", ctypes.c_int), ("box", ctypes.c_float), ("kT", ctypes.c_float), ("nve", ctypes.c_int),
+                ("verlet_cap", ctypes.c_longlong), ("h_pos", ctypes.c_void_p), ("h_quat", ctypes.c_void_p),
+                ("h_vel", ctypes.c_void_p), ("h_angmom", ctypes.c_void_p), ("h_mass", ctypes.c_void_p)]
+
+
+FORCES = {"fd": 0, "adjoint": 1}
+POOL_ACTIVE, POOL_PENDING = 0, 1
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _LL = ctypes.c_longlong
@@ -109,6 +136,32 @@ SIGNATURES = {
     "amlp_multi_nvt_init": [_P, _P, _P, _P, _P, _I, _I, ctypes.POINTER(Nvt), _P, _P],
     "amlp_multi_nvt_step_two": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _P, ctypes.POINTER(Nvt), _P, _P],
     "amlp_multi_nvt_step_one": [_P, _P, _P, _P, _P, _P, _P, _P, _I, _P, ctypes.POINTER(Nvt), _P, _P],
+    # simulation handles and the serving pool (handles are opaque pointers)
+    "amlp_create": [ctypes.POINTER(SimConfig), ctypes.POINTER(_P)],
+    "amlp_set_shape": [_P, _P, _I, _F, _F, _D, _F],
+    "amlp_set_model": [_P, ctypes.POINTER(Mlp), _P],
+    "amlp_set_state": [_P, _P, _P, _P, _P, _P, _P, _F, _P],
+    "amlp_build_nlist": [_P, _P],
+    "amlp_sim_descriptors": [_P, _P, _P, _LL, ctypes.POINTER(_LL), _P],
+    "amlp_forces": [_P, _P, _P, _I, _P],
+    "amlp_step": [_P, _I, _I, _P],
+    "amlp_get_state": [_P, _P, _P, _P, _P, _P],
+    "amlp_get_thermostat": [_P, ctypes.POINTER(Thermostat), _P],
+    "amlp_pool_create": [ctypes.POINTER(PoolConfig), ctypes.POINTER(_P)],
+    "amlp_pool_admit": [_P, ctypes.POINTER(PoolSystem), ctypes.POINTER(_I)],
+    "amlp_pool_evict": [_P, _I, _P, _P, _P, _P, ctypes.POINTER(Thermostat)],
+    "amlp_pool_step_segment": [_P, _I, _P],
+    "amlp_pool_system_status": [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_LL), ctypes.POINTER(Thermostat)],
+}
+
+# entry points that do not return a status: name -> (argtypes, restype)
+OTHER_SIGNATURES = {
+    "amlp_destroy": ([_P], None),
+    "amlp_timestep": ([_P], _LL),
+    "amlp_last_error": ([_P], ctypes.c_char_p),
+    "amlp_pool_destroy": ([_P], None),
+    "amlp_pool_size": ([_P], _I),
+    "amlp_pool_last_error": ([_P], ctypes.c_char_p),
 }
 
 lib.amlp_version.restype = ctypes.c_int
@@ -119,6 +172,10 @@ for _name, _args in SIGNATURES.items():
     _fn = getattr(lib, _name)
     _fn.argtypes = _args
     _fn.restype = ctypes.c_int
+for _name, (_args, _res) in OTHER_SIGNATURES.items():
+    _fn = getattr(lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = _res
 
 
 def status_string(s: int) -> str:
@@ -151,4 +208,4 @@ def device_error(clear: bool = True) -> int:
 
 
 def exported_symbols() -> list[str]:
-    return ["amlp_version", "amlp_status_string", "amlp_last_cuda_error"] + list(SIGNATURES)
+    return ["amlp_version", "amlp_status_string", "amlp_last_cuda_error"] + list(SIGNATURES) + list(OTHER_SIGNATURES)

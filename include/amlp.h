@@ -16,8 +16,10 @@
  *     angular momenta (N,4) f32 as (w,x,y,z) quaternions (HOOMD convention),
  *     forces/torques (N,3) f32, pair lists (P,2) with i < j. Pair indices are
  *     int32 here (the reference keeps int64 from scipy).
- *   - Handles are not used; calls on one stream are ordered, calls on
- *     different streams that share output buffers race.
+ *   - The stateless calls take every buffer from the caller; calls on one
+ *     stream are ordered, calls on different streams that share output
+ *     buffers race. The handles at the end of this file (amlp_sim,
+ *     amlp_pool) own their buffers and sequence those calls.
  *
  * Reference interfaces replaced (paths inside the reference project):
  *   amlp_nlist_build      Sim.setNeighborList / Sim.refreshNList   Sim.py:85-92, :192-198
@@ -300,6 +302,127 @@ amlp_status amlp_multi_nvt_step_one(float *d_pos, float *d_vel, const float *d_a
                                     float *d_angmom, const float *d_dp, const float *d_mass, const int *d_rep, int n,
                                     const amlp_replica *d_rp, const amlp_nvt *prm, amlp_thermostat *d_th,
                                     void *stream);
+
+/* --------------------------------------------------------------- simulation handles
+ * A handle owns one system's device state and buffers and runs the reference's
+ * step (Sim.step, Sim.py:257-285) through the calls above. It rebuilds the
+ * Verlet list every nlist_every steps (Sim.py:87, :218-221) and replays the
+ * steps in between as one CUDA graph. Reference interfaces replaced:
+ *   amlp_create / amlp_destroy   Sim.__init__ + setDevice + setNepDescriptors + setkT + setdt
+ *                                Sim.py:14-25, :67-74, :99-116
+ *   amlp_set_state               initializeSystem + move_data_to_device   Sim.py:27-51, :147-169
+ *   amlp_set_shape               setShape   Sim.py:76-83, DescriptorGenerator.py:58-125
+ *   amlp_set_model               setEvaluator (weights already on the device)   Sim.py:53-65
+ *   amlp_build_nlist             setNeighborList / refreshNList   Sim.py:85-92, :192-198
+ *   amlp_sim_descriptors         DescriptorGenerator.generate_nep_descriptors   DescriptorGenerator.py:136-161
+ *                                (named apart from the stateless amlp_descriptors above)
+ *   amlp_forces                  descriptors + ForceEvaluator.evaluate_interactions   Sim.py:261-266
+ *   amlp_step                    Sim.run   Sim.py:207-255
+ *   amlp_get_state, amlp_get_thermostat   the arrays and integrator variables Sim.dumpConfig writes
+ *                                Sim.py:117-145
+ * Order: create, then set_shape, set_model and set_state (any order), then
+ * the rest. set_state resets the time step to 0 and computes the initial
+ * kinetic energies (amlp_nvt_init). A handle is used from one host thread at a
+ * time; its work is ordered on the stream each call gets, and calls that read
+ * a count back (build_nlist, sim_descriptors, step when it rebuilds)
+ * synchronise that stream. d_* arguments are device memory, copied in or out. */
+typedef struct amlp_sim amlp_sim;
+
+typedef struct amlp_sim_config {
+    int n;                    /* bodies */
+    int nrad, nang, lmax;     /* descriptor hypers (setNepDescriptors) */
+    float kT, dt;             /* setkT, setdt */
+    float tau;                /* thermostat time constant; <= 0: float(100 dt) as Sim.py:115 */
+    int nve;                  /* 1: no thermostat */
+    int initial_ke_quirk;     /* 1: the reference's first-step kinetic energy (amlp_nvt_init) */
+    int nlist_every;          /* Verlet rebuild period; <= 0: 100 */
+    double skin;              /* Verlet radius = cutoff + skin; <= 0: 2.0 (Sim.py:86) */
+    float dx, dteta;          /* finite-difference steps; <= 0: 1e-5 (Sim.py:49-50) */
+} amlp_sim_config;
+
+#define AMLP_FORCES_FD 0          /* the reference's finite differences (amlp_forces_fd) */
+#define AMLP_FORCES_ADJOINT 1     /* analytic forces (amlp_forces_adjoint / _wide by net width) */
+
+amlp_status amlp_create(const amlp_sim_config *cfg, amlp_sim **out);
+void amlp_destroy(amlp_sim *h);
+/* h_pts: host (npts,3) body-frame points. */
+amlp_status amlp_set_shape(amlp_sim *h, const float *h_pts, int npts, float en_min, float en_max,
+                           double cutoff, float nep_cutoff);
+/* mlp->d_w (device) is copied; dims[0] must equal the descriptor length. */
+amlp_status amlp_set_model(amlp_sim *h, const amlp_mlp *mlp, void *stream);
+/* h_moi: host, 3 principal moments shared by the bodies. */
+amlp_status amlp_set_state(amlp_sim *h, const float *d_pos, const float *d_quat, const float *d_vel,
+                           const float *d_angmom, const float *d_mass, const float *h_moi, float box,
+                           void *stream);
+amlp_status amlp_build_nlist(amlp_sim *h, void *stream);
+/* Filters the pairs and writes g_all (10 P rows of D, amlp_descriptors'
+ * layout) to d_g and the filtered pairs to d_pairs (P x 2 int32); *h_P gets P.
+ * With P > cap nothing is written and AMLP_ERR_CAPACITY is returned. */
+amlp_status amlp_sim_descriptors(amlp_sim *h, float *d_g, int *d_pairs, long long cap, long long *h_P,
+                                 void *stream);
+/* One force pass (filter, forces, torques, pair-energy sum) on the current
+ * state; d_F, d_T (N,3) receive copies when not NULL. */
+amlp_status amlp_forces(amlp_sim *h, float *d_F, float *d_T, int mode, void *stream);
+amlp_status amlp_step(amlp_sim *h, int nsteps, int mode, void *stream);
+/* Any of the outputs may be NULL. */
+amlp_status amlp_get_state(amlp_sim *h, float *d_pos, float *d_quat, float *d_vel, float *d_angmom,
+                           void *stream);
+amlp_status amlp_get_thermostat(amlp_sim *h, amlp_thermostat *h_th, void *stream);
+long long amlp_timestep(const amlp_sim *h);
+/* Message of the last failed call on h ("" when none). */
+const char *amlp_last_error(const amlp_sim *h);
+
+/* --------------------------------------------------------------- serving pool
+ * Many independent systems of one shape and one net, resident on one GPU and
+ * advanced together. Each pool step runs one launch per stage over every
+ * system (amlp_multi_*). No reference counterpart: the reference runs one
+ * system per process. Admitted systems join, and evicted ones leave, between
+ * segments. A segment rebuilds every system's Verlet list and then replays its
+ * steps as one CUDA graph. The status is kept per system. */
+typedef struct amlp_pool amlp_pool;
+
+typedef struct amlp_pool_config {
+    int nrad, nang, lmax;
+    float dt, tau;            /* tau <= 0: float(100 dt) */
+    const float *h_pts;       /* host (npts,3) */
+    int npts;
+    float en_min, en_max;
+    double cutoff;
+    float nep_cutoff;
+    double skin;              /* <= 0: 2.0 */
+    const float *h_moi;       /* host, 3 */
+    const amlp_mlp *mlp;      /* d_w (device) is copied */
+} amlp_pool_config;
+
+typedef struct amlp_pool_system {
+    int n;
+    float box, kT;
+    int nve;
+    long long verlet_cap;     /* capacity of its Verlet list; <= 0: 1.5 x the ideal-gas pair
+                                 count at radius cutoff + skin, plus 4 n + 1024 */
+    /* host arrays, copied: (n,3), (n,4), (n,3), (n,4), (n) */
+    const float *h_pos, *h_quat, *h_vel, *h_angmom, *h_mass;
+} amlp_pool_system;
+
+/* Per-system status (amlp_pool_system_status). A system whose Verlet list
+ * outgrows its capacity gets a larger one at the next segment. */
+#define AMLP_POOL_ACTIVE 0          /* packed and stepping */
+#define AMLP_POOL_PENDING 1         /* admitted; joins at the next segment */
+
+amlp_status amlp_pool_create(const amlp_pool_config *cfg, amlp_pool **out);
+void amlp_pool_destroy(amlp_pool *p);
+/* Adds a system (thermostat at the reference's seeds); *id identifies it. */
+amlp_status amlp_pool_admit(amlp_pool *p, const amlp_pool_system *sys, int *id);
+/* Removes a system, copying its state to the host arrays given (any may be
+ * NULL) and its thermostat to *h_th (may be NULL). */
+amlp_status amlp_pool_evict(amlp_pool *p, int id, float *h_pos, float *h_quat, float *h_vel, float *h_angmom,
+                            amlp_thermostat *h_th);
+/* nsteps steps of every active system (adjoint forces). Synchronises the stream. */
+amlp_status amlp_pool_step_segment(amlp_pool *p, int nsteps, void *stream);
+amlp_status amlp_pool_system_status(amlp_pool *p, int id, int *status, long long *steps_done,
+                                    amlp_thermostat *h_th);
+int amlp_pool_size(const amlp_pool *p);
+const char *amlp_pool_last_error(const amlp_pool *p);
 
 #ifdef __cplusplus
 }

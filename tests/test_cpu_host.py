@@ -20,7 +20,7 @@ def lib():
 
 def _declared():
     text = open(os.path.join(REPO, "include", "amlp.h")).read()
-    decl = r"^(?:amlp_status|int|const char \*)\s*\*?(amlp_[a-z0-9_]+)\s*\("
+    decl = r"^(?:amlp_status|int|void|long long|const char \*)\s*\*?(amlp_[a-z0-9_]+)\s*\("
     return sorted(set(re.findall(decl, text, flags=re.M)))
 
 
@@ -52,6 +52,22 @@ def test_argument_validation_without_gpu(lib):
     assert lib.call_status("amlp_descriptors", 1, 1, 10.0, 1, 1, ctypes.byref(n), 1, None) == 2
     with pytest.raises(lib.AmlpError):
         lib.call("amlp_nvt_workspace_bytes", -5, ctypes.byref(sz))
+    # simulation handles and the pool: null and out-of-range arguments, no CUDA call
+    h = ctypes.c_void_p()
+    assert lib.call_status("amlp_create", None, ctypes.byref(h)) == 1 and not h.value
+    cfg = lib.SimConfig()
+    cfg.n, cfg.nrad, cfg.nang, cfg.lmax, cfg.dt = 0, 10, 8, 4, 0.005
+    assert lib.call_status("amlp_create", ctypes.byref(cfg), ctypes.byref(h)) == 1 and not h.value
+    assert lib.call_status("amlp_step", None, 1, 0, None) == 1
+    assert lib.lib.amlp_last_error(None) == b"null handle"
+    assert lib.lib.amlp_timestep(None) == -1
+    lib.lib.amlp_destroy(None)
+    assert lib.call_status("amlp_pool_create", None, ctypes.byref(h)) == 1
+    pc = lib.PoolConfig()
+    assert lib.call_status("amlp_pool_create", ctypes.byref(pc), ctypes.byref(h)) == 1 and not h.value
+    assert lib.lib.amlp_pool_size(None) == 0
+    assert lib.call_status("amlp_pool_step_segment", None, 1, None) == 1
+    lib.lib.amlp_pool_destroy(None)
 
 
 def test_gsd_reads_hoomd_file_and_roundtrips(tmp_path):
