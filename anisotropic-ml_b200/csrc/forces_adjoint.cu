@@ -410,6 +410,11 @@ __device__ __forceinline__ void body_point_sum(const AdjShared &S, int npts) {
 __device__ __forceinline__ char *op_tile(char *ops, int k) { return ops + (k & 1) * (2 * kAP * kWpad * 2); }
 
 // A (128 x K) times B, three split terms, into TMEM columns at d_tmem.
+// STEP_DESC: build the four descriptors of K-step 0 once and move only their
+// start address (bits 0-13, in 16-byte units, below 2^14 for any shared-memory
+// address) from step to step; otherwise build them per MMA. Measured: stepping
+// is 0.4 % faster in the fused kernel (K <= 64) and 0.7 % slower in k_mlp_grad.
+template <bool STEP_DESC>
 __device__ __forceinline__ void mma3(uint32_t d_tmem, const char *a_hi, int K, const char *b_hi, size_t b_lo_off,
                                      int N, bool b_mn, int b_kstride /* bytes per K-step of 16 */, uint32_t b_lbo,
                                      uint32_t b_sbo) {
@@ -417,12 +422,25 @@ __device__ __forceinline__ void mma3(uint32_t d_tmem, const char *a_hi, int K, c
     const uint32_t a0 = tc::smem_u32(a_hi), a1 = a0 + (uint32_t)(kAP * K * 2);
     const uint32_t b0 = tc::smem_u32(b_hi), b1 = b0 + (uint32_t)b_lo_off;
     const uint32_t a_sbo = (uint32_t)K * 16;
-    for (int ks = 0; ks < K / 16; ++ks) {
-        const uint32_t ao = ks * 256, bo = ks * b_kstride;
-        tc::mma_bf16(d_tmem, tc::smem_desc(a0 + ao, 128, a_sbo), tc::smem_desc(b0 + bo, b_lbo, b_sbo), idesc,
-                     ks > 0 ? 1u : 0u);
-        tc::mma_bf16(d_tmem, tc::smem_desc(a0 + ao, 128, a_sbo), tc::smem_desc(b1 + bo, b_lbo, b_sbo), idesc, 1u);
-        tc::mma_bf16(d_tmem, tc::smem_desc(a1 + ao, 128, a_sbo), tc::smem_desc(b0 + bo, b_lbo, b_sbo), idesc, 1u);
+    if constexpr (STEP_DESC) {
+        const uint64_t da = tc::smem_desc(a0, 128, a_sbo), da1 = tc::smem_desc(a1, 128, a_sbo);
+        const uint64_t db = tc::smem_desc(b0, b_lbo, b_sbo), db1 = tc::smem_desc(b1, b_lbo, b_sbo);
+        for (int ks = 0; ks < K / 16; ++ks) {
+            const uint64_t oa = (uint64_t)(ks * 16), ob = (uint64_t)((ks * b_kstride) >> 4);
+            tc::mma_bf16(d_tmem, da + oa, db + ob, idesc, ks > 0 ? 1u : 0u);
+            tc::mma_bf16(d_tmem, da + oa, db1 + ob, idesc, 1u);
+            tc::mma_bf16(d_tmem, da1 + oa, db + ob, idesc, 1u);
+        }
+    } else {
+        for (int ks = 0; ks < K / 16; ++ks) {
+            const uint32_t ao = ks * 256, bo = ks * b_kstride;
+            tc::mma_bf16(d_tmem, tc::smem_desc(a0 + ao, 128, a_sbo), tc::smem_desc(b0 + bo, b_lbo, b_sbo), idesc,
+                         ks > 0 ? 1u : 0u);
+            tc::mma_bf16(d_tmem, tc::smem_desc(a0 + ao, 128, a_sbo), tc::smem_desc(b1 + bo, b_lbo, b_sbo), idesc,
+                         1u);
+            tc::mma_bf16(d_tmem, tc::smem_desc(a1 + ao, 128, a_sbo), tc::smem_desc(b0 + bo, b_lbo, b_sbo), idesc,
+                         1u);
+        }
     }
 }
 
@@ -585,7 +603,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         for (int k = tid; k < kWpad; k += kAThreads) S.par[net.bias_off[net.nh] + k] = k < K ? Wl[k] : 0.f;
         if (tid == 0) S.par[net.bias_off[net.nh] + kWpad] = Wl[K];  // last bias
     }
-    if (warp == 0) tc::tmem_alloc(&tmem_slot, 256);
+    if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);
     if (tid == 0) {
         tc::mbar_init(&mbar, 1);
         abort_flag = 0;
@@ -597,9 +615,11 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     const uint32_t tmem = tmem_slot;
     const uint32_t bar = tc::smem_u32(&mbar);
     uint32_t phase = 0;
-    // TMEM column regions: Z_k (hidden layer k) at 64k, backward product at 192, dE/dg at 192 too
+    // TMEM column regions: Z_k (hidden layer k) at 64k, backward product at 192, dE/dg at 192 too,
+    // act'(Z_k) of the hidden layers before the last at 256 + 64k
     auto zcol = [&](int k) { return (uint32_t)(k * kWpad); };
     const uint32_t bcol = (uint32_t)(3 * kWpad);
+    auto dfcol = [&](int k) { return (uint32_t)(4 * kWpad + k * kWpad); };
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
 
     auto wait_mma = [&]() -> bool {
@@ -668,7 +688,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             if (tid == 0 && !abort_flag) {
                 tc::fence_after();
                 const char *wb = S.wts + net.wsm_off[L2];
-                mma3(tmem + zcol(L2), op_tile(S.ops, L2), Kp, wb, (size_t)Np * Kp * 2, Np, false, 256, 128,
+                mma3<true>(tmem + zcol(L2), op_tile(S.ops, L2), Kp, wb, (size_t)Np * Kp * 2, Np, false, 256, 128,
                      (uint32_t)Kp * 16);
                 tc::commit(bar);
             }
@@ -689,7 +709,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 for (int ch = 0; ch < 2; ++ch) {
                     if (g + ch < nch) {
                         const int c0 = cb + 8 * (g + ch);
-                        float v[8];
+                        float v[8], dv[8];
 #pragma unroll
                         for (int k = 0; k < 8; ++k) {
                             float zz = z[8 * ch + k] + bias[c0 + k], fz, dfz;
@@ -699,13 +719,16 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                                 v[k] = wl[c0 + k] * dfz;
                             } else {
                                 v[k] = fz;
+                                dv[k] = dfz;
                             }
                         }
                         store_split8(dst, Np, p, c0, v);
+                        if (!last) tc::tmem_st8(tmem + lane_base + dfcol(L2) + c0, dv);  // for the backward
                     }
                 }
             }
             if (last) S.eps[h * kAP + p] = esum;
+            else tc::tmem_wait_st();
             tc::fence_before();
             tc::fence_async_smem();
             __syncthreads();
@@ -717,25 +740,24 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 tc::fence_after();
                 const char *wb = S.wts + net.wsm_off[L2];
                 // B = W_k read as MN-major (the transpose): N' = Kp, K' = Np
-                mma3(tmem + bcol, op_tile(S.ops, L2 + 1), Np, wb, (size_t)Np * Kp * 2, Kp, true,
+                mma3<true>(tmem + bcol, op_tile(S.ops, L2 + 1), Np, wb, (size_t)Np * Kp * 2, Kp, true,
                      2 * Kp * 16, (uint32_t)Kp * 16, 128);
                 tc::commit(bar);
             }
             wait_mma();
             if (L2 > 0) {
-                const float *bias = S.par + net.bias_off[L2 - 1];
                 char *dst = op_tile(S.ops, L2);
                 const int cb = h * (Kp / 2), nch = Kp / 16;
-                for (int ch = 0; ch < nch; ++ch) {  // a chunk of dz and of z per TMEM wait
+                for (int ch = 0; ch < nch; ++ch) {  // a chunk of dz and of act'(z) per TMEM wait
                     const int c0 = cb + 8 * ch;
                     uint32_t r[16];
                     float x[16];
                     tc::tmem_ld8_issue(tmem + lane_base + bcol + c0, r);
-                    tc::tmem_ld8_issue(tmem + lane_base + zcol(L2 - 1) + c0, r + 8);
+                    tc::tmem_ld8_issue(tmem + lane_base + dfcol(L2 - 1) + c0, r + 8);
                     tc::tmem_wait_ld<16>(r, x);
                     float v[8];
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) v[k] = x[k] * act_dfast(net.act, x[8 + k] + bias[c0 + k]);
+                    for (int k = 0; k < 8; ++k) v[k] = x[k] * x[8 + k];
                     store_split8(dst, Kp, p, c0, v);
                 }
                 tc::fence_async_smem();
@@ -872,7 +894,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     __syncthreads();
     if (warp == 0) {
         tc::fence_after();
-        tc::tmem_dealloc(tmem, 256);
+        tc::tmem_dealloc(tmem, 512);
     }
 }
 
@@ -1284,8 +1306,8 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             if (tid == 0) ensure();
             if (tid == 0 && !abort_flag) {
                 tc::fence_after();
-                mma3(tmem + (uint32_t)(L2 * kWideMax), tile(L2), Kp, wbuf, (size_t)Np * Kp * 2, Np, false, 256, 128,
-                     (uint32_t)Kp * 16);
+                mma3<false>(tmem + (uint32_t)(L2 * kWideMax), tile(L2), Kp, wbuf, (size_t)Np * Kp * 2, Np, false,
+                            256, 128, (uint32_t)Kp * 16);
                 tc::commit(bar);
             }
             wait_mma();
@@ -1326,7 +1348,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             if (tid == 0) ensure();
             if (tid == 0 && !abort_flag) {
                 tc::fence_after();
-                mma3(tmem + bcol, tile(L2 + 1), Np, wbuf, (size_t)Np * Kp * 2, Kp, true, 2 * Kp * 16,
+                mma3<false>(tmem + bcol, tile(L2 + 1), Np, wbuf, (size_t)Np * Kp * 2, Kp, true, 2 * Kp * 16,
                      (uint32_t)Kp * 16, 128);
                 tc::commit(bar);
             }
