@@ -282,7 +282,7 @@ __device__ __forceinline__ void half_backward(const float *r, int npts, float in
     float grad_rad[Cfg::NR];
 #pragma unroll
     for (int n = 0; n < Cfg::NR; ++n) grad_rad[n] = H == 0 ? dg[n] : 0.f;
-    float Si[3] = {0, 0, 0}, Sa[3] = {0, 0, 0}, Xi[3] = {0, 0, 0}, Xj[3] = {0, 0, 0};
+    float Si[3] = {0, 0, 0}, Sj[3] = {0, 0, 0}, Xi[3] = {0, 0, 0}, Xj[3] = {0, 0, 0};
     const int nd = 2 * npts;
     for (int a = 0; a < nd; ++a) {
         const float rx = r[3 * a], ry = r[3 * a + 1], rz = r[3 * a + 2];
@@ -340,14 +340,12 @@ __device__ __forceinline__ void half_backward(const float *r, int npts, float in
             gy = fmaf(V[m], C[m - 1], fmaf(-U[m], Sn[m - 1], gy));
             gz = fmaf(Wc[m], C[m], fmaf(Ws[m], Sn[m], gz));
         }
-        // dE/dr = gr rhat + (g - rhat (rhat . g)) / d
-        float dot = ux * gx + uy * gy + uz * gz;
-        float Gx = gr * ux + (gx - ux * dot) * inv_d;
-        float Gy = gr * uy + (gy - uy * dot) * inv_d;
-        float Gz = gr * uz + (gz - uz * dot) * inv_d;
-        Sa[0] += Gx;
-        Sa[1] += Gy;
-        Sa[2] += Gz;
+        // dE/dr = gr rhat + (g - rhat (rhat . g)) / d = rhat (gr - (rhat . g) / d) + g / d
+        const float dot = ux * gx + uy * gy + uz * gz;
+        const float c1 = fmaf(-dot, inv_d, gr);
+        const float Gx = fmaf(ux, c1, gx * inv_d);
+        const float Gy = fmaf(uy, c1, gy * inv_d);
+        const float Gz = fmaf(uz, c1, gz * inv_d);
         if (a < npts) {
             Si[0] += Gx;
             Si[1] += Gy;
@@ -356,6 +354,9 @@ __device__ __forceinline__ void half_backward(const float *r, int npts, float in
             Xi[1] += rz * Gx - rx * Gz;
             Xi[2] += rx * Gy - ry * Gx;
         } else {
+            Sj[0] += Gx;
+            Sj[1] += Gy;
+            Sj[2] += Gz;
             Xj[0] += ry * Gz - rz * Gy;
             Xj[1] += rz * Gx - rx * Gz;
             Xj[2] += rx * Gy - ry * Gx;
@@ -364,7 +365,7 @@ __device__ __forceinline__ void half_backward(const float *r, int npts, float in
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         out[k] = Si[k];
-        out[3 + k] = Sa[k];
+        out[3 + k] = Si[k] + Sj[k];
         out[6 + k] = Xi[k];
         out[9 + k] = Xj[k];
     }
