@@ -70,13 +70,13 @@ LAUNCHES = {"amlp_nlist_build": 11, "amlp_pair_filter": 2, "amlp_forces_fd": 1, 
 # dram__bytes_read.sum + dram__bytes_write.sum at 32,768 cube26 bodies (436,636 pairs; the kernels'
 # profiles give the command). The traffic grows with the pairs (a capture at 131,072 bodies gave the
 # same bytes per pair), so the roofline's traffic is this figure times the launch's pairs.
-DRAM_BYTES_PER_PAIR = {"adjoint": 5.340672e6 / 436636, "fd": 5.318912e6 / 436636}
+DRAM_BYTES_PER_PAIR = {"adjoint": 5.340928e6 / 436636, "fd": 5.318912e6 / 436636}
 # The wide path (nets wider than 64) stores each pair's descriptor row, harmonic sums and dE/dg in
 # HBM between its three launches: the sum over k_adj_desc forward, k_mlp_grad and k_adj_desc backward
 # captured at 32,768 cyl24 bodies (381,342 pairs). The per-pair rows do not depend on the shape or the
 # net, so the figure serves every wide workload.
-DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.039936e6 + 349.910784e6 + 79.480064e6 + 26.586624e6 + 409.201152e6
-                                       + 4.866304e6) / 381342
+DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.084992e6 + 349.997824e6 + 79.480064e6 + 26.586624e6 + 409.252608e6
+                                       + 4.352e6) / 381342
 
 
 def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS):
