@@ -1,8 +1,10 @@
 // Pair filter of DescriptorGenerator.pos_to_pts (DescriptorGenerator.py:168-182):
 // minimum-image translation in FP32 and |t| < cutoff (compared in double, the
 // reference's cutoff being a Python float), keeping the Verlet order.
-// Two passes over a fixed grid of chunks: count per chunk, then every block
-// sums the counts of the chunks before it and writes its kept pairs in order.
+// Two passes over a fixed grid of chunks: the first tests every pair, stores
+// one keep bit per pair and counts per chunk; the second sums the counts of
+// the chunks before its own and writes the kept pairs in order, reading the
+// bits instead of testing the pairs again.
 #include "common.cuh"
 
 namespace amlp {
@@ -56,23 +58,35 @@ __device__ __forceinline__ unsigned keep_mask(const float *pos, const int *vp, l
     return m;
 }
 
-// Chunks of whole rounds' alignment (multiples of kFilterItems pairs, so the
-// 16-byte loads are aligned).
+// Chunks of whole 32-pair words of the keep bits (and so multiples of
+// kFilterItems pairs: the 16-byte loads are aligned).
 __device__ __forceinline__ void chunk_range(long long nv, long long *s, long long *e) {
     long long chunk = (nv + gridDim.x - 1) / gridDim.x;
-    chunk = (chunk + kFilterItems - 1) / kFilterItems * kFilterItems;
+    chunk = (chunk + 31) / 32 * 32;
     *s = min(nv, (long long)blockIdx.x * chunk);
     *e = min(nv, *s + chunk);
 }
 
 __global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *pos, BoxOf L, double cutoff, const int *vp,
-                                                                 const long long *d_nv, long long cap, int *counts) {
+                                                                 const long long *d_nv, long long cap, int *counts,
+                                                                 unsigned *bits) {
     long long nv = min(*d_nv, cap), s, e;
     chunk_range(nv, &s, &e);
+    const int lane = threadIdx.x & 31;
     int c = 0;
     int ij[2 * kFilterItems];
-    for (long long k0 = s + (long long)threadIdx.x * kFilterItems; k0 < e; k0 += kFilterRound)
-        c += __popc(keep_mask(pos, vp, k0, e, L, cutoff, ij));
+    // every thread of a warp runs the same rounds (a round starts at s + multiple of 1024)
+    for (long long r0 = s; r0 < e; r0 += kFilterRound) {
+        const long long k0 = r0 + (long long)threadIdx.x * kFilterItems;
+        const unsigned m = k0 < e ? keep_mask(pos, vp, k0, e, L, cutoff, ij) : 0u;
+        c += __popc(m);
+        // eight lanes' four bits make the 32-bit word of pairs k0 - 4 (lane % 8) ...
+        unsigned w = m << (4 * (lane & 7));
+        w |= __shfl_xor_sync(0xffffffffu, w, 1);
+        w |= __shfl_xor_sync(0xffffffffu, w, 2);
+        w |= __shfl_xor_sync(0xffffffffu, w, 4);
+        if ((lane & 7) == 0 && k0 < e) bits[k0 >> 5] = w;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     __shared__ int ws[kFilterThreads / 32];
@@ -85,8 +99,8 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *po
     }
 }
 
-__global__ void __launch_bounds__(kFilterThreads) k_filter_write(const float *pos, BoxOf L, double cutoff, const int *vp,
-                                                                 const long long *d_nv, long long cap, const int *counts,
+__global__ void __launch_bounds__(kFilterThreads) k_filter_write(const int *vp, const long long *d_nv, long long cap,
+                                                                 const int *counts, const unsigned *bits, int vec,
                                                                  int *out, long long *d_np) {
     __shared__ long long base_s;
     __shared__ int wsum[kFilterThreads / 32];
@@ -106,7 +120,22 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_write(const float *po
     int ij[2 * kFilterItems];
     for (long long r0 = s; r0 < e; r0 += kFilterRound) {
         const long long k0 = r0 + (long long)threadIdx.x * kFilterItems;
-        const unsigned m = k0 < e ? keep_mask(pos, vp, k0, e, L, cutoff, ij) : 0u;
+        const unsigned m = k0 < e ? (bits[k0 >> 5] >> (k0 & 31)) & ((1u << kFilterItems) - 1u) : 0u;
+        if (m) {  // the pair rows of this thread's group, only when one of them is kept
+            if (vec && k0 + kFilterItems <= e) {
+                const int4 a = *reinterpret_cast<const int4 *>(vp + 2 * k0);
+                const int4 b = *reinterpret_cast<const int4 *>(vp + 2 * k0 + 4);
+                ij[0] = a.x; ij[1] = a.y; ij[2] = a.z; ij[3] = a.w;
+                ij[4] = b.x; ij[5] = b.y; ij[6] = b.z; ij[7] = b.w;
+            } else {
+#pragma unroll
+                for (int u = 0; u < kFilterItems; ++u) {
+                    const bool in = k0 + u < e;
+                    ij[2 * u] = in ? vp[2 * (k0 + u)] : 0;
+                    ij[2 * u + 1] = in ? vp[2 * (k0 + u) + 1] : 0;
+                }
+            }
+        }
         // block-wide exclusive scan of the kept counts (thread order = pair order)
         const int cnt = __popc(m);
         int incl = cnt;
@@ -143,9 +172,14 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_write(const float *po
 
 using namespace amlp;
 
+// Workspace: the per-chunk counts, then one keep bit per Verlet pair.
+static size_t filter_ws_bytes(long long cap_verlet) {
+    return align_up(kFilterBlocks * sizeof(int)) + align_up((size_t)((cap_verlet + 31) / 32 + 1) * sizeof(unsigned));
+}
+
 extern "C" amlp_status amlp_filter_workspace_bytes(long long cap_verlet, size_t *bytes) {
     if (cap_verlet < 0 || !bytes) return AMLP_ERR_INVALID_ARG;
-    *bytes = align_up(kFilterBlocks * sizeof(int));
+    *bytes = filter_ws_bytes(cap_verlet);
     return AMLP_OK;
 }
 
@@ -153,13 +187,14 @@ extern "C" amlp_status amlp_pair_filter(const float *d_pos, float box, double cu
                                         const long long *d_nverlet, long long cap_verlet, int *d_pairs,
                                         long long *d_npairs, void *d_ws, size_t ws_bytes, void *stream) {
     if (!d_pos || !d_nverlet || !d_npairs || !(box > 0.f) || cap_verlet < 0) return AMLP_ERR_INVALID_ARG;
-    if (!d_ws || ws_bytes < kFilterBlocks * sizeof(int)) return AMLP_ERR_WORKSPACE;
+    if (!d_ws || ws_bytes < filter_ws_bytes(cap_verlet)) return AMLP_ERR_WORKSPACE;
     cudaStream_t s = as_stream(stream);
     int *counts = static_cast<int *>(d_ws);
+    unsigned *bits = reinterpret_cast<unsigned *>(static_cast<char *>(d_ws) + align_up(kFilterBlocks * sizeof(int)));
     double c = cutoff;
     BoxOf b{box, nullptr, nullptr, ((uintptr_t)d_vpairs & 15) == 0};
-    k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, c, d_vpairs, d_nverlet, cap_verlet, counts);
-    k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, c, d_vpairs, d_nverlet, cap_verlet, counts,
+    k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, c, d_vpairs, d_nverlet, cap_verlet, counts, bits);
+    k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_vpairs, d_nverlet, cap_verlet, counts, bits, b.vec,
                                                             d_pairs, d_npairs);
     return check_launch();
 }
@@ -169,12 +204,14 @@ extern "C" amlp_status amlp_multi_pair_filter(const float *d_pos, const int *d_r
                                               long long cap_verlet, int *d_pairs, long long *d_npairs, void *d_ws,
                                               size_t ws_bytes, void *stream) {
     if (!d_pos || !d_rep || !d_rp || !d_nverlet || !d_npairs || cap_verlet < 0) return AMLP_ERR_INVALID_ARG;
-    if (!d_ws || ws_bytes < kFilterBlocks * sizeof(int)) return AMLP_ERR_WORKSPACE;
+    if (!d_ws || ws_bytes < filter_ws_bytes(cap_verlet)) return AMLP_ERR_WORKSPACE;
     cudaStream_t s = as_stream(stream);
     int *counts = static_cast<int *>(d_ws);
+    unsigned *bits = reinterpret_cast<unsigned *>(static_cast<char *>(d_ws) + align_up(kFilterBlocks * sizeof(int)));
     BoxOf b{0.f, d_rep, d_rp, ((uintptr_t)d_vpairs & 15) == 0};
-    k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, cutoff, d_vpairs, d_nverlet, cap_verlet, counts);
-    k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, cutoff, d_vpairs, d_nverlet, cap_verlet, counts,
+    k_filter_count<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_pos, b, cutoff, d_vpairs, d_nverlet, cap_verlet, counts,
+                                                            bits);
+    k_filter_write<<<kFilterBlocks, kFilterThreads, 0, s>>>(d_vpairs, d_nverlet, cap_verlet, counts, bits, b.vec,
                                                             d_pairs, d_npairs);
     return check_launch();
 }

@@ -161,16 +161,36 @@ __device__ void reduce_ke(double kt, double kr, double *part, unsigned int *done
         last = prev == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    if (last) {
+        // the last block adds the partials: thread t takes blocks t, t + 256, ... in
+        // order, then a fixed tree over the threads (the same order in every run)
         __threadfence();
         double a = 0.0, b = 0.0;
-        for (unsigned int k = 0; k < gridDim.x; ++k) {
+        for (unsigned int k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
             a += ((volatile double *)part)[2 * k];
             b += ((volatile double *)part)[2 * k + 1];
         }
-        th->ke_t = a;
-        th->ke_r = b;
-        *done = 0;  // ready for the next launch
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        __syncthreads();  // sh is reused
+        if ((threadIdx.x & 31) == 0) {
+            sh[0][threadIdx.x >> 5] = a;
+            sh[1][threadIdx.x >> 5] = b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double ta = 0.0, tb = 0.0;
+            for (int w = 0; w < kIntThreads / 32; ++w) {
+                ta += sh[0][w];
+                tb += sh[1][w];
+            }
+            th->ke_t = ta;
+            th->ke_r = tb;
+            *done = 0;  // ready for the next launch
+        }
     }
 }
 
