@@ -595,8 +595,10 @@ struct amlp_pool {
                 if (!e)
                     e = cudaMemcpyAsync(nmass.as<char>() + off * 4, mass.as<char>() + x.first * 4, b1,
                                         cudaMemcpyDeviceToDevice, st);
+                const int row = th_row(x.id);  // packed systems always have a row
+                if (!e && row < 0) e = cudaErrorInvalidValue;
                 if (!e)
-                    e = cudaMemcpyAsync(nth.as<amlp_thermostat>() + r, th.as<amlp_thermostat>() + find_old(x.id),
+                    e = cudaMemcpyAsync(nth.as<amlp_thermostat>() + r, th.as<amlp_thermostat>() + row,
                                         sizeof(amlp_thermostat), cudaMemcpyDeviceToDevice, st);
             } else {
                 seeds[r] = seeded_thermostat(x.nve);
@@ -629,7 +631,7 @@ struct amlp_pool {
         nmass.release();
         nth.release();
         N = (int)n_new;
-        old_ids.clear();
+        packed_ids.clear();
         off = 0;
         slot.assign(sys.size(), 0);
         cap = 0;
@@ -645,7 +647,7 @@ struct amlp_pool {
             std::vector<float>().swap(x.vel);
             std::vector<float>().swap(x.angmom);
             std::vector<float>().swap(x.mass);
-            old_ids.push_back(x.id);
+            packed_ids.push_back(x.id);
             for (int k = 0; k < x.n; ++k) rep_h[(size_t)(off + k)] = (int)r;
             std::memset(&rp_h[r], 0, sizeof(amlp_replica));
             rp_h[r].kT = x.kT;
@@ -688,12 +690,12 @@ struct amlp_pool {
         if (s) return lib(s, "amlp_multi_nvt_init");
         return cuda(cudaStreamSynchronize(st), "pool repack");  // rep_h, rp_h
     }
-    // system ids in the order of the current packed arrays (thermostat rows)
-    std::vector<int> old_ids;
-    int find_old(int id) const {
-        for (size_t r = 0; r < old_ids.size(); ++r)
-            if (old_ids[r] == id) return (int)r;
-        return 0;
+    // ids of the systems in the current packed arrays, in row order (their thermostat rows)
+    std::vector<int> packed_ids;
+    int th_row(int id) const {
+        for (size_t r = 0; r < packed_ids.size(); ++r)
+            if (packed_ids[r] == id) return (int)r;
+        return -1;
     }
 
     // Every system's Verlet list into its slot, then one list with global indices.
@@ -885,8 +887,10 @@ extern "C" amlp_status amlp_pool_evict(amlp_pool *p, int id, float *h_pos, float
             if (c.dst && !s)
                 s = p->cuda(cudaMemcpy(c.dst, c.src->as<float>() + x.first * c.w, n * c.w * 4, cudaMemcpyDeviceToHost),
                             "evict copy");
+        const int row = p->th_row(id);
+        if (h_th && !s && row < 0) s = p->fail(AMLP_ERR_INVALID_ARG, "packed system without a thermostat row");
         if (h_th && !s)
-            s = p->cuda(cudaMemcpy(h_th, p->th.as<amlp_thermostat>() + p->find_old(id), sizeof(amlp_thermostat),
+            s = p->cuda(cudaMemcpy(h_th, p->th.as<amlp_thermostat>() + row, sizeof(amlp_thermostat),
                                    cudaMemcpyDeviceToHost),
                         "evict copy");
     } else {
@@ -946,8 +950,10 @@ extern "C" amlp_status amlp_pool_system_status(amlp_pool *p, int id, int *status
         if (!x.packed) {
             *h_th = seeded_thermostat(x.nve);
         } else {
-            amlp_status s = p->cuda(cudaMemcpy(h_th, p->th.as<amlp_thermostat>() + p->find_old(id),
-                                               sizeof(amlp_thermostat), cudaMemcpyDeviceToHost),
+            const int row = p->th_row(id);
+            if (row < 0) return p->fail(AMLP_ERR_INVALID_ARG, "packed system without a thermostat row");
+            amlp_status s = p->cuda(cudaMemcpy(h_th, p->th.as<amlp_thermostat>() + row, sizeof(amlp_thermostat),
+                                               cudaMemcpyDeviceToHost),
                                     "thermostat");
             if (s) return s;
         }
