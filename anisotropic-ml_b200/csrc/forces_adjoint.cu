@@ -1094,6 +1094,15 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
         // pass; layout [tile][half][n][kk][pair] so that a warp's accesses coalesce
         float A[Cfg::NA][KC];
         float *a_tile = a_rows ? a_rows + ((size_t)tile * 2 + h) * (Cfg::NA * KC) * kAP + p : nullptr;
+        if (BWD && a_rows && tid == 0 && tile + gridDim.x < ntiles) {
+            // the next tile's harmonic sums and dE/dg rows into L2 while this tile runs
+            const long long nt = tile + gridDim.x;
+            const char *an = reinterpret_cast<const char *>(a_rows + (size_t)nt * 2 * (Cfg::NA * KC) * kAP);
+            constexpr uint32_t kABytes = 2u * Cfg::NA * KC * kAP * 4u, kPiece = 16384u;
+            for (uint32_t o = 0; o < kABytes; o += kPiece) tc::bulk_prefetch_l2(an + o, min(kPiece, kABytes - o));
+            const uint32_t gb = (uint32_t)(min((long long)kAP, P - nt * kAP) * kGP * 4);
+            tc::bulk_prefetch_l2(dg_rows + nt * kAP * kGP, gb);
+        }
         if (BWD && a_rows) {
             // the backward's inputs first, so that their loads overlap the rotation pass
 #pragma unroll
