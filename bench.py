@@ -75,8 +75,8 @@ DRAM_BYTES_PER_PAIR = {"adjoint": 5.340928e6 / 436636, "fd": 5.318912e6 / 436636
 # HBM between its three launches: the sum over k_adj_desc forward, k_mlp_grad and k_adj_desc backward
 # captured at 32,768 cyl24 bodies (381,342 pairs). The per-pair rows do not depend on the shape or the
 # net, so the figure serves every wide workload.
-DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.084992e6 + 349.997824e6 + 79.480064e6 + 26.586624e6 + 409.252608e6
-                                       + 4.352e6) / 381342
+DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.141824e6 + 350.520064e6 + 79.480064e6 + 26.586624e6 + 409.184e6
+                                       + 5.303552e6) / 381342
 
 
 def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS):
