@@ -71,12 +71,6 @@ __device__ __forceinline__ void act_pair(int act, float z, float &f, float &df) 
     }
 }
 
-__device__ __forceinline__ float act_dfast(int act, float z) {
-    float f, df;
-    act_pair(act, z, f, df);
-    return df;
-}
-
 // Radial basis f_n of the adjoint kernels, with the cutoff function from the
 // hardware sine/cosine (__sincosf: a few 1e-7 absolute error for the
 // arguments here, far below the tensor-core net's 1e-5), used by both their
@@ -1333,8 +1327,9 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             const float *wl = par + net.bias_off[net.nh];
             float esum = 0.f;
             for (int c0 = 8 * h; c0 < Np; c0 += 8 * kMQ) {
-                float z[8], v[8];
-                tc::tmem_ld8(tmem + lane_base + (uint32_t)(L2 * kWideMax) + c0, z);
+                float z[8], v[8], dv[8];
+                const uint32_t zaddr = tmem + lane_base + (uint32_t)(L2 * kWideMax) + c0;
+                tc::tmem_ld8(zaddr, z);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     float zz = z[k] + bias[c0 + k], fz, dfz;
@@ -1344,11 +1339,15 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
                         v[k] = wl[c0 + k] * dfz;
                     } else {
                         v[k] = fz;
+                        dv[k] = dfz;
                     }
                 }
                 store_split8(tile(L2 + 1), Np, p, c0, v);
+                // act'(z) replaces z in TMEM: the backward needs only the derivative
+                if (!last) tc::tmem_st8(zaddr, dv);
             }
             if (last) eps[h * kAP + p] = esum;
+            else tc::tmem_wait_st();
             tc::fence_before();
             tc::fence_async_smem();
             __syncthreads();
@@ -1371,13 +1370,12 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             wait_mma();
             request(L2 > 0 ? L2 - 1 : 0);  // the next layer needed (layer 0 again for the next tile)
             if (L2 > 0) {
-                const float *bias = par + net.bias_off[L2 - 1];
                 for (int c0 = 8 * h; c0 < Kp; c0 += 8 * kMQ) {
-                    float dz[8], z[8], v[8];
+                    float dz[8], df[8], v[8];
                     tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
-                    tc::tmem_ld8(tmem + lane_base + (uint32_t)((L2 - 1) * kWideMax) + c0, z);
+                    tc::tmem_ld8(tmem + lane_base + (uint32_t)((L2 - 1) * kWideMax) + c0, df);  // act'(z)
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * act_dfast(net.act, z[k] + bias[c0 + k]);
+                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * df[k];
                     store_split8(tile(L2), Kp, p, c0, v);
                 }
             } else {
