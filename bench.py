@@ -214,6 +214,24 @@ def run_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line))
 
 
+# ----------------------------------------------------------------------------- ranks
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of every rank's x (one process per GPU, replicas): the slowest
+    replica's device time is the job's time. x itself without a process group."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world: int, n_bodies: int, steps: int, job_ms: float) -> float:
+    """Particle-steps/s of the whole job: every rank steps its own replica of
+    n_bodies, and job_ms is the time over ranks (max_over_ranks)."""
+    return world * n_bodies * steps / (job_ms / 1e3)
+
+
 # ----------------------------------------------------------------------------- GPU arm
 def _measure(system, method: str, steps: int, warmup: int, dist, dev):
     """Device time of `steps` full steps (L2 flushed between steps, outside the
@@ -272,11 +290,7 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         force_ms.append(f0.elapsed_time(f1))
-    total = sum(step_ms)
-    if dist:
-        t = torch.tensor([total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = max_over_ranks(sum(step_ms), dist, dev)
     assert _lib.device_error() == 0, "a bounded device wait gave up"
     finite = bool(torch.isfinite(system.pos).all() and torch.isfinite(system.vel).all())
     return {"total_ms": total, "force_ms": statistics.mean(force_ms), "force_share": sum(force_ms) / sum(step_ms),
@@ -305,11 +319,7 @@ def _e2e(system, method, steps, dist, dev):
             host[k].copy_(getattr(system, k), non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     return ms, nbytes
 
 
@@ -417,7 +427,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             tensor = {"algorithmic_tflops": tc_alg, "executed_tflops": 3.0 * tc_alg,
                       "peak": peaks["bf16_tflops"], "frac_executed": 3.0 * tc_alg / peaks["bf16_tflops"],
                       "note": "net on the tensor cores as three bf16 products per multiply-add (bf16x3)"}
-        return {"value": world * N_BODIES * args.steps / (r["total_ms"] / 1e3), "ms_per_step": r["total_ms"] / args.steps,
+        return {"value": job_throughput(world, N_BODIES, args.steps, r["total_ms"]), "ms_per_step": r["total_ms"] / args.steps,
                 "roofline": {"bound": "fp32",
                              "kernel": "k_forces_" + m if max(WIDTHS) <= 64 else "k_adj_desc x2 + k_mlp_grad", "achieved": achieved, "peak": fp32_peak,
                              "unit": "TFLOP/s", "frac": achieved / fp32_peak,
@@ -432,7 +442,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                              "work": ("achieved counts the FP32 SIMT work only (descriptor forward and backward); "
                                       "the net's tensor-core work is reported under 'tensor'") if tc_pair else
                                      "achieved counts all the work (descriptors and net, FP32 SIMT)"},
-                "e2e": {"value": world * N_BODIES * r["e2e_steps"] / (r["e2e_ms"] / 1e3), "unit": "particle-steps/s",
+                "e2e": {"value": job_throughput(world, N_BODIES, r["e2e_steps"], r["e2e_ms"]), "unit": "particle-steps/s",
                         "h2d_bytes_per_step": r["e2e_bytes"], "d2h_bytes_per_step": r["e2e_bytes"],
                         "steps": r["e2e_steps"]},
                 "gpu_launches": r["launches"]}
