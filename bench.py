@@ -469,7 +469,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         line["tuned_over_plain"] = hs["value"] / ps["value"]
         line["gpu_launches"] += ps["gpu_launches"]
     if rank == 0 and world == 1 and not args.no_serving and IS_BENCHMARK:
-        line["serving"] = run_serving(dev)
+        line["serving"] = run_serving(dev, args.serving_requests, args.serving_steps, args.serving_rate)
     if rank == 0 and not args.no_cpu_baseline and world == 1 and SHAPE == "cube26":
         from amlp.configs import make_state as _ms
         t_cpu, sample, _ = cpu_step_sample(_ms(N_BODIES, "cube26", PHI, kT=KT, seed=SEED))
@@ -570,6 +570,11 @@ def main():
     ap.add_argument("--method", choices=["both", "fd", "adjoint"], default="both")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=48,
+                    help="requests of the served stream (the full stream of the serving configuration is 512)")
+    ap.add_argument("--serving-steps", type=int, default=300,
+                    help="NVT steps per request (2000 in the full serving configuration)")
+    ap.add_argument("--serving-rate", type=float, default=8.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--bodies", type=int, default=N_BODIES,
                     help="system size (the benchmark workload is 131072; smaller sizes are for profiling)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cube26",
