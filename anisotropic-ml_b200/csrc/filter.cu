@@ -67,9 +67,9 @@ __device__ __forceinline__ void chunk_range(long long nv, long long *s, long lon
     *e = min(nv, *s + chunk);
 }
 
-__global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *pos, BoxOf L, double cutoff, const int *vp,
-                                                                 const long long *d_nv, long long cap, int *counts,
-                                                                 unsigned *bits) {
+__global__ void __launch_bounds__(kFilterThreads) k_filter_count(const float *pos, BoxOf L, double cutoff,
+                                                                 const int *vp, const long long *d_nv, long long cap,
+                                                                 int *counts, unsigned *bits) {
     long long nv = min(*d_nv, cap), s, e;
     chunk_range(nv, &s, &e);
     const int lane = threadIdx.x & 31;

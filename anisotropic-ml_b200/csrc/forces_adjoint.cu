@@ -148,7 +148,9 @@ __device__ __forceinline__ void sh_recurrences(float x, float y, float z, float 
         for (int l = m; l <= LMAX; ++l) {
             if (l == m) Q[l][m] = (float)dfact_odd(m);
             else if (l == m + 1) Q[l][m] = (float)(2 * m + 1) * z * Q[l - 1][m];
-            else Q[l][m] = ((float)(2 * l - 1) * z * Q[l - 1][m] - (float)(l + m - 1) * Q[l - 2][m]) * (1.0f / (float)(l - m));
+            else
+                Q[l][m] = ((float)(2 * l - 1) * z * Q[l - 1][m] - (float)(l + m - 1) * Q[l - 2][m]) *
+                          (1.0f / (float)(l - m));
         }
     }
 }
@@ -175,8 +177,8 @@ __host__ __device__ constexpr float sh_weight(int k) {
 // The unnormalised harmonics Q_l^m {C_m, S_m} (m > 0) and Q_l^0 of this half
 // (indices k0 .. k0 + KC - 1, zero past K) from the recurrences.
 template <class Cfg, int KC, int k0>
-__device__ __forceinline__ void sh_half_u(const float *C, const float *Sn, const float (&Q)[Cfg::LMAX + 2][Cfg::LMAX + 2],
-                                          float *Y) {
+__device__ __forceinline__ void sh_half_u(const float *C, const float *Sn,
+                                          const float (&Q)[Cfg::LMAX + 2][Cfg::LMAX + 2], float *Y) {
 #pragma unroll
     for (int kk = 0; kk < KC; ++kk) {
         const int k = k0 + kk;
@@ -778,7 +780,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             __syncthreads();
         }
         if (!MULTI && h == 0 && p < valid)
-            pe_acc += (double)en_min + (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
+            pe_acc += (double)en_min +
+                      (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
         // ---- 4. recompute the rotated points (their area held the MLP tiles)
         if (!keep_r) {
             rotate_tile(S, npts, rs);
@@ -1187,12 +1190,13 @@ __global__ void k_split_weights(AdjNet net, const float *w, char *dst) {
 // Net forward and backward over rows of g on the tensor cores (bf16x3 splits,
 // fp32 TMEM accumulators). 16 warps: warp w reads TMEM lanes 32 (w % 4) ..
 // 32 (w % 4) + 31 (its pairs) and, of every layer's columns, the 8-column
-// chunks c with c % 4 == w / 4, so that four warps share each epilogue's rows. One layer's weights at a time sit in shared memory,
-// brought in by a bulk copy from the pre-split copy (k_split_weights) that
-// thread 0 starts as soon as the previous layer's MMAs are done, so it overlaps
-// the epilogue; the layer order fwd 0..nh-1, bwd nh-1..0 reuses the last
-// forward layer and, across tiles, layer 0. Outputs per row: y = net(g) and
-// dE/dg (kGP floats).
+// chunks c with c % 4 == w / 4, so that four warps share each epilogue's rows.
+// One layer's weights at a time sit in shared memory, brought in by a bulk copy
+// from the pre-split copy (k_split_weights) that thread 0 starts as soon as the
+// previous layer's MMAs are done, so it overlaps the epilogue; the layer order
+// fwd 0..nh-1, bwd nh-1..0 reuses the last forward layer and, across tiles,
+// layer 0. The forward epilogues replace each hidden layer's z in TMEM with
+// act'(z) for the backward. Outputs per row: y = net(g) and dE/dg (kGP floats).
 constexpr int kMQ = 4;                  // column groups of the k_mlp_grad epilogues
 constexpr int kMThreads = kMQ * kAP;    // 512
 __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
@@ -1210,7 +1214,8 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
     float *eps = par + net.par_total;
     // the next tile's descriptor rows, brought in by a bulk copy during this tile's net
     float *gbuf = reinterpret_cast<float *>(
-        smem_raw + align_up(2 * tile_bytes + (size_t)2 * kWideMax * kWideMax * 2 + (size_t)(net.par_total + kMQ * kAP) * 4,
+        smem_raw + align_up(2 * tile_bytes + (size_t)2 * kWideMax * kWideMax * 2 +
+                                (size_t)(net.par_total + kMQ * kAP) * 4,
                             128));
     auto tile = [&](int k) { return ops + (k & 1) * tile_bytes; };
     for (int L2 = 0; L2 < net.nh; ++L2) {
@@ -1534,8 +1539,8 @@ static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
 
 extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes) {
     if (cap < 0 || !bytes) return AMLP_ERR_INVALID_ARG;
-    *bytes = align_up((size_t)cap * kGRow * 4) + align_up((size_t)cap * kGP * 4) + align_up((size_t)cap * 4) + align_up(kWeightSplitBytes) +
-             align_up(adj_a_bytes(cap)) + 256;
+    *bytes = align_up((size_t)cap * kGRow * 4) + align_up((size_t)cap * kGP * 4) + align_up((size_t)cap * 4) +
+             align_up(kWeightSplitBytes) + align_up(adj_a_bytes(cap)) + 256;
     return AMLP_OK;
 }
 

@@ -683,7 +683,8 @@ struct amlp_pool {
             (s = cuda(cudaMemcpyAsync(rp.p, rp_h.data(), rp_h.size() * sizeof(amlp_replica), cudaMemcpyHostToDevice,
                                       st),
                       "pool")) ||
-            (s = cuda(cudaMemsetAsync(accel.p, 0, n3, st), "pool")) || (s = cuda(cudaMemsetAsync(dp.p, 0, n4, st), "pool")))
+            (s = cuda(cudaMemsetAsync(accel.p, 0, n3, st), "pool")) ||
+            (s = cuda(cudaMemsetAsync(dp.p, 0, n4, st), "pool")))
             return s;
         s = amlp_multi_nvt_init(vel.as<float>(), quat.as<float>(), angmom.as<float>(), mass.as<float>(), rep.as<int>(),
                                 N, (int)sys.size(), &prm, th.as<amlp_thermostat>(), st);
@@ -794,8 +795,8 @@ extern "C" amlp_status amlp_pool_create(const amlp_pool_config *cfg, amlp_pool *
         !(cfg->dt > 0.f) || !(cfg->cutoff > 0.0) || !(cfg->nep_cutoff > 0.f) || !(cfg->en_max > cfg->en_min))
         return AMLP_ERR_INVALID_ARG;
     const amlp_mlp &m = *cfg->mlp;
-    if (m.n_layers < 1 || m.n_layers > AMLP_MAX_LAYERS || m.dims[0] != descriptor_length(cfg->nrad, cfg->nang, cfg->lmax) ||
-        m.dims[m.n_layers] != 1)
+    if (m.n_layers < 1 || m.n_layers > AMLP_MAX_LAYERS ||
+        m.dims[0] != descriptor_length(cfg->nrad, cfg->nang, cfg->lmax) || m.dims[m.n_layers] != 1)
         return AMLP_ERR_INVALID_ARG;
     amlp_pool *p = new amlp_pool();
     const size_t wbytes = (size_t)packed_weight_count(m) * sizeof(float);
