@@ -1,7 +1,7 @@
 """Drop-in ``Sim`` (reference: ``nep_simulator/Sim.py``).
 
 Same builder methods, call order and run loop as the reference
-(``sim_input.py:338-349``, ``Sim.py:207-285``); the state lives on the GPU in
+(``sim_input.py:50-61``, ``Sim.py:207-285``); the state lives on the GPU in
 an ``amlp.engine.System`` and every step runs through ``libamlp``.
 
 Run loop: the Verlet list is rebuilt every 100 steps and a GSD frame is

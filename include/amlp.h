@@ -137,7 +137,10 @@ amlp_status amlp_nlist_build(const float *d_pos, int n, float box, double r,
  * inside the library (13 MiB per GPU, held until exit); n is limited to
  * 262,144 bodies (AMLP_ERR_TOO_LARGE beyond). The first call on a device looks
  * up the array's device address and should come before any stream capture.
- * Calls share the array, so calls that overlap on the GPU race. */
+ * The address is kept for the life of the process: it assumes the device's
+ * one primary context throughout, so after cudaDeviceReset this entry point
+ * must not be called again. Calls share the array, so calls that overlap on
+ * the GPU race. */
 amlp_status amlp_nlist_build_noalloc(const float *d_pos, int n, float box, double r,
                                      int *d_pairs, long long cap, long long *d_count, void *stream);
 

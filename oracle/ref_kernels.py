@@ -26,7 +26,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF_ROOT = os.environ.get("AMLP_REFERENCE_ROOT", "/root/reference")
+# The reference checkout: AMLP_REFERENCE_ROOT, else a directory named "reference" beside this
+# repository. Without it nothing is built (the fixtures under tests/golden stand in for it).
+REF_ROOT = os.environ.get("AMLP_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 KERNEL_DIR = os.path.join(REF_ROOT, "nep_simulator", "cudakernels")
 SKIP = {"radial_grad", "g_all"}
 

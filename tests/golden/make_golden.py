@@ -2,11 +2,11 @@
 ``NVT``/``Sim``/``DescriptorGenerator``/``ForceEvaluator`` classes on the CPU.
 
 Runs only where the reference checkout is present (``AMLP_REFERENCE_ROOT``,
-default ``/root/reference``). The reference imports CuPy and gsd, which are not
+else a ``reference`` directory beside this repository). The reference imports CuPy and gsd, which are not
 installed; ``oracle.ref_cupy_shim`` supplies numpy-backed stand-ins and runs
 the reference's CUDA kernel strings compiled for the host
 (``oracle/ref_kernels.py``). The reference's sequence of builder calls is the
-one of ``nep_simulator/sim_input.py:338-349``.
+one of ``nep_simulator/sim_input.py:50-61``.
 
 Cases (one ``case_<name>.npz`` each, weights in ``model_<model>.npz``):
 

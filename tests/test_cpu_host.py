@@ -107,7 +107,8 @@ def test_gsd_rejects_corrupt(tmp_path):
 
 
 def test_reference_init_file_reader():
-    ref = "/root/reference/nep_simulator/init/th_init_N200.gsd"
+    from oracle.ref_kernels import REF_ROOT
+    ref = os.path.join(REF_ROOT, "nep_simulator", "init", "th_init_N200.gsd")
     if not os.path.exists(ref):
         pytest.skip("reference checkout not present")
     from amlp.gsd import read_last_frame

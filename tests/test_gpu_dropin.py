@@ -2,7 +2,7 @@
 ``ForceEvaluator``, ``sim_input``) on the reference's own case: 200 ``th_v1``
 bodies from ``init/th_init_N200.gsd``, ``model_th_C104`` (47 -> 150 x 3 -> 1
 ReLU), hypers 10 8 4 4.5, kT 0.5, dt 0.005, driven through the reference's
-builder calls (``sim_input.py:338-349``) from a GSD file and a ``.pth`` state
+builder calls (``sim_input.py:50-61``) from a GSD file and a ``.pth`` state
 dict written here from the fixtures.
 
 * ``generate_nep_descriptors`` returns the reference's filtered pairs (as a

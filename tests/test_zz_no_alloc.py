@@ -56,11 +56,24 @@ def test_noalloc_matches_workspace_entry_point_twice():
     # two different systems one after the other: the second call must not see the first one's scratch
     cases = [make_state(20000, "cube26", 0.45, seed=21), make_state(3000, "cyl24", 0.30, seed=22)]
     for s in cases:
-        pos_t = torch.tensor(s.pos, device=DEV)
-        ref = _workspace_list(pos_t, s.N, s.L, 4.5)
-        got = _noalloc_list(pos_t, s.N, s.L, 4.5)
-        assert len(ref) > 0
-        assert np.array_equal(got, ref)
+        _check_same_list(s.pos, s.L)
+
+
+def test_noalloc_box_beyond_its_cell_limit():
+    # a box of 230 at radius 4.5 would take 51 cells per edge; the entry point caps them at 48
+    # (larger cells, the same list)
+    L = np.float32(230.0)
+    assert L / 4.5 > 48
+    pos = (np.random.default_rng(23).random((40000, 3)) * L - L / 2).astype(np.float32)
+    _check_same_list(pos, float(L))
+
+
+def _check_same_list(pos, L):
+    pos_t = torch.tensor(pos, device=DEV)
+    ref = _workspace_list(pos_t, len(pos), L, 4.5)
+    got = _noalloc_list(pos_t, len(pos), L, 4.5)
+    assert len(ref) > 0
+    assert np.array_equal(got, ref)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
