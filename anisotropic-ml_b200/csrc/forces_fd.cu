@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
                                                                const int *pairs, const long long *d_np, long long cap,
                                                                const float *pts, int npts, float inv_rc, FdConst c,
                                                                FusedNet net, const float *w, float *F, float *T,
-                                                               double *pe) {
+                                                               double *pe, float *e_out) {
     extern __shared__ __align__(16) float smem[];
     const TileGeom g = tile_geom(npts);
     // layout: activations (2 x kFusedMaxWidth x kRows) | weights | e | fd | pts | R | t | ij
@@ -372,6 +372,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
             const int col = act_col(threadIdx.x);
             for (int k = 0; k < K; ++k) acc = fmaf(wl[k * net.npad[Ll]], X[k * kRows + col], acc);
             e[threadIdx.x] = acc;
+            if (e_out && (threadIdx.x & 31) < valid)  // row (variant v, pair p) of e_all: e_out[v P + p0 + p]
+                e_out[(long long)(threadIdx.x >> 5) * P + p0 + (threadIdx.x & 31)] = acc;
         }
         __syncthreads();
         for (int idx = threadIdx.x; idx < 9 * kPT; idx += blockDim.x) {
@@ -502,9 +504,9 @@ extern "C" amlp_status amlp_fd_scatter(const float *d_e, long long P, const int 
     return check_launch();
 }
 
-extern "C" amlp_status amlp_forces_fd(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
-                                      const long long *d_npairs, long long cap, const amlp_nep *nep,
-                                      const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe, void *stream) {
+static amlp_status launch_fd(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                             const long long *d_npairs, long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
+                             float *d_F, float *d_T, double *d_pe, float *d_e, void *stream) {
     amlp_status st = check_nep(nep);
     if (st) return st;
     int D = nep_D(nep);
@@ -539,9 +541,23 @@ extern "C" amlp_status amlp_forces_fd(const float *d_pos, const float *d_quat, f
     if (hyper_kind(nep) == 1) {
         if ((st = set_smem(k_forces_fd<CfgA>, smem))) return st;
         k_forces_fd<CfgA><<<grid, kTileThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts,
-                                                           nep->npts, inv_rc, c, net, mlp->d_w, d_F, d_T, d_pe);
+                                                           nep->npts, inv_rc, c, net, mlp->d_w, d_F, d_T, d_pe, d_e);
     } else {
         return AMLP_ERR_UNSUPPORTED;
     }
     return check_launch();
+}
+
+extern "C" amlp_status amlp_forces_fd(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                      const long long *d_npairs, long long cap, const amlp_nep *nep,
+                                      const amlp_mlp *mlp, float *d_F, float *d_T, double *d_pe, void *stream) {
+    return launch_fd(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, nullptr, stream);
+}
+
+extern "C" amlp_status amlp_forces_fd_energies(const float *d_pos, const float *d_quat, float box,
+                                               const int *d_pairs, const long long *d_npairs, long long cap,
+                                               const amlp_nep *nep, const amlp_mlp *mlp, float *d_F, float *d_T,
+                                               double *d_pe, float *d_e, void *stream) {
+    if (!d_e && cap > 0) return AMLP_ERR_INVALID_ARG;
+    return launch_fd(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, d_e, stream);
 }

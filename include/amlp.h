@@ -208,6 +208,16 @@ amlp_status amlp_forces_fd(const float *d_pos, const float *d_quat, float box,
                            const amlp_nep *nep, const amlp_mlp *mlp,
                            float *d_F, float *d_T, double *d_pe, void *stream);
 
+/* amlp_forces_fd that also writes the net output of every finite-difference
+ * variant, d_e[v * P + p] for variant v = 0..9 of filtered pair p
+ * (P = min(*d_npairs, cap); d_e holds 10 cap floats): the e_all of
+ * ForceEvaluator.evaluate_gradients (ForceEvaluator.py:80-96), for checking
+ * the fused kernel's energies row by row. */
+amlp_status amlp_forces_fd_energies(const float *d_pos, const float *d_quat, float box,
+                                    const int *d_pairs, const long long *d_npairs, long long cap,
+                                    const amlp_nep *nep, const amlp_mlp *mlp,
+                                    float *d_F, float *d_T, double *d_pe, float *d_e, void *stream);
+
 /* Adjoint path: one descriptor evaluation per pair and the exact derivative of
  * the pair energy with respect to the translation of body i and the rotations
  * of bodies i and j; the same scaling, clip and scatter as the plain path. */

@@ -18,7 +18,14 @@ Cases (one ``case_<name>.npz`` each, weights in ``model_<model>.npz``):
   (``runner.sh:4``); step-0 intermediates and state after 1 step;
 * ``cube_C104`` -- 200 ``cube_v2`` bodies on a seeded lattice (L = 26; the
   cube init file of ``runner.sh:2`` is not in the reference checkout) with
-  ``model_nep_C104``; step-0 intermediates and state after 3 steps.
+  ``model_nep_C104``; step-0 intermediates and state after 3 steps;
+* ``cube_R64`` -- 400 ``cube_v2`` bodies on a seeded lattice (L = 30) with a
+  seeded 47 -> 64 -> 64 -> 1 ReLU net (``model_cube_R64``, torch's default
+  initialisation under ``torch.manual_seed(64)``), the width of the fused
+  finite-difference kernel. ``Sim.setEvaluator`` fixes the net at 150 x 3
+  (``Sim.py:60``); this case drives the same ``ForceEvaluator`` with
+  ``setNN_dimensions(64, 1)`` (``ForceEvaluator.py:38-40``) and keeps all 10 P
+  per-variant energies of step 0 (``e0``) besides the usual intermediates.
 
 Usage: ``python tests/golden/make_golden.py``.
 """
@@ -61,15 +68,42 @@ def _snapshot(sim):
                                                                 sim.m_exp_thermo_fac)], np.float32))
 
 
-def run_case(root, name, init_gsd, hypers, model, shape, kT, dt, steps_list, long_run=None):
+def save_seeded_relu_net(path, name, D, width, depth, seed):
+    """TheEnergyNet(width, depth, D) of the reference (ForceEvaluator.py:6-26) with
+    torch's default initialisation under ``torch.manual_seed(seed)``, saved as a
+    state dict (.pth) for ``read_model`` and as ``model_<name>.npz``."""
+    import torch
+    from ForceEvaluator import TheEnergyNet  # reference module, loaded by the shim's source finder
+    torch.manual_seed(seed)
+    net = TheEnergyNet(width, depth, D)
+    torch.save(net.state_dict(), path)
+    save_model(path, name)
+
+
+def run_case(root, name, init_gsd, hypers, model, shape, kT, dt, steps_list, long_run=None, model_path=None,
+             nn_dims=None):
+    from ForceEvaluator import ForceEvaluator
     from NVT import NVT  # reference module, loaded by the shim's source finder
 
+    model_path = model_path or os.path.join(root, "models", model + ".pth")
+    if nn_dims is not None:
+        # Sim.setEvaluator calls setNN_dimensions(150, 3) (Sim.py:60); the net of this case is nn_dims
+        orig_dims = ForceEvaluator.setNN_dimensions
+        ForceEvaluator.setNN_dimensions = lambda self, w, d: orig_dims(self, *nn_dims)
+    try:
+        _run_case(name, init_gsd, hypers, model, model_path, shape, kT, dt, steps_list, long_run, NVT)
+    finally:
+        if nn_dims is not None:
+            ForceEvaluator.setNN_dimensions = orig_dims
+
+
+def _run_case(name, init_gsd, hypers, model, model_path, shape, kT, dt, steps_list, long_run, NVT):
     def build(dump, fn):
         sim = NVT()
         sim.setDevice(0)
         sim.initializeSystem(init_gsd)
         sim.setNepDescriptors(list(hypers))
-        sim.setEvaluator(os.path.join(root, "models", model + ".pth"))
+        sim.setEvaluator(model_path)
         sim.setShape(shape)
         sim.setNeighborList()
         sim.setGsdDump(dump, fn)
@@ -151,13 +185,12 @@ def _continue(sim, nsteps):
         sim.step()
 
 
-def cube_init(path):
+def cube_init(path, n=200, L=26.0, m=6, shuffle=False):
     from amlp.gsd import Frame, GsdFile
     rng = np.random.default_rng(7)
-    n, L = 200, 26.0
-    m = 6
     g = np.arange(m)
-    sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)[:n]
+    sites = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    sites = sites[rng.permutation(len(sites))[:n]] if shuffle else sites[:n]
     pos = ((sites + 0.5) * (L / m) - L / 2 + rng.uniform(-0.3, 0.3, (n, 3))).astype(np.float32)
     q = rng.standard_normal((n, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
@@ -171,11 +204,27 @@ def cube_init(path):
         gf.append(f)
 
 
+def make_r64(root):
+    tmp = tempfile.mkdtemp()
+    mpath = os.path.join(tmp, "model_cube_R64.pth")
+    save_seeded_relu_net(mpath, "cube_R64", 47, 64, 1, seed=64)
+    cpath = os.path.join(tmp, "cube_init_400.gsd")
+    cube_init(cpath, n=400, L=30.0, m=8, shuffle=True)
+    run_case(root, "cube_R64", cpath, (10, 8, 4, 4.5), "model_cube_R64", "cube_v2", 0.5, 0.005, [1],
+             model_path=mpath, nn_dims=(64, 1))
+
+
 def main():
     from oracle import ref_cupy_shim
     root = ref_cupy_shim.install()
     cwd = os.getcwd()
     os.chdir(tempfile.mkdtemp())
+    if "--r64" in sys.argv:  # only the 64-wide case
+        try:
+            make_r64(root)
+        finally:
+            os.chdir(cwd)
+        return
     try:
         for m in ("model_th_C104", "model_th_C100", "model_nep_C104"):
             save_model(os.path.join(root, "models", m + ".pth"), m[len("model_"):])
@@ -187,6 +236,8 @@ def main():
         cpath = os.path.join(tempfile.mkdtemp(), "cube_init.gsd")
         cube_init(cpath)
         run_case(root, "cube_C104", cpath, (10, 8, 4, 4.5), "model_nep_C104", "cube_v2", 0.5, 0.005, [1, 3])
+        if "--r64" in sys.argv or "--all" in sys.argv or len(sys.argv) == 1:
+            make_r64(root)
         # the init frames themselves (the GPU box has no reference checkout)
         for nm in ("th_init_N200", "th_init_N200_seed20"):
             f = read_last_frame(os.path.join(root, "init", nm + ".gsd"))

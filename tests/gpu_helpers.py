@@ -115,5 +115,10 @@ def fused_forces(pos, quat, L, pairs, shape, hypers, layers, act, method="amlp_f
     if method == "amlp_forces_adjoint_wide":
         ws = torch.empty(size_query("amlp_adjoint_workspace_bytes", max(P, 1)), dtype=torch.uint8, device=DEV)
         args += [ws.data_ptr(), ws.numel()]
+    e = None
+    if method == "amlp_forces_fd_energies":
+        e = torch.full((10 * max(P, 1),), float("nan"), dtype=torch.float32, device=DEV)
+        args += [e.data_ptr()]
     call(method, *args, stream())
-    return F.cpu().numpy(), T.cpu().numpy(), float(pe.item())
+    out = (F.cpu().numpy(), T.cpu().numpy(), float(pe.item()))
+    return out + (e[:10 * P].cpu().numpy(),) if e is not None else out

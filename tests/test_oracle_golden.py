@@ -8,7 +8,7 @@ from conftest import case_model, case_shape, load_case
 from oracle import nep, nlist
 from oracle.sim import OracleSim
 
-CASES = ["th_C104", "th_C100", "cube_C104"]
+CASES = ["th_C104", "th_C100", "cube_C104", "cube_R64"]
 
 
 def _sim(c, steps_dt=np.float32):
