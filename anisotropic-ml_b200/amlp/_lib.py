@@ -115,6 +115,8 @@ SIGNATURES = {
     "amlp_mlp_loss_grad": [_P, _P, _LL, ctypes.POINTER(Mlp), _P, _P, _P],
     "amlp_fd_scatter": [_P, _LL, _P, ctypes.POINTER(Nep), _P, _P, _P, _P],
     "amlp_forces_fd": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
+    "amlp_forces_fd_energies": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P,
+                                _P, _P],
     "amlp_forces_adjoint": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P, _P],
     "amlp_adjoint_workspace_bytes": [_LL, _PSZ],
     "amlp_forces_adjoint_wide": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P,
