@@ -128,6 +128,7 @@ SIGNATURES = {
                              _P, _P, _SZ, _P],
     "amlp_mlp_backward": [_P, _P, _LL, ctypes.POINTER(Mlp), _P, _P],
     "amlp_device_error": [ctypes.POINTER(ctypes.c_uint), _I],
+    "amlp_test_first_wait_limit": [_I],
     "amlp_nvt_workspace_bytes": [_I, _PSZ],
     "amlp_nvt_init": [_P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _I, _P, _P, _SZ, _P],
     "amlp_nvt_step_two": [_P, _P, _P, _P, _P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _P, _P],
@@ -207,6 +208,19 @@ def device_error(clear: bool = True) -> int:
     v = ctypes.c_uint(0)
     call("amlp_device_error", ctypes.byref(v), int(clear))
     return int(v.value)
+
+
+class AmlpDeviceError(RuntimeError):
+    """A bounded device-side wait gave up: the results of the launches since the
+    last check are not to be trusted (the kernels stopped early, no fault)."""
+
+
+def check_device() -> None:
+    """Raise ``AmlpDeviceError`` if a bounded device-side wait gave up since the
+    last check (the flags are cleared). Synchronises the device."""
+    flags = device_error(clear=True)
+    if flags:
+        raise AmlpDeviceError(f"a bounded device-side wait gave up (flags {flags:#x})")
 
 
 def exported_symbols() -> list[str]:

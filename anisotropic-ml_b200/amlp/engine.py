@@ -220,6 +220,7 @@ class System:
             if not check:
                 return -1
             n = int(self.nv.item())
+            _lib.check_device()  # the count read has synchronised: the check costs one small copy
             if n <= self.cap:
                 if self.nlist_policy == "displacement":
                     self.nl_ref.copy_(self.pos)
@@ -334,7 +335,12 @@ class System:
         self.timestep += seg
 
     def run(self, nsteps: int, method: str = "fd", graph: bool = True) -> None:
-        """``nsteps`` steps; between Verlet rebuilds the steps replay as one CUDA graph."""
+        """``nsteps`` steps; between Verlet rebuilds the steps replay as one CUDA graph.
+        Raises ``AmlpDeviceError`` (after the steps) if a bounded device wait gave up."""
+        self._run(nsteps, method, graph)
+        _lib.check_device()
+
+    def _run(self, nsteps: int, method: str, graph: bool) -> None:
         end = self.timestep + nsteps
         if self.nlist_policy == "displacement":
             while self.timestep < end:

@@ -25,6 +25,10 @@
 namespace amlp {
 
 __device__ unsigned int g_amlp_device_error = 0;
+// Test hook (amlp_test_first_wait_limit): polls allowed to the first MMA-completion
+// wait of every CTA of k_forces_adjoint; -1 keeps the normal limit. 0 makes that
+// wait give up at once, which exercises the abort path without any fault.
+__device__ int g_amlp_first_wait_limit = -1;
 
 namespace {
 
@@ -522,13 +526,13 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     extern __shared__ __align__(128) char smem_raw[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_slot;
-    __shared__ int abort_flag;
     __shared__ double pe_s[kAThreads / 32];
     __shared__ float psum_s[3];
 
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
     const int Kg = net.kin[0];
+    const int first_limit = g_amlp_first_wait_limit;
 
     // ---- shared memory carve-up (offsets are multiples of 128 bytes)
     AdjShared S;
@@ -607,10 +611,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         if (tid == 0) S.par[net.bias_off[net.nh] + kWpad] = Wl[K];  // last bias
     }
     if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);
-    if (tid == 0) {
-        tc::mbar_init(&mbar, 1);
-        abort_flag = 0;
-    }
+    if (tid == 0) tc::mbar_init(&mbar, 1);
     tc::fence_async_smem();
     tc::fence_before();
     __syncthreads();
@@ -618,6 +619,12 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     const uint32_t tmem = tmem_slot;
     const uint32_t bar = tc::smem_u32(&mbar);
     uint32_t phase = 0;
+    // A bounded wait that gives up sets gave_up in its thread; the barrier that
+    // ends each net stage ORs it over the block into `aborted`, so that every
+    // thread agrees on it: no further MMA is issued or waited for, the tile loop
+    // ends, and the MMA still in flight is drained before TMEM is released.
+    bool gave_up = false, aborted = false;
+    int waits = 0, commits = 0;
     // TMEM column regions: Z_k (hidden layer k) at 64k, backward product at 192, dE/dg at 192 too,
     // act'(Z_k) of the hidden layers before the last at 256 + 64k
     auto zcol = [&](int k) { return (uint32_t)(k * kWpad); };
@@ -625,14 +632,12 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
     auto dfcol = [&](int k) { return (uint32_t)(4 * kWpad + k * kWpad); };
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
 
-    auto wait_mma = [&]() -> bool {
-        if (!tc::mbar_wait(bar, phase)) {
-            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
-            abort_flag = 1;
-        }
+    auto wait_mma = [&]() {
+        if (aborted) return;  // nothing was issued
+        const int limit = (waits++ == 0 && first_limit >= 0) ? first_limit : tc::kWaitLimit;
+        if (!tc::mbar_wait(bar, phase, limit)) gave_up = true;
         phase ^= 1u;
         tc::fence_after();
-        return true;
     };
 
     const long long P = min(*d_np, cap);
@@ -688,12 +693,13 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         // forward layers
         for (int L2 = 0; L2 < net.nh; ++L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
-            if (tid == 0 && !abort_flag) {
+            if (tid == 0 && !aborted) {
                 tc::fence_after();
                 const char *wb = S.wts + net.wsm_off[L2];
                 mma3<true>(tmem + zcol(L2), op_tile(S.ops, L2), Kp, wb, (size_t)Np * Kp * 2, Np, false, 256, 128,
                      (uint32_t)Kp * 16);
                 tc::commit(bar);
+                ++commits;
             }
             wait_mma();
             // epilogue: a = act(z + b) into the next operand tile; the last hidden
@@ -734,18 +740,19 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             else tc::tmem_wait_st();
             tc::fence_before();
             tc::fence_async_smem();
-            __syncthreads();
+            aborted = __syncthreads_or(gave_up) != 0;
         }
         // backward layers: delta_{k-1} = (delta_k W_k) * act'(z_{k-1}); dE/dg = delta_1 W_1
         for (int L2 = net.nh - 1; L2 >= 0; --L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
-            if (tid == 0 && !abort_flag) {
+            if (tid == 0 && !aborted) {
                 tc::fence_after();
                 const char *wb = S.wts + net.wsm_off[L2];
                 // B = W_k read as MN-major (the transpose): N' = Kp, K' = Np
                 mma3<true>(tmem + bcol, op_tile(S.ops, L2 + 1), Np, wb, (size_t)Np * Kp * 2, Kp, true,
                      2 * Kp * 16, (uint32_t)Kp * 16, 128);
                 tc::commit(bar);
+                ++commits;
             }
             wait_mma();
             if (L2 > 0) {
@@ -777,8 +784,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 }
             }
             tc::fence_before();
-            __syncthreads();
+            aborted = __syncthreads_or(gave_up) != 0;
         }
+        if (aborted) break;  // the net's outputs are not to be trusted: no forces from this tile
         if (!MULTI && h == 0 && p < valid)
             pe_acc += (double)en_min +
                       (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
@@ -878,7 +886,6 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
             }
         }
         __syncthreads();
-        if (abort_flag) break;
     }
     // ---- pair-energy sum, TMEM release
     if (!MULTI && pe) {
@@ -894,7 +901,12 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
         for (int k = 0; k < kAThreads / 32; ++k) s += pe_s[k];
         if (s != 0.0) atomicAdd(pe, s);
     }
-    if (abort_flag && tid == 0) tc::mbar_wait(bar, phase);  // let an MMA still in flight finish
+    if (aborted && tid == 0) {
+        atomicOr(&g_amlp_device_error, kErrMbarTimeout);
+        // the last MMA issued may still be in flight (thread 0 flipped `phase` after waiting for it):
+        // let it finish, with the normal limit, before TMEM is released
+        if (commits > 0) tc::mbar_wait(bar, phase ^ 1u, tc::kWaitLimit);
+    }
     __syncthreads();
     if (warp == 0) {
         tc::fence_after();
@@ -1651,6 +1663,12 @@ extern "C" amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_
                                                         nullptr, 1, nullptr, nullptr, nullptr, nullptr, nullptr,
                                                         nullptr);
     return check_launch();
+}
+
+extern "C" amlp_status amlp_test_first_wait_limit(int polls) {
+    if (polls < -1) return AMLP_ERR_INVALID_ARG;
+    AMLP_CHECK_CUDA(cudaMemcpyToSymbol(g_amlp_first_wait_limit, &polls, sizeof(int)));
+    return AMLP_OK;
 }
 
 extern "C" amlp_status amlp_device_error(unsigned int *flags, int clear) {

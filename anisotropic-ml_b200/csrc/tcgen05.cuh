@@ -130,8 +130,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t phase) {
     return ok != 0;
 }
 
-// Bounded wait for the completion of `phase`; false after `limit` polls.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int limit = 1 << 22) {
+constexpr int kWaitLimit = 1 << 22;  // polls of a bounded mbarrier wait
+
+// Bounded wait for the completion of `phase`; false after `limit` polls (at once for 0).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int limit = kWaitLimit) {
     for (int i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, phase)) return true;
     return false;

@@ -264,6 +264,14 @@ amlp_status amlp_mlp_backward(const float *d_g, const float *d_dy, long long row
  * wait for tensor-core completion gave up; the kernel then stops early). */
 amlp_status amlp_device_error(unsigned int *flags, int clear);
 
+/* Test hook (no reference counterpart): the number of polls allowed to the
+ * first tensor-core completion wait of every CTA of amlp_forces_adjoint's
+ * kernel, so that a test can make that wait give up without a fault: with 0 it
+ * gives up at once, the kernel raises bit 1 of amlp_device_error, issues no
+ * further MMA, drains the one in flight (normal limit) and frees its tensor
+ * memory. -1 restores the normal limit. It applies to later launches. */
+amlp_status amlp_test_first_wait_limit(int polls);
+
 /* --------------------------------------------------------------- NVT integrator
  * d_th: one amlp_thermostat in device memory.
  * init: kinetic energies before the first step. With initial_ke_quirk = 1 the
