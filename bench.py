@@ -1,7 +1,9 @@
 """Benchmark: particle-steps/s of the NVT step of 131,072 rigid cubes on B200.
 
 Workload (one "step" = one full time step: pair filter, force pass, both NVT
-halves; the Verlet list is rebuilt every 100 steps inside the timed region):
+halves; the Verlet list is rebuilt at the first timed step and every 100 steps
+after it, so every timed window holds ceil(K / 100) rebuilds -- for K < 100
+more than the amortised 1/100 share):
 131,072 cube26 bodies at packing fraction 0.45, jittered lattice, random unit
 quaternions, seed 1, NEP hypers (10, 8, 4), FFNN 47 -> 64 -> 64 -> 1 tanh with
 seeded Xavier weights, dt 0.005, kT 1.0 (synthetic; no dataset involved).
@@ -11,9 +13,12 @@ Arms:
       "value" is the tuned method (exact adjoint forces, net on the tensor
       cores); with "both" the plain FP32 finite-difference drop-in is measured
       in the same run under "plain"
-  python bench.py --impl reference ...   CPU restatement of the reference's
-      step (the oracle, bit-identical to the reference's own classes) on the
-      host cores, timed on a bounded sample of the same workload.
+  python bench.py --impl reference ...   the reference's step on the host
+      cores through the oracle (bit-identical to the reference's own classes),
+      on a process pool; each timed step covers a random sample of the bodies
+      (their pair filter and force pass) and both NVT halves of all bodies, and
+      "value" counts the sampled bodies only. The arm imports nothing of the
+      product package (oracle.workload generates the same state and net).
 
 With --gpus N > 1 (launched by torch.distributed.run) every rank runs an
 independent replica on its own GPU (weak scaling, no data-path collective);
@@ -134,58 +139,92 @@ def measured_peaks() -> dict:
 
 
 # ----------------------------------------------------------------------------- reference arm / CPU baseline
-class CpuReferenceStep:
-    """One step of the reference's algorithm on the host cores, through the
-    oracle (bit-identical to the reference's own classes run on the CPU): FP32
-    descriptors of the 10 finite-difference clouds, torch-CPU net, differences,
-    scatter, both NVT halves, and 1/100 of a cKDTree Verlet rebuild. The force
-    pass runs on a random sample of the filtered pairs and is scaled to all."""
+def common_config(world: int) -> dict:
+    """The workload's description, the same in both arms."""
+    return {"workload": WORKLOAD, "bodies": N_BODIES, "shape": SHAPE, "phi": PHI, "seed": SEED,
+            "net": f"47x{'x'.join(str(w) for w in WIDTHS)}x1 {ACT} ({NET})", "dt": DT, "kT": KT,
+            "nlist_every": 100, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "GPU arm: flushed between timed steps (256 MB write); CPU arm: not applicable"}
 
-    def __init__(self, state, pairs_sample: int = 256):
+
+def _oracle_layers():
+    """The workload's net from the oracle side (numpy only)."""
+    import numpy as np
+    from oracle import workload
+    if NET == "trained":
+        z = np.load(os.path.join(REPO, "tests", "golden", f"model_{SHAPE}_soft.npz"))
+        return [(z[f"W{k}"], z[f"b{k}"]) for k in range(len(z.files) // 2)]
+    layers = workload.xavier_layers(47, WIDTHS, SEED)
+    if NET == "xavier_out0.05":
+        W, b = layers[-1]
+        layers[-1] = (W * np.float32(0.05), b)
+    return layers
+
+
+class CpuRun:
+    """The reference's step on the host cores (oracle.workload.CpuStep): timed
+    steps on random samples of `bodies_per_step` bodies, sized at set-up so that
+    a step takes about `target_s` seconds."""
+
+    def __init__(self, n, shape, phi, seed, target_s=2.0, workers=None):
         import numpy as np
-        import torch
-        from amlp.engine import EnergyNet
-        from oracle import nep, nlist
-        from oracle.shapes import SHAPES
-        torch.set_num_threads(os.cpu_count() or 1)
-        self.np, self.nep = np, nep
-        self.state = state
-        self.shape = SHAPES["cube26"]
-        self.net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device="cpu")
-        t0 = time.perf_counter()
-        vp = nlist.reference_pairs(state.pos, state.L, self.shape["cutoff"] + 2.0)
-        self.t_nlist = time.perf_counter() - t0
-        _, self.pairs, _ = nep.min_image_filter(state.pos, vp, state.L, self.shape["cutoff"])
-        self.P = len(self.pairs)
-        self.sample = min(pairs_sample, self.P)
+        from oracle import workload
+        self.np = np
+        state = workload.make_state(n, shape, phi, kT=KT, seed=seed)
+        self.n = n
+        self.step = workload.CpuStep(state, shape, (10, 8, 4), _oracle_layers(), ACT, KT, DT, workers=workers)
         self.rng = np.random.default_rng(0)
-        self.st = nep.NVTState(state.pos, state.vel, state.orient, state.angmom, state.mass, state.moi, state.L,
-                               KT, DT)
-        self.threads = torch.get_num_threads()
+        self.bodies = n
+        if target_s is not None and n > 256:
+            self.step.step(self._sample(256))  # the workers' first call loads their libraries
+            t = self.step.step(self._sample(256))
+            self.bodies = int(min(n, max(64, 256 * target_s / max(t, 1e-3))))
 
-    def step_seconds(self) -> float:
-        np, nep = self.np, self.nep
-        sel = np.sort(self.rng.choice(self.P, size=self.sample, replace=False))
-        t0 = time.perf_counter()
-        o = nep.pair_forces(self.st.pos, self.st.orient, self.pairs[sel], self.state.L, self.shape, (10, 8, 4),
-                            self.net.layers, ACT)
-        t_f = (time.perf_counter() - t0) * self.P / self.sample
-        t0 = time.perf_counter()
-        self.st.step_two(o["forces"], o["torques"])
-        self.st.step_one()
-        t_i = time.perf_counter() - t0
-        return t_f + t_i + self.t_nlist / 100.0
+    def _sample(self, k):
+        return None if k >= self.n else self.np.sort(self.rng.choice(self.n, size=k, replace=False))
 
-    def describe(self) -> str:
-        return (f"per step: force pass on {self.sample} of {self.P} filtered pairs scaled by "
-                f"{self.P / self.sample:.0f}x, both NVT halves on all {self.state.N} bodies, 1/100 of a cKDTree "
-                f"rebuild; oracle FP32 path (numpy + torch CPU, {self.threads} threads)")
+    def timed(self, steps):
+        times, pairs = [], 0
+        for _ in range(steps):
+            times.append(self.step.step(self._sample(self.bodies)))
+            pairs += self.step.pairs_last
+        return times, pairs
+
+    def describe(self, pairs_per_step):
+        full = self.bodies >= self.n
+        what = "all bodies" if full else f"a random sample of {self.bodies} of the {self.n} bodies"
+        return (f"each step: {what} (pair filter of the Verlet pairs they own, force pass of the "
+                f"{pairs_per_step:.0f} filtered pairs on average: 10 FP32 finite-difference clouds, direct "
+                f"descriptors, torch-CPU net, differences, clip, scatter) and both NVT halves of all {self.n} "
+                f"bodies; the oracle's FP32 path (bit-identical to the reference's classes) on "
+                f"{self.step.workers} worker processes; value counts the {'' if full else 'sampled '}bodies; "
+                f"the Verlet rebuild (one cKDTree call, {self.step.t_nlist:.2f} s for all bodies, every 100 steps) "
+                f"is outside the timed steps")
+
+    def close(self):
+        self.step.close()
 
 
-def cpu_step_sample(state, steps: int = 3):
-    ref = CpuReferenceStep(state)
-    t = statistics.mean(ref.step_seconds() for _ in range(steps))
-    return t, ref.describe(), ref.P
+def cpu_step_sample(steps: int = 5):
+    """cpu_baseline leg of the GPU arm: a bounded run of the reference's step on the host cores."""
+    run = CpuRun(N_BODIES, SHAPE, PHI, SEED)
+    try:
+        run.timed(1)
+        times, pairs = run.timed(steps)
+        t = statistics.mean(times)
+        return {"value": run.bodies / t, "unit": "particle-steps/s", "cores": run.step.workers, "kind": "port",
+                "sample": run.describe(pairs / steps), "bodies_per_step": run.bodies,
+                "s_per_step": t, "extrapolated_s_per_full_step": t * N_BODIES / run.bodies}
+    finally:
+        run.close()
+
+
+def _product_library_mapped() -> bool:
+    try:
+        with open("/proc/self/maps") as fh:
+            return "libamlp.so" in fh.read()
+    except OSError:
+        return False
 
 
 def run_reference(args, rank: int, world: int) -> None:
@@ -194,23 +233,37 @@ def run_reference(args, rank: int, world: int) -> None:
     if SHAPE != "cube26":
         print(json.dumps({"impl": "reference", "unavailable": "the CPU arm is timed on the cube26 benchmark workload"}))
         return
-    from amlp.configs import make_state
-    state = make_state(N_BODIES, "cube26", PHI, kT=KT, seed=SEED)
-    ref = CpuReferenceStep(state)
-    for _ in range(args.warmup):
-        ref.step_seconds()
-    times = [ref.step_seconds() for _ in range(args.steps)]
+    run = CpuRun(N_BODIES, SHAPE, PHI, SEED)
+    try:
+        run.timed(args.warmup)
+        times, pairs = run.timed(args.steps)
+    finally:
+        run.close()
     per_step = statistics.mean(times)
-    value = N_BODIES / per_step
-    cores = os.cpu_count() or 1
+    value = run.bodies / per_step
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "bodies": N_BODIES, "filtered_pairs": ref.P, "parallelism": "replicas",
-                       "method": "fd (the reference's finite differences)"},
-            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-                             "sample": ref.describe()},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, Xavier weights)",
+            "config": common_config(world),
+            "method": "fd (the reference's finite differences)",
+            "sample": {"bodies_per_step": run.bodies, "bodies_total": N_BODIES,
+                       "filtered_pairs_per_step": pairs / args.steps, "measured_s_per_step": per_step,
+                       "timed_s": sum(times), "extrapolated_s_per_full_step": per_step * N_BODIES / run.bodies},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": run.step.workers, "kind": "port",
+                             "sample": run.describe(pairs / args.steps)},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    assert not _product_library_mapped(), "the reference arm must not load libamlp.so"
+    if WORKLOAD.startswith("nvt-step-131072-cube26"):
+        # the small configuration (1,000 cubes, packing fraction 0.30, seed 0) run in full: every body, every pair
+        small = CpuRun(1000, "cube26", 0.30, 0, target_s=None)
+        try:
+            small.timed(2)
+            st, sp = small.timed(10)
+        finally:
+            small.close()
+        line["full_run_1000_cubes"] = {"value": 1000 * len(st) / sum(st), "unit": "particle-steps/s", "steps": len(st),
+                                       "ms_per_step": statistics.mean(st) * 1e3, "filtered_pairs_per_step": sp / len(st),
+                                       "sample": "none: all 1,000 bodies and all their pairs every step"}
     print(json.dumps(line))
 
 
@@ -247,10 +300,19 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
     if wide:
         entry = "amlp_forces_adjoint_wide"
 
+    # Verlet rebuilds: every nlist_every steps counted from the first timed step, so that
+    # the timed window starts with one (warm-up steps follow the engine's own schedule)
+    origin = [None]
+    rebuilds = [0]
+
     def one_step(ev_force=None):
-        if system.timestep % system.nlist_every == 0 and system.timestep > 0:
+        t = system.timestep
+        due = (t - origin[0]) % system.nlist_every == 0 if origin[0] is not None else \
+            (t % system.nlist_every == 0 and t > 0)
+        if due:
             system.build_nlist(check=False)
             launches[0] += LAUNCHES["amlp_nlist_build"]
+            rebuilds[0] += 1
         system.F.zero_()
         system.T.zero_()
         system.th[_lib.Thermostat.pe.offset:_lib.Thermostat.pe.offset + 8].zero_()
@@ -279,6 +341,8 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
         dist.barrier()
     torch.cuda.synchronize()
     launches[0] = 0
+    rebuilds[0] = 0
+    origin[0] = system.timestep
     step_ms, force_ms = [], []
     for _ in range(steps):
         flush.zero_()
@@ -294,7 +358,8 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
     assert _lib.device_error() == 0, "a bounded device wait gave up"
     finite = bool(torch.isfinite(system.pos).all() and torch.isfinite(system.vel).all())
     return {"total_ms": total, "force_ms": statistics.mean(force_ms), "force_share": sum(force_ms) / sum(step_ms),
-            "P": P, "NV": NV, "launches": launches[0], "P_end": int(system.nf.item()), "finite": finite}
+            "P": P, "NV": NV, "launches": launches[0], "P_end": int(system.nf.item()), "finite": finite,
+            "rebuilds": rebuilds[0]}
 
 
 def _e2e(system, method, steps, dist, dev):
@@ -303,6 +368,9 @@ def _e2e(system, method, steps, dist, dev):
     import numpy as np
     import torch
     stream = torch.cuda.current_stream()
+    adv = (-system.timestep) % system.nlist_every
+    if adv:  # untimed: the timed steps start with a Verlet rebuild, as in the device-timed window
+        system.run(adv, method)
     host = {k: torch.from_numpy(np.ascontiguousarray(getattr(system, k).cpu().numpy())).pin_memory()
             for k in ("pos", "quat", "vel", "angmom")}
     nbytes = sum(t.numel() * t.element_size() for t in host.values())
@@ -453,14 +521,13 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             "warmup": args.warmup, "ms_per_step": hs["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice, " + ("Xavier weights)" if NET != "trained" else
                                                                  "net fitted to a soft repulsion, committed fixture)"),
-            "config": {"workload": WORKLOAD, "method": head, "bodies": N_BODIES,
-                       "verlet_pairs": results[head]["NV"], "filtered_pairs": results[head]["P"],
-                       "filtered_pairs_last_step": results[head]["P_end"], "state_finite": results[head]["finite"],
-                       "nlist_every": 100,
-                       "l2": "flushed between timed steps (256 MB write)",
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "precision": ("FP32 descriptors; net on tensor cores as bf16x3 splits with FP32 accumulation"
-                                     if head == "adjoint" else "FP32 throughout")},
+            "config": common_config(world),
+            "run": {"method": head, "verlet_pairs": results[head]["NV"], "filtered_pairs": results[head]["P"],
+                    "filtered_pairs_last_step": results[head]["P_end"], "state_finite": results[head]["finite"],
+                    "nlist_rebuilds_in_window": results[head]["rebuilds"],
+                    "nlist_schedule": "rebuild at the first timed step and every 100 steps after it",
+                    "precision": ("FP32 descriptors; net on tensor cores as bf16x3 splits with FP32 accumulation"
+                                  if head == "adjoint" else "FP32 throughout")},
             "roofline": hs["roofline"], "e2e": hs["e2e"], "gpu_launches": hs["gpu_launches"], "clocks": clk}
     if len(methods) > 1:
         ps = summary("fd")
@@ -471,10 +538,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     if rank == 0 and world == 1 and not args.no_serving and IS_BENCHMARK:
         line["serving"] = run_serving(dev, args.serving_requests, args.serving_steps, args.serving_rate)
     if rank == 0 and not args.no_cpu_baseline and world == 1 and SHAPE == "cube26":
-        from amlp.configs import make_state as _ms
-        t_cpu, sample, _ = cpu_step_sample(_ms(N_BODIES, "cube26", PHI, kT=KT, seed=SEED))
-        line["cpu_baseline"] = {"value": N_BODIES / t_cpu, "unit": "particle-steps/s", "cores": os.cpu_count() or 1,
-                                "kind": "port", "sample": sample}
+        line["cpu_baseline"] = cpu_step_sample()
     if rank == 0:
         print(json.dumps(line))
     if dist:

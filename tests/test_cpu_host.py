@@ -191,3 +191,19 @@ def test_central_differences_oracle_matches_exact_derivative():
     a = adjoint.exact_pair_forces(s.pos, s.orient, sub, s.L, shape, (10, 8, 4), net.layers, "silu", clip=False)
     for got, want in ((F, a["forces"][bodies]), (T, a["torques"][bodies])):
         assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max())
+
+
+def test_oracle_workload_is_the_products():
+    """bench.py's reference arm builds its state and net with oracle.workload (it
+    imports nothing of the product): the arrays must be the product's, bit for bit."""
+    from amlp.configs import make_state
+    from amlp.engine import EnergyNet
+    from oracle import workload
+    for args in ((1000, "cube26", 0.30, 1.0, 0), (4096, "tetra16", 0.40, 0.7, 2), (3000, "cyl24", 0.35, 1.3, 3)):
+        a, b = workload.make_state(*args), make_state(*args[:3], kT=args[3], seed=args[4])
+        assert a.L == b.L
+        for k in ("pos", "orient", "vel", "angmom", "mass", "moi"):
+            assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    for (Wa, ba), (Wb, bb) in zip(workload.xavier_layers(47, (64, 64), 1),
+                                  EnergyNet.xavier(47, (64, 64), "tanh", seed=1, device="cpu").layers):
+        assert np.array_equal(Wa, Wb) and np.array_equal(ba, bb)
