@@ -80,6 +80,17 @@ __device__ __forceinline__ float act_df(int act, float z) {
     return s * (1.0f + z * (1.0f - s));
 }
 
+// True when the keys of the valid lanes never decrease from one lane to the
+// next, so that equal keys form contiguous runs and a segmented warp sum over
+// runs is exact. `ok` marks the valid lanes, a prefix of the warp. Pair lists
+// from amlp_pair_filter are sorted by (i, j); other callers may pass any order,
+// and the scatters then fall back to one atomic per lane.
+__device__ __forceinline__ bool warp_keys_sorted(int key, bool ok) {
+    const int lane = threadIdx.x & 31;
+    const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+    return __all_sync(0xffffffffu, !ok || lane == 0 || prev <= key) != 0;
+}
+
 __device__ __forceinline__ float clip100(float v) { return v > 100.0f ? 100.0f : (v < -100.0f ? -100.0f : v); }
 
 }  // namespace amlp

@@ -852,7 +852,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                     atomicAdd(T + 3 * j + k, S.fd[9 * q + 6 + k]);
                 }
             }
-            int key = ok ? i : -1 - q;
+            const bool runs = warp_keys_sorted(i, ok);  // every lane takes part (warp vote)
+            int key = ok && runs ? i : -1 - q;  // unsorted pairs: no merging
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 int ko = __shfl_up_sync(0xffffffffu, key, o);
@@ -874,7 +875,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 double e = ok ? (double)en_min + (double)en_range *
                                     (double)(S.eps[q] + S.eps[kAP + q] + S.par[net.bias_off[net.nh] + kWpad])
                               : 0.0;
-                int rk = ok ? rep[i] : -1 - lane;
+                const int sys = ok ? rep[i] : 0;
+                const bool sys_runs = warp_keys_sorted(sys, ok);
+                int rk = ok && sys_runs ? sys : -1 - lane;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
                     int ro = __shfl_up_sync(0xffffffffu, rk, o);
@@ -882,7 +885,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                     if (lane >= o && ro == rk) e += y;
                 }
                 int rn = __shfl_down_sync(0xffffffffu, rk, 1);
-                if (ok && (lane == 31 || rn != rk)) atomicAdd(pe + rk, e);
+                if (ok && (lane == 31 || rn != rk)) atomicAdd(pe + sys, e);
             }
         }
         __syncthreads();
@@ -1000,7 +1003,8 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
                 atomicAdd(T + 3 * j + k, S.fd[9 * q + 6 + k]);
             }
         }
-        int key = ok ? i : -1 - q;
+        const bool runs = warp_keys_sorted(i, ok);  // every lane takes part (warp vote)
+        int key = ok && runs ? i : -1 - q;  // unsorted pairs: no merging
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             int ko = __shfl_up_sync(0xffffffffu, key, o);
@@ -1020,7 +1024,9 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
         }
         if (MULTI && pe) {
             double e = ok ? (double)en_min + (double)en_range * (double)y_rows[p0 + q] : 0.0;
-            int rk = ok ? rep[i] : -1 - lane;
+            const int sys = ok ? rep[i] : 0;
+            const bool sys_runs = warp_keys_sorted(sys, ok);
+            int rk = ok && sys_runs ? sys : -1 - lane;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 int ro = __shfl_up_sync(0xffffffffu, rk, o);
@@ -1028,7 +1034,7 @@ __device__ __forceinline__ void adj_finish_tile(const AdjShared &S, int rs, int 
                 if (lane >= o && ro == rk) e += yv;
             }
             int rn = __shfl_down_sync(0xffffffffu, rk, 1);
-            if (ok && (lane == 31 || rn != rk)) atomicAdd(pe + rk, e);
+            if (ok && (lane == 31 || rn != rk)) atomicAdd(pe + sys, e);
         }
     }
     __syncthreads();

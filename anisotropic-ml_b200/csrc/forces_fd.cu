@@ -284,8 +284,9 @@ __device__ __forceinline__ bool segmented_sum(int key, float *v, int nv) {
 
 // Scatter of one tile's per-pair forces/torques, fd[p*9 + (F xyz, T_i xyz, T_j xyz)]:
 // F[i] += F, F[j] -= F, T[i] += T_i, T[j] += T_j (ForceEvaluator.py:135-142).
-// Warp 0, lane = pair. The i side is summed over runs of equal i first
-// (pairs are sorted by i), so one atomic per run and component.
+// Warp 0, lane = pair. When the tile's pairs are sorted by i (lists from
+// amlp_pair_filter), the i side is summed over runs of equal i first, so one
+// atomic per run and component; otherwise one atomic per pair.
 __device__ __forceinline__ void scatter_tile(const float *fd, const int *ij, int valid, float *F, float *T) {
     if (threadIdx.x >= 32) return;
     const int p = threadIdx.x;
@@ -304,7 +305,9 @@ __device__ __forceinline__ void scatter_tile(const float *fd, const int *ij, int
             atomicAdd(T + 3 * j + k, fd[9 * p + 6 + k]);
         }
     }
-    bool last = segmented_sum(ok ? i : -1 - p, v, 6);
+    const bool runs = warp_keys_sorted(i, ok);  // warp-uniform
+    bool last = true;
+    if (runs) last = segmented_sum(ok ? i : -1 - p, v, 6);
     if (ok && last) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {

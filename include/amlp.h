@@ -15,7 +15,9 @@
  *   - Layouts follow the reference: positions (N,3) f32, orientations and
  *     angular momenta (N,4) f32 as (w,x,y,z) quaternions (HOOMD convention),
  *     forces/torques (N,3) f32, pair lists (P,2) with i < j. Pair indices are
- *     int32 here (the reference keeps int64 from scipy).
+ *     int32 here (the reference keeps int64 from scipy). Filtered pair lists
+ *     may come in any order; the lists amlp_pair_filter writes are sorted by
+ *     (i, j), which lets the force kernels merge a warp's atomics per body.
  *   - The stateless calls take every buffer from the caller; calls on one
  *     stream are ordered, calls on different streams that share output
  *     buffers race. The handles at the end of this file (amlp_sim,

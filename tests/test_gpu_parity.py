@@ -440,3 +440,22 @@ def test_adjoint_wide_nets_vs_fp64_exact(shape_name, phi, widths, act):
         err = np.linalg.norm(got - want) / np.linalg.norm(want)
         assert err <= 1e-3, err
     assert abs(pe - ref["E"].sum()) <= 1e-4 * max(1.0, np.abs(ref["E"]).sum())
+
+
+@pytest.mark.parametrize("method", ["amlp_forces_adjoint", "amlp_forces_adjoint_wide", "amlp_forces_fd"])
+def test_force_scatter_takes_pairs_in_any_order(method):
+    """The fused kernels sum the i side of a warp's pairs over runs of equal i
+    when the list is sorted (as amlp_pair_filter writes it); any other order,
+    e.g. the reference's own cKDTree order, must give the same forces."""
+    from amlp.engine import EnergyNet
+    s = make_state(600, "cube26", 0.45, seed=13)
+    shape = SHAPES["cube26"]
+    vp, _ = gh.nlist(s.pos, s.L, 4.5)
+    pairs = gh.pair_filter(s.pos, s.L, 2.5, vp)
+    shuffled = pairs[np.random.default_rng(1).permutation(len(pairs))]
+    net = EnergyNet.xavier(47, (64, 64), "tanh", seed=2, device="cpu")
+    a = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, (10, 8, 4), net.layers, "tanh", method=method)
+    b = gh.fused_forces(s.pos, s.orient, s.L, shuffled, shape, (10, 8, 4), net.layers, "tanh", method=method)
+    for x, y in zip(a[:2], b[:2]):
+        np.testing.assert_allclose(x, y, rtol=0, atol=1e-5 * max(1.0, np.abs(x).max()))
+    assert abs(a[2] - b[2]) <= 1e-9 * max(1.0, abs(a[2]))
