@@ -204,7 +204,7 @@ class System:
         self.f_ws = torch.empty(max(1, size_query("amlp_filter_workspace_bytes", self.cap)), dtype=torch.uint8,
                                 device=self.device)
         self.adj_ws = None
-        if self.net.max_hidden > 64:  # nets wider than the fused adjoint kernel take the three-kernel path
+        if self.net.max_hidden > 64 or self.hypers.D > 48:  # beyond the fused adjoint kernel: the wide path
             self.adj_ws = torch.empty(size_query("amlp_adjoint_workspace_bytes", self.cap), dtype=torch.uint8,
                                       device=self.device)
         self._graphs.clear()

@@ -20,6 +20,7 @@
 //      to [-100, 100] and scattered like the reference (ForceEvaluator.py:119-142).
 // Nets: 1 to 3 hidden layers of width <= 64, D <= 64.
 #include "descriptor.cuh"
+#include "descriptor_direct.cuh"
 #include "tcgen05.cuh"
 
 namespace amlp {
@@ -34,7 +35,8 @@ namespace {
 
 constexpr int kAP = 128;          // pairs per tile (MMA M)
 constexpr int kAThreads = 256;
-constexpr int kMaxHidden = 3;
+constexpr int kMaxHidden = 3;      // hidden layers of the fused kernel
+constexpr int kMaxHiddenWide = 4;  // hidden layers of the wide path: layer_first + 3 (TheEnergyNet(150, 3, D))
 constexpr int kWpad = 64;          // hidden widths padded to 64 in TMEM regions
 constexpr uint32_t kErrMbarTimeout = 1u;
 // Shared-memory row strides of per-pair arrays, odd so that the 32 pairs of a
@@ -43,17 +45,22 @@ constexpr int kGS = 49;           // descriptor partials / dE/dg rows (48 used)
 constexpr int kPartStride = 13;   // gradient partial sums (12 used)
 
 struct AdjNet {
-    int nh;                         // hidden layers
+    int nh;                              // hidden layers
     int act;
-    int kin[kMaxHidden + 1];        // padded input width of hidden layer k (multiple of 16)
-    int nout[kMaxHidden + 1];       // padded output width of hidden layer k (multiple of 16)
-    int dims[kMaxHidden + 2];       // true dims: D, h1, .., h_nh, 1
-    long long woff[kMaxHidden + 1];  // offset of W_k in the packed global weights (k = 0..nh)
-    int wsm_off[kMaxHidden];        // byte offset of W_k (hi) in the weight area; lo follows (the wide
-                                    // path: in the pre-split global copy of the weights)
-    int wsm_total;                  // bytes of the weight area
-    int bias_off[kMaxHidden + 1];   // float offsets of b_k in the fp32 parameter area; last = w_last
+    int kin[kMaxHiddenWide + 1];         // padded input width of hidden layer k (multiple of 16)
+    int nout[kMaxHiddenWide + 1];        // padded output width of hidden layer k (multiple of 16)
+    int dims[kMaxHiddenWide + 2];        // true dims: D, h1, .., h_nh, 1
+    long long woff[kMaxHiddenWide + 1];  // offset of W_k in the packed global weights (k = 0..nh)
+    int wsm_off[kMaxHiddenWide];         // byte offset of W_k (hi) in the weight area; lo follows (the wide
+                                         // path: in the pre-split global copy of the weights)
+    int wsm_total;                       // bytes of the weight area
+    int bias_off[kMaxHiddenWide + 1];    // float offsets of b_k in the fp32 parameter area; last = w_last
     int par_total;
+    // k_mlp_grad only (set by wide_net): row strides of the g and dE/dg rows, widest
+    // hidden layer, TMEM columns of the product region, act'(z) as bits (ReLU),
+    // shared-memory carve-up and whether the next tile's g rows are prefetched
+    int g_ld, gp, wmax, zbw, relu_bits;
+    int wbuf_off, par_off, eps_off, gbuf_off, prefetch_g, smem;
 };
 
 // Activation and its derivative from one exponential, for the tensor-core
@@ -928,13 +935,16 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
 //   k_adj_desc<..., true>   recomputes the per-pair sums, descriptor backward,
 //                           forces, torques, scatter.
 // ============================================================================
-constexpr int kWideMax = 128;
+constexpr int kWideMax = 160;  // hidden widths up to 150 (the reference's nets), padded to 160
 constexpr int kGP = 48;  // padded descriptor width in the workspace rows
 // Row stride of the descriptor rows in the workspace and in k_mlp_grad's shared
 // copy: 52 floats, 13 units of 16 bytes, odd, so that the 16-byte reads of 32
 // consecutive rows by a warp fall in distinct bank groups.
 constexpr int kGRow = 52;
-constexpr size_t kWeightSplitBytes = (size_t)kMaxHidden * kWideMax * kWideMax * 4;  // bf16 hi/lo of every layer
+// The same for the hypers (10, 10, 10), D = 121: padded to 128, rows of 132 floats (33 x 16 bytes)
+constexpr int kGP2 = 128;
+constexpr int kGRow2 = 132;
+constexpr size_t kWeightSplitBytes = (size_t)kMaxHiddenWide * kWideMax * kWideMax * 4;  // bf16 hi/lo, every layer
 constexpr size_t kAdjAFloats = 2 * 9 * 12;  // harmonic sums per pair kept between the passes (two halves of 9 x 12)
 
 __host__ __device__ inline size_t adj_a_bytes(long long cap) {
@@ -1206,36 +1216,36 @@ __global__ void k_split_weights(AdjNet net, const float *w, char *dst) {
 }
 
 // Net forward and backward over rows of g on the tensor cores (bf16x3 splits,
-// fp32 TMEM accumulators). 16 warps: warp w reads TMEM lanes 32 (w % 4) ..
-// 32 (w % 4) + 31 (its pairs) and, of every layer's columns, the 8-column
-// chunks c with c % 4 == w / 4, so that four warps share each epilogue's rows.
-// One layer's weights at a time sit in shared memory, brought in by a bulk copy
-// from the pre-split copy (k_split_weights) that thread 0 starts as soon as the
-// previous layer's MMAs are done, so it overlaps the epilogue; the layer order
-// fwd 0..nh-1, bwd nh-1..0 reuses the last forward layer and, across tiles,
-// layer 0. The forward epilogues replace each hidden layer's z in TMEM with
-// act'(z) for the backward. Outputs per row: y = net(g) and dE/dg (kGP floats).
+// fp32 TMEM accumulators), hidden layers up to 160 wide and up to four of them
+// (the reference's TheEnergyNet(150, 3, D): layer_first and three hidden
+// layers). 16 warps: warp w reads TMEM lanes 32 (w % 4) .. 32 (w % 4) + 31 (its
+// rows) and, of every layer's columns, the 8-column chunks c with
+// c % 4 == w / 4, so that four warps share each epilogue's rows.
+// Shared memory holds one operand tile: each epilogue overwrites the tile its
+// MMA read, complete by then. One layer's weights at a time sit beside it,
+// brought in by a bulk copy from the pre-split copy (k_split_weights) that
+// thread 0 starts as soon as the previous layer's MMAs are done, so that it
+// overlaps the epilogue; the layer order fwd 0..nh-1, bwd nh-1..0 reuses the
+// last forward layer and, across tiles, layer 0. One TMEM region (net.zbw
+// columns) takes every product in turn. The forward epilogues keep act'(z) of
+// each hidden layer but the last for the backward: for ReLU (derivative 0 or
+// 1) as bits in registers, otherwise in TMEM after the product region.
+// Outputs per row: y = net(g) and dE/dg (net.gp floats).
 constexpr int kMQ = 4;                  // column groups of the k_mlp_grad epilogues
 constexpr int kMThreads = kMQ * kAP;    // 512
+static_assert(kWideMax <= 8 * kMQ * 8, "a thread's 8-column chunks of a layer fit one 64-bit mask");
 __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
                                                           AdjNet net, const float *w, const char *wsplit,
                                                           float *y_rows, float *dg_rows) {
     extern __shared__ __align__(128) char smem_raw[];
     __shared__ uint64_t mbar, wbar, gbar;
     __shared__ uint32_t tmem_slot;
-    __shared__ int abort_flag;
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5;
-    const size_t tile_bytes = (size_t)2 * kAP * kWideMax * 2;  // hi + lo, 128 rows x 128
-    char *ops = smem_raw;                                         // two activation tiles
-    char *wbuf = smem_raw + 2 * tile_bytes;                       // one layer's weights, hi + lo
-    float *par = reinterpret_cast<float *>(wbuf + (size_t)2 * kWideMax * kWideMax * 2);
-    float *eps = par + net.par_total;
-    // the next tile's descriptor rows, brought in by a bulk copy during this tile's net
-    float *gbuf = reinterpret_cast<float *>(
-        smem_raw + align_up(2 * tile_bytes + (size_t)2 * kWideMax * kWideMax * 2 +
-                                (size_t)(net.par_total + kMQ * kAP) * 4,
-                            128));
-    auto tile = [&](int k) { return ops + (k & 1) * tile_bytes; };
+    char *tile = smem_raw;  // the operand tile: bf16 hi, then lo
+    char *wbuf = smem_raw + net.wbuf_off;
+    float *par = reinterpret_cast<float *>(smem_raw + net.par_off);
+    float *eps = reinterpret_cast<float *>(smem_raw + net.eps_off);
+    float *gbuf = reinterpret_cast<float *>(smem_raw + net.gbuf_off);
     for (int L2 = 0; L2 < net.nh; ++L2) {
         const int N = net.dims[L2 + 1], Np = net.nout[L2];
         const float *b = w + net.woff[L2] + (size_t)N * net.dims[L2];
@@ -1252,7 +1262,6 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
         tc::mbar_init(&mbar, 1);
         tc::mbar_init(&wbar, 1);
         tc::mbar_init(&gbar, 1);
-        abort_flag = 0;
     }
     tc::fence_before();
     __syncthreads();
@@ -1260,12 +1269,16 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
     const uint32_t tmem = tmem_slot, bar = tc::smem_u32(&mbar);
     uint32_t phase = 0;
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
-    const uint32_t bcol = 3u * kWideMax;
+    auto dfcol = [&](int k) { return (uint32_t)(net.zbw + k * net.wmax); };  // act'(z_k), smooth activations
+    const bool relu = net.relu_bits != 0;
+    // A bounded wait that gives up sets gave_up in its thread; the barriers that
+    // end the stages OR it over the block into `aborted`: no further MMA or copy
+    // is issued, the tile loop ends and what is in flight is drained at the end.
+    bool gave_up = false, aborted = false;
+    int commits = 0;
     auto wait_mma = [&]() {
-        if (!tc::mbar_wait(bar, phase)) {
-            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
-            abort_flag = 1;
-        }
+        if (aborted) return;  // nothing was issued
+        if (!tc::mbar_wait(bar, phase)) gave_up = true;
         phase ^= 1u;
         tc::fence_after();
     };
@@ -1279,7 +1292,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
     auto request = [&](int L2) {
         if (L2 == in_buf) return;
         in_buf = L2;
-        if (tid == 0 && !abort_flag) {
+        if (tid == 0 && !aborted && !gave_up) {
             const uint32_t bytes = (uint32_t)(4 * net.nout[L2] * net.kin[L2]);
             tc::mbar_arrive_expect_tx(wbar_u32, bytes);
             tc::bulk_g2s(wb_u32, wsplit + net.wsm_off[L2], bytes, wbar_u32);
@@ -1288,10 +1301,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
     };
     auto ensure = [&]() {  // thread 0 only
         if (!w_pending) return;
-        if (!tc::mbar_wait(wbar_u32, wphase)) {
-            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
-            abort_flag = 1;
-        }
+        if (!tc::mbar_wait(wbar_u32, wphase)) gave_up = true;
         wphase ^= 1u;
         w_pending = false;
     };
@@ -1304,44 +1314,46 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
     uint32_t gphase = 0;
     const uint32_t gbuf_u32 = tc::smem_u32(gbuf), gbar_u32 = tc::smem_u32(&gbar);
     auto request_g = [&](long long tl) {
-        if (tid != 0 || abort_flag || tl >= ntiles) return;
+        if (!net.prefetch_g || tid != 0 || aborted || gave_up || tl >= ntiles) return;
         const long long r0 = tl * kAP;
-        const uint32_t bytes = (uint32_t)(min((long long)kAP, P - r0) * kGRow * 4);
+        const uint32_t bytes = (uint32_t)(min((long long)kAP, P - r0) * net.g_ld * 4);
         tc::mbar_arrive_expect_tx(gbar_u32, bytes);
-        tc::bulk_g2s(gbuf_u32, g_rows + r0 * kGRow, bytes, gbar_u32);
+        tc::bulk_g2s(gbuf_u32, g_rows + r0 * net.g_ld, bytes, gbar_u32);
         g_pending = true;
     };
     request_g(blockIdx.x);
     for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        if (aborted) break;
         const long long r0 = tl * kAP;
         const int valid = (int)min((long long)kAP, P - r0);
-        if (!tc::mbar_wait(gbar_u32, gphase)) {  // every thread reads gbuf
-            atomicOr(&g_amlp_device_error, kErrMbarTimeout);
-            abort_flag = 1;
+        if (net.prefetch_g) {  // every thread reads gbuf
+            if (!tc::mbar_wait(gbar_u32, gphase)) gave_up = true;
+            gphase ^= 1u;
+            if (tid == 0) g_pending = false;
         }
-        gphase ^= 1u;
-        if (tid == 0) g_pending = false;
         for (int c0 = 8 * h; c0 < Kg; c0 += 8 * kMQ) {
             float v[8];
-            const float4 *src = reinterpret_cast<const float4 *>(gbuf + p * kGRow + c0);
-            const float4 lo4 = p < valid ? src[0] : make_float4(0.f, 0.f, 0.f, 0.f);
-            const float4 hi4 = p < valid ? src[1] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float *src = net.prefetch_g ? gbuf + p * net.g_ld + c0 : g_rows + (r0 + p) * net.g_ld + c0;
+            const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 lo4 = p < valid ? reinterpret_cast<const float4 *>(src)[0] : zero4;
+            const float4 hi4 = p < valid ? reinterpret_cast<const float4 *>(src)[1] : zero4;
             v[0] = lo4.x, v[1] = lo4.y, v[2] = lo4.z, v[3] = lo4.w;
             v[4] = hi4.x, v[5] = hi4.y, v[6] = hi4.z, v[7] = hi4.w;
-            store_split8(tile(0), Kg, p, c0, v);
+            store_split8(tile, Kg, p, c0, v);
         }
+        uint64_t m0 = 0, m1 = 0, m2 = 0;  // ReLU: act'(z) bits of hidden layers 0, 1, 2 (this thread's chunks)
         for (int L2 = 0; L2 < net.nh; ++L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
             request(L2);
             tc::fence_async_smem();
-            __syncthreads();
+            aborted = __syncthreads_or(gave_up) != 0;
             if (L2 == 0) request_g(tl + gridDim.x);  // gbuf has been read: prefetch the next tile
             if (tid == 0) ensure();
-            if (tid == 0 && !abort_flag) {
+            if (tid == 0 && !aborted && !gave_up) {
                 tc::fence_after();
-                mma3<false>(tmem + (uint32_t)(L2 * kWideMax), tile(L2), Kp, wbuf, (size_t)Np * Kp * 2, Np, false,
-                            256, 128, (uint32_t)Kp * 16);
+                mma3<false>(tmem, tile, Kp, wbuf, (size_t)Np * Kp * 2, Np, false, 256, 128, (uint32_t)Kp * 16);
                 tc::commit(bar);
+                ++commits;
             }
             wait_mma();
             if (L2 + 1 < net.nh) request(L2 + 1);  // overlaps this layer's epilogue
@@ -1349,10 +1361,10 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             const float *bias = par + net.bias_off[L2];
             const float *wl = par + net.bias_off[net.nh];
             float esum = 0.f;
-            for (int c0 = 8 * h; c0 < Np; c0 += 8 * kMQ) {
+            uint64_t bits = 0;
+            for (int j = 0, c0 = 8 * h; c0 < Np; ++j, c0 += 8 * kMQ) {
                 float z[8], v[8], dv[8];
-                const uint32_t zaddr = tmem + lane_base + (uint32_t)(L2 * kWideMax) + c0;
-                tc::tmem_ld8(zaddr, z);
+                tc::tmem_ld8(tmem + lane_base + c0, z);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
                     float zz = z[k] + bias[c0 + k], fz, dfz;
@@ -1363,50 +1375,65 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
                     } else {
                         v[k] = fz;
                         dv[k] = dfz;
+                        if (dfz != 0.f) bits |= 1ull << (8 * j + k);
                     }
                 }
-                store_split8(tile(L2 + 1), Np, p, c0, v);
-                // act'(z) replaces z in TMEM: the backward needs only the derivative
-                if (!last) tc::tmem_st8(zaddr, dv);
+                store_split8(tile, Np, p, c0, v);  // the MMA that read the tile is complete
+                if (!last && !relu) tc::tmem_st8(tmem + lane_base + dfcol(L2) + c0, dv);  // for the backward
             }
-            if (last) eps[h * kAP + p] = esum;
-            else tc::tmem_wait_st();
+            if (last) {
+                eps[h * kAP + p] = esum;
+            } else if (relu) {
+                if (L2 == 0) m0 = bits;
+                else if (L2 == 1) m1 = bits;
+                else m2 = bits;
+            } else {
+                tc::tmem_wait_st();
+            }
             tc::fence_before();
             tc::fence_async_smem();
-            __syncthreads();
+            aborted = __syncthreads_or(gave_up) != 0;
         }
         if (tid < kAP && p < valid)
             y_rows[r0 + p] = (eps[p] + eps[kAP + p]) + (eps[2 * kAP + p] + eps[3 * kAP + p]) +
                              par[net.bias_off[net.nh] + kWideMax];
+        // backward: delta_{k-1} = (delta_k W_k) * act'(z_{k-1}); dE/dg = delta_0 W_0
         for (int L2 = net.nh - 1; L2 >= 0; --L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
             request(L2);
             tc::fence_async_smem();
-            __syncthreads();
+            aborted = __syncthreads_or(gave_up) != 0;
             if (tid == 0) ensure();
-            if (tid == 0 && !abort_flag) {
+            if (tid == 0 && !aborted && !gave_up) {
                 tc::fence_after();
-                mma3<false>(tmem + bcol, tile(L2 + 1), Np, wbuf, (size_t)Np * Kp * 2, Kp, true, 2 * Kp * 16,
-                     (uint32_t)Kp * 16, 128);
+                // B = W_k read as MN-major (the transpose): N' = Kp, K' = Np
+                mma3<false>(tmem, tile, Np, wbuf, (size_t)Np * Kp * 2, Kp, true, 2 * Kp * 16, (uint32_t)Kp * 16, 128);
                 tc::commit(bar);
+                ++commits;
             }
             wait_mma();
             request(L2 > 0 ? L2 - 1 : 0);  // the next layer needed (layer 0 again for the next tile)
             if (L2 > 0) {
-                for (int c0 = 8 * h; c0 < Kp; c0 += 8 * kMQ) {
+                const uint64_t bits = L2 == 1 ? m0 : (L2 == 2 ? m1 : m2);
+                for (int j = 0, c0 = 8 * h; c0 < Kp; ++j, c0 += 8 * kMQ) {
                     float dz[8], df[8], v[8];
-                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dz);
-                    tc::tmem_ld8(tmem + lane_base + (uint32_t)((L2 - 1) * kWideMax) + c0, df);  // act'(z)
+                    tc::tmem_ld8(tmem + lane_base + c0, dz);
+                    if (relu) {
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) v[k] = dz[k] * df[k];
-                    store_split8(tile(L2), Kp, p, c0, v);
+                        for (int k = 0; k < 8; ++k) v[k] = (bits >> (8 * j + k)) & 1ull ? dz[k] : 0.f;
+                    } else {
+                        tc::tmem_ld8(tmem + lane_base + dfcol(L2 - 1) + c0, df);
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) v[k] = dz[k] * df[k];
+                    }
+                    store_split8(tile, Kp, p, c0, v);
                 }
             } else {
                 for (int c0 = 8 * h; c0 < Kp; c0 += 8 * kMQ) {
                     float dg[8];
-                    tc::tmem_ld8(tmem + lane_base + bcol + c0, dg);
+                    tc::tmem_ld8(tmem + lane_base + c0, dg);
                     if (p < valid) {
-                        float4 *dst = reinterpret_cast<float4 *>(dg_rows + (r0 + p) * kGP + c0);
+                        float4 *dst = reinterpret_cast<float4 *>(dg_rows + (r0 + p) * net.gp + c0);
                         dst[0] = make_float4(dg[0], dg[1], dg[2], dg[3]);
                         dst[1] = make_float4(dg[4], dg[5], dg[6], dg[7]);
                     }
@@ -1414,13 +1441,18 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             }
             tc::fence_before();
             tc::fence_async_smem();
-            __syncthreads();
+            aborted = __syncthreads_or(gave_up) != 0;
         }
-        if (abort_flag) break;
     }
-    if (abort_flag && tid == 0) tc::mbar_wait(bar, phase);
-    if (tid == 0) ensure();  // no copy may still be writing shared memory at exit
-    if (tid == 0 && g_pending) tc::mbar_wait(gbar_u32, gphase);
+    aborted = __syncthreads_or(gave_up) != 0;
+    if (tid == 0) {
+        bool drained = true;
+        // the last MMA issued (commit number `commits`, parity (commits - 1) & 1) may still be in flight
+        if (commits > 0) drained &= tc::mbar_wait(bar, (uint32_t)((commits - 1) & 1));
+        if (w_pending) drained &= tc::mbar_wait(wbar_u32, wphase);  // no copy may still write shared memory
+        if (g_pending) drained &= tc::mbar_wait(gbar_u32, gphase);
+        if (aborted || !drained) atomicOr(&g_amlp_device_error, kErrMbarTimeout);
+    }
     __syncthreads();
     if (warp == 0) {
         tc::fence_after();
@@ -1527,14 +1559,18 @@ extern "C" amlp_status amlp_multi_forces_adjoint(const float *d_pos, const float
 }
 
 
-static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
+constexpr size_t kMlpSmemMax = 226 * 1024;  // dynamic shared memory of k_mlp_grad
+
+// The net of the wide path and k_mlp_grad's geometry: Kg = padded descriptor
+// width (the first layer's K), g_ld = row stride of the g rows.
+static amlp_status wide_net(const amlp_mlp *mlp, int Kg, int g_ld, AdjNet *net) {
     const int nh = mlp->n_layers - 1;
-    if (nh < 1 || nh > kMaxHidden) return AMLP_ERR_UNSUPPORTED;
+    if (nh < 1 || nh > kMaxHiddenWide) return AMLP_ERR_UNSUPPORTED;
     *net = AdjNet{};
     net->nh = nh;
     net->act = mlp->act;
     long long off = 0;
-    int par = 0;
+    int par = 0, wbytes = 0;
     for (int k = 0; k <= mlp->n_layers; ++k) net->dims[k] = mlp->dims[k];
     for (int k = 0; k <= nh; ++k) {
         net->woff[k] = off;
@@ -1542,16 +1578,36 @@ static amlp_status wide_net(const amlp_mlp *mlp, AdjNet *net) {
     }
     for (int k = 0; k < nh; ++k) {
         if (mlp->dims[k + 1] > kWideMax) return AMLP_ERR_UNSUPPORTED;
-        net->kin[k] = k == 0 ? kGP : net->nout[k - 1];
+        net->kin[k] = k == 0 ? Kg : net->nout[k - 1];
         net->nout[k] = (mlp->dims[k + 1] + 15) / 16 * 16;
         net->bias_off[k] = par;
         par += net->nout[k];
         net->wsm_off[k] = net->wsm_total;  // pre-split weights of layer k: hi then lo
         net->wsm_total += 4 * net->nout[k] * net->kin[k];
+        wbytes = std::max(wbytes, 4 * net->nout[k] * net->kin[k]);
+        net->wmax = std::max(net->wmax, net->nout[k]);
     }
     net->bias_off[nh] = par;
     par += kWideMax + 4;
     net->par_total = par;
+    net->g_ld = g_ld;
+    net->gp = Kg;
+    net->zbw = std::max(Kg, net->wmax);
+    net->relu_bits = mlp->act == AMLP_ACT_RELU ? 1 : 0;
+    // smooth activations keep act'(z) of nh - 1 layers in TMEM beside the product region
+    if (!net->relu_bits && net->zbw + (nh - 1) * net->wmax > 512) return AMLP_ERR_UNSUPPORTED;
+    size_t o = align_up((size_t)2 * kAP * net->zbw * 2, 128);  // operand tile, bf16 hi + lo
+    net->wbuf_off = (int)o;
+    o += align_up((size_t)wbytes, 128);
+    net->par_off = (int)o;
+    o += align_up((size_t)par * 4, 128);
+    net->eps_off = (int)o;
+    o += align_up((size_t)kMQ * kAP * 4, 128);
+    net->gbuf_off = (int)o;
+    const size_t with_g = o + (size_t)kAP * g_ld * 4;
+    net->prefetch_g = with_g <= kMlpSmemMax ? 1 : 0;
+    net->smem = (int)(net->prefetch_g ? with_g : o);
+    if ((size_t)net->smem > kMlpSmemMax) return AMLP_ERR_UNSUPPORTED;
     return AMLP_OK;
 }
 
@@ -1574,9 +1630,13 @@ static amlp_status check_pair_args(const float *d_pos, const float *d_quat, cons
     amlp_status st = check_nep(nep);
     if (st) return st;
     if (!d_pos || !d_quat || !d_npairs || cap < 0 || (cap > 0 && !d_pairs)) return AMLP_ERR_INVALID_ARG;
+    if (hyper_kind(nep) == 2) return 2 * nep->npts <= direct::kMaxNd ? AMLP_OK : AMLP_ERR_UNSUPPORTED;
     if (hyper_kind(nep) != 1 || nep_D(nep) > kGP) return AMLP_ERR_UNSUPPORTED;
     return AMLP_OK;
 }
+
+// Grid of the direct-form descriptor kernels (one warp per pair, grid-stride).
+constexpr int kDirectBlocks = 8 * kNumSM;
 
 static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
                                        const long long *d_npairs, long long cap, const amlp_nep *nep,
@@ -1591,8 +1651,29 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     size_t need;
     amlp_adjoint_workspace_bytes(cap, &need);
     if (!d_ws || ws_bytes < need) return AMLP_ERR_WORKSPACE;
+    cudaStream_t s = as_stream(stream);
+    const float inv_rc = 1.0f / nep->nep_cutoff, rng = nep->en_max - nep->en_min;
     AdjNet net;
-    if ((st = wide_net(mlp, &net))) return st;
+    if (hyper_kind(nep) == 2) {  // D = 121: the direct-form descriptor passes around the same net kernel
+        if (d_rep) return AMLP_ERR_UNSUPPORTED;
+        if ((st = wide_net(mlp, kGP2, kGRow2, &net))) return st;
+        Carver c(d_ws, ws_bytes);
+        float *g_rows = c.take<float>((size_t)cap * kGRow2);
+        float *dg_rows = c.take<float>((size_t)cap * kGP2);
+        float *y_rows = c.take<float>((size_t)cap);
+        char *wsplit = c.take<char>(kWeightSplitBytes);
+        if (!c.ok()) return AMLP_ERR_WORKSPACE;
+        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, net.smem));
+        direct::k_desc_direct_fwd<<<kDirectBlocks, 32 * direct::kWarps, 0, s>>>(
+            d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, nep->npts, inv_rc, g_rows, kGRow2);
+        k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
+        k_mlp_grad<<<kNumSM, kMThreads, net.smem, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
+        direct::k_desc_direct_bwd<<<kDirectBlocks, 32 * direct::kWarps, 0, s>>>(
+            d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, nep->npts, inv_rc, nep->en_min, rng, dg_rows,
+            kGP2, y_rows, d_wt, clip, d_F, d_T, d_pe);
+        return check_launch();
+    }
+    if ((st = wide_net(mlp, kGP, kGRow, &net))) return st;
     Carver c(d_ws, ws_bytes);
     float *g_rows = c.take<float>((size_t)cap * kGRow);
     float *dg_rows = c.take<float>((size_t)cap * kGP);
@@ -1601,13 +1682,9 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     float *a_rows = c.take<float>(adj_a_bytes(cap) / 4);
     const int npts = nep->npts;
     const size_t smem_desc = wide_desc_smem(npts);
-    const size_t smem_mlp = align_up((size_t)2 * (2 * kAP * kWideMax * 2) + (size_t)2 * kWideMax * kWideMax * 2 +
-                                     (size_t)(net.par_total + kMQ * kAP) * 4, 128) +
-                            (size_t)kAP * kGRow * 4;
-    if (smem_desc > 220 * 1024 || smem_mlp > 226 * 1024) return AMLP_ERR_UNSUPPORTED;
+    const size_t smem_mlp = (size_t)net.smem;
+    if (smem_desc > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
-    cudaStream_t s = as_stream(stream);
-    const float inv_rc = 1.0f / nep->nep_cutoff, rng = nep->en_max - nep->en_min;
     const bool multi = d_rep != nullptr;
     auto fwd = multi ? k_adj_desc<Cfg, true, false> : k_adj_desc<Cfg, false, false>;
     auto bwd = multi ? k_adj_desc<Cfg, true, true> : k_adj_desc<Cfg, false, true>;
@@ -1658,6 +1735,11 @@ extern "C" amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_
     if (st) return st;
     if (!d_g || ld_g < nep_D(nep)) return AMLP_ERR_INVALID_ARG;
     if (cap == 0) return AMLP_OK;
+    if (hyper_kind(nep) == 2) {
+        direct::k_desc_direct_fwd<<<kDirectBlocks, 32 * direct::kWarps, 0, as_stream(stream)>>>(
+            d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, nep->npts, 1.0f / nep->nep_cutoff, d_g, ld_g);
+        return check_launch();
+    }
     const size_t smem = wide_desc_smem(nep->npts);
     if (smem > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;

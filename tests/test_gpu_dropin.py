@@ -208,3 +208,16 @@ def test_command_line_adjoint_method(files, monkeypatch):
     a, b = sim.system.pos.cpu().numpy(), e.pos.cpu().numpy()
     assert np.abs(a - b).max() <= 1e-4, np.abs(a - b).max()
     assert read_last_frame(os.path.join(files["dir"], "out", "adj.gsd")).step == 0
+
+
+def test_reference_model_on_the_tensor_core_adjoint(files):
+    """The reference's own 150-wide model (model_th_C104, four ReLU layers)
+    through the drop-in classes with the adjoint method runs on the tensor-core
+    wide path; its forces are checked against FP64 in test_gpu_parity."""
+    from amlp import _lib
+    sim = _builder(files, method="adjoint")
+    sim.run(5)
+    torch.cuda.synchronize()
+    assert sim.system.adj_ws is not None
+    assert np.isfinite(sim.system.pos.cpu().numpy()).all()
+    assert _lib.device_error() == 0

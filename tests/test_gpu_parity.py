@@ -459,3 +459,38 @@ def test_force_scatter_takes_pairs_in_any_order(method):
     for x, y in zip(a[:2], b[:2]):
         np.testing.assert_allclose(x, y, rtol=0, atol=1e-5 * max(1.0, np.abs(x).max()))
     assert abs(a[2] - b[2]) <= 1e-9 * max(1.0, abs(a[2]))
+
+
+@pytest.mark.parametrize("name", ["th_C104", "th_C100", "cube_C104"])
+def test_adjoint_reference_models_vs_fp64_exact(name):
+    """The reference's own trained models (TheEnergyNet(150, 3, D): four 150-wide
+    ReLU layers, Sim.py:60, ForceEvaluator.py:6-26; D = 47 for the C104 models,
+    121 for C100 with its direct-form descriptor passes) on the tensor-core adjoint
+    path (amlp_forces_adjoint_wide) against the FP64 exact derivative of the same
+    pair energy: relative 1e-3 on forces and torques (norm over bodies)."""
+    from amlp import _lib
+    from oracle import adjoint
+    c = load_case(name)
+    shape, hyp, layers = case_shape(c), _hyp(c), case_model(c)
+    assert [W.shape[0] for W, _ in layers[:-1]] == [150] * 4
+    pairs = c["pairs0"]
+    F, T, pe = gh.fused_forces(c["pos0"], c["orient0"], c["L"], pairs, shape, hyp, layers, "relu",
+                               method="amlp_forces_adjoint_wide")
+    assert _lib.device_error() == 0
+    ref = adjoint.exact_pair_forces(c["pos0"], c["orient0"], pairs, c["L"], shape, hyp, layers, "relu")
+    for got, want in ((F, ref["forces"]), (T, ref["torques"])):
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert err <= 1e-3, err
+    assert abs(pe - ref["E"].sum()) <= 1e-4 * max(1.0, np.abs(ref["E"]).sum())
+
+
+@pytest.mark.parametrize("widths,act", [((150, 150, 150, 150), "relu"), ((150, 150, 150), "silu"),
+                                        ((128, 128, 128, 128), "tanh"), ((160, 96), "relu")])
+def test_adjoint_wide_nets_to_160_and_four_layers(widths, act):
+    """k_mlp_grad at the widths and depths beyond the fused kernel: up to 160 wide
+    and four hidden layers; ReLU derivatives kept as bits, smooth ones in TMEM."""
+    F, T, pe, ref = _adjoint_case("cube26", 500, 0.45, 17, widths, act, method="amlp_forces_adjoint_wide")
+    for got, want in ((F, ref["forces"]), (T, ref["torques"])):
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert err <= 1e-3, err
+    assert abs(pe - ref["E"].sum()) <= 1e-4 * max(1.0, np.abs(ref["E"]).sum())
