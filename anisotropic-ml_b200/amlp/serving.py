@@ -5,22 +5,28 @@ over time. Each is admitted, in arrival order, as soon as its memory fits a
 fixed HBM budget. Admitted systems stay resident on the device until they
 finish.
 
-Systems of one shape are packed into a bucket:
-- bodies are concatenated, and a per-body system index points at per-system
-  box, temperature, degrees of freedom and thermostat;
+Systems of one shape share a bucket, buffers of a fixed capacity:
+- each system owns a contiguous range of body slots and one system slot; a
+  per-body system index points at per-system box, temperature, degrees of
+  freedom and thermostat; free body slots (index -1) and free system slots are
+  skipped by the kernels;
 - one time step of a bucket is: the pair filter, the adjoint force kernel
   (net on the tensor cores), and the two NVT halves, each a single launch over
-  every system of the bucket (``amlp_multi_*``).
+  the bucket's capacity (``amlp_multi_*``), with the same arguments whatever
+  systems are resident.
 
 The server advances all buckets in segments of ``segment`` steps (100, the
 Verlet rebuild period of the reference, ``Sim.py:87``). Each segment:
 - rebuilds every system's Verlet list;
-- replays one captured CUDA graph holding all steps of all buckets;
+- replays one CUDA graph holding all steps of all buckets. It is captured once
+  and captured again only when a bucket's capacity grows, so admissions and
+  departures cost a few small copies, not a capture;
 - then admits new arrivals and retires finished systems. This is the only time
   the set of systems can change.
 
-Throughput (particle-steps/s), per-segment latency percentiles and
-per-request completion latencies are recorded.
+Throughput (particle-steps/s), per-segment latency percentiles (device time of
+the replay, and wall time of lists + replay) and per-request completion
+latencies are recorded.
 """
 from __future__ import annotations
 
@@ -83,9 +89,17 @@ def system_bytes(n: int, shape, phi: float) -> int:
 
 
 class _Bucket:
-    """All active systems of one shape, packed for multi-system launches."""
+    """All active systems of one shape, in buffers of a fixed capacity.
 
-    def __init__(self, shape_name: str, net: EnergyNet, hypers: Hypers, dt: float, device):
+    Every admitted system gets a system slot r (its box, temperature, degrees of
+    freedom and thermostat in row r of ``rp`` / ``th``) and a contiguous range of
+    body slots; free body slots have ``rep = -1`` and free system slots
+    ``n_dof = 0``, which the multi-system kernels skip. The launches of a step
+    therefore have the same arguments whatever the active set, and one captured
+    CUDA graph serves every segment until a capacity has to grow."""
+
+    def __init__(self, shape_name: str, net: EnergyNet, hypers: Hypers, dt: float, device,
+                 body_cap: int = 1 << 16, sys_cap: int = 64):
         self.shape = get_shape(shape_name)
         self.net, self.hypers, self.dt, self.device = net, hypers, dt, device
         self.systems: list[_System] = []
@@ -104,116 +118,211 @@ class _Bucket:
         for k in range(3):
             self.prm.moi[k] = float(self.shape.moi[k])
         self.r_verlet = float(self.shape.cutoff) + 2.0
-        self.N = 0
+        self.where = {}            # rid -> (system slot, first body slot)
+        self.generation = 0        # bumped whenever the buffers are reallocated
+        self._alloc(body_cap, sys_cap, 1 << 20)
 
-    # -------------------------------------------------------------- packing
-    def pack(self, systems: list[_System]) -> None:
-        """Lay out `systems` (states from the previous packing or new) contiguously."""
-        old = self._snapshot_states() if self.N else {}
-        self.systems = systems
+    # -------------------------------------------------------------- buffers
+    def _alloc(self, body_cap: int, sys_cap: int, pair_cap: int) -> None:
+        """(Re)allocate every buffer at the given capacities, keeping the
+        resident systems' state."""
+        keep = self._snapshot_states() if getattr(self, "systems", None) and hasattr(self, "pos") else {}
+        keep_th = {s.req.rid: self._thermostat_bytes(s) for s in self.systems} if keep else {}
         f32 = dict(dtype=torch.float32, device=self.device)
-        ns = [s.req.n for s in systems]
-        self.N = sum(ns)
-        self.first = np.concatenate([[0], np.cumsum(ns)[:-1]]).astype(np.int64) if ns else np.zeros(0, np.int64)
-        if not systems:
-            return
-        host = {k: [] for k in ("pos", "orient", "vel", "angmom", "mass")}
-        for s in systems:
-            st = old.get(s.req.rid, s.state)
-            for k in host:
-                host[k].append(np.asarray(getattr(st, k), np.float32))
-        self.pos = torch.tensor(np.concatenate(host["pos"]), **f32)
-        self.quat = torch.tensor(np.concatenate(host["orient"]), **f32)
-        self.vel = torch.tensor(np.concatenate(host["vel"]), **f32)
-        self.angmom = torch.tensor(np.concatenate(host["angmom"]), **f32)
-        self.mass = torch.tensor(np.concatenate(host["mass"]), **f32)
-        self.rep = torch.tensor(np.repeat(np.arange(len(systems), dtype=np.int32), ns), device=self.device)
-        self.F = torch.zeros(self.N, 3, **f32)
-        self.T = torch.zeros(self.N, 3, **f32)
-        self.accel = torch.zeros(self.N, 3, **f32)
-        self.dp = torch.zeros(self.N, 4, **f32)
-        rp = (Replica * len(systems))()
-        th = bytearray()
-        for r, s in enumerate(systems):
-            rp[r].kT = s.req.kT
-            rp[r].n_dof = float((s.req.n - 1) * 3)
-            rp[r].rn_dof = float(s.req.n * 3)
-            rp[r].box = float(s.state.L)
-            rp[r].nve = 0
-            if s.th:
-                th += s.th
-            else:
-                t = Thermostat()
-                t.xi, t.eta, t.xi_rot, t.eta_rot, t.thermo_fac = THERMOSTAT_SEED
-                th += bytes(t)
-        self.rp = torch.frombuffer(bytearray(bytes(rp)), dtype=torch.uint8).to(self.device)
-        self.th = torch.frombuffer(th, dtype=torch.uint8).to(self.device)
-        self.pe = torch.zeros(len(systems), dtype=torch.float64, device=self.device)
-        caps = [verlet_capacity(s.req.n, self.shape, s.req.phi, self.r_verlet) for s in systems]
-        self.caps = caps
-        self.cap = sum(caps)
+        self.body_cap, self.sys_cap, self.cap = int(body_cap), int(sys_cap), int(pair_cap)
+        self.pos = torch.zeros(self.body_cap, 3, **f32)
+        self.quat = torch.zeros(self.body_cap, 4, **f32)
+        self.quat[:, 0] = 1.0
+        self.vel = torch.zeros(self.body_cap, 3, **f32)
+        self.angmom = torch.zeros(self.body_cap, 4, **f32)
+        self.mass = torch.ones(self.body_cap, **f32)
+        self.rep = torch.full((self.body_cap,), -1, dtype=torch.int32, device=self.device)
+        self.F = torch.zeros(self.body_cap, 3, **f32)
+        self.T = torch.zeros(self.body_cap, 3, **f32)
+        self.accel = torch.zeros(self.body_cap, 3, **f32)
+        self.dp = torch.zeros(self.body_cap, 4, **f32)
+        self.rp = torch.zeros(self.sys_cap * ctypes.sizeof(Replica), dtype=torch.uint8, device=self.device)
+        self.th = torch.zeros(self.sys_cap * ctypes.sizeof(Thermostat), dtype=torch.uint8, device=self.device)
+        self.pe = torch.zeros(self.sys_cap, dtype=torch.float64, device=self.device)
         self.vpairs = torch.empty(self.cap, 2, dtype=torch.int32, device=self.device)
         self.vgap = torch.empty(self.cap, 2, dtype=torch.int32, device=self.device)
         self.fpairs = torch.empty(self.cap, 2, dtype=torch.int32, device=self.device)
         self.nv = torch.zeros(1, dtype=torch.int64, device=self.device)
         self.nf = torch.zeros(1, dtype=torch.int64, device=self.device)
-        self.counts = torch.zeros(len(systems), dtype=torch.int64, device=self.device)
-        self.nl_ws = torch.empty(max(size_query("amlp_nlist_workspace_bytes", s.req.n, float(s.state.L), self.r_verlet)
-                                     for s in systems), dtype=torch.uint8, device=self.device)
+        self.counts = torch.zeros(self.sys_cap, dtype=torch.int64, device=self.device)
+        self.nl_ws = torch.empty(0, dtype=torch.uint8, device=self.device)
         self.f_ws = torch.empty(size_query("amlp_filter_workspace_bytes", self.cap), dtype=torch.uint8,
                                 device=self.device)
         self.adj_ws = None
-        if self.net.max_hidden > 64:  # wider nets take the three-kernel adjoint path
+        if self.net.max_hidden > 64 or self.hypers.D > 48:  # beyond the fused adjoint kernel: the wide path
             self.adj_ws = torch.empty(size_query("amlp_adjoint_workspace_bytes", self.cap), dtype=torch.uint8,
                                       device=self.device)
+        self.free_sys = list(range(self.sys_cap))
+        self.free_bodies = [(0, self.body_cap)]   # (first, length), sorted by first
+        self.where = {}
+        self.generation += 1
+        old = self.systems
+        self.systems = []
+        if old:
+            self._place([(s, keep[s.req.rid], keep_th[s.req.rid]) for s in old])
+
+    def _take_bodies(self, n: int) -> int | None:
+        for k, (a, m) in enumerate(self.free_bodies):
+            if m >= n:
+                self.free_bodies[k] = (a + n, m - n)
+                if m == n:
+                    del self.free_bodies[k]
+                return a
+        return None
+
+    def _give_bodies(self, a: int, n: int) -> None:
+        self.free_bodies.append((a, n))
+        self.free_bodies.sort()
+        merged = []
+        for b, m in self.free_bodies:
+            if merged and merged[-1][0] + merged[-1][1] == b:
+                merged[-1] = (merged[-1][0], merged[-1][1] + m)
+            else:
+                merged.append((b, m))
+        self.free_bodies = merged
+
+    # -------------------------------------------------------------- admission
+    def _thermostat_bytes(self, s: _System) -> bytes:
+        r = self.where[s.req.rid][0]
+        tsz = ctypes.sizeof(Thermostat)
+        return self.th[r * tsz:(r + 1) * tsz].cpu().numpy().tobytes()
+
+    def _place(self, entries) -> None:
+        """Put (system, host state, thermostat bytes or b"") entries into free slots."""
+        tsz, rsz = ctypes.sizeof(Thermostat), ctypes.sizeof(Replica)
+        for s, st, thb in entries:
+            n = s.req.n
+            r = self.free_sys.pop(0)
+            a = self._take_bodies(n)
+            for name, t in (("pos", self.pos), ("orient", self.quat), ("vel", self.vel), ("angmom", self.angmom),
+                            ("mass", self.mass)):
+                t[a:a + n].copy_(torch.from_numpy(np.ascontiguousarray(getattr(st, name), np.float32)))
+            self.rep[a:a + n] = r
+            q = Replica()
+            q.kT, q.n_dof, q.rn_dof, q.box, q.nve = s.req.kT, float((n - 1) * 3), float(n * 3), float(st.L), 0
+            self.rp[r * rsz:(r + 1) * rsz].copy_(torch.frombuffer(bytearray(bytes(q)), dtype=torch.uint8))
+            if not thb:
+                t = Thermostat()
+                t.xi, t.eta, t.xi_rot, t.eta_rot, t.thermo_fac = THERMOSTAT_SEED
+                thb = bytes(t)
+            self.th[r * tsz:(r + 1) * tsz].copy_(torch.frombuffer(bytearray(thb), dtype=torch.uint8))
+            self.where[s.req.rid] = (r, a)
+            s.state = st
+            self.systems.append(s)
+        # kinetic energies of every system from its current state (the value step one
+        # would have left), so that step two of the next segment starts right
         call("amlp_multi_nvt_init", self.vel.data_ptr(), self.quat.data_ptr(), self.angmom.data_ptr(),
-             self.mass.data_ptr(), self.rep.data_ptr(), self.N, len(systems), ctypes.byref(self.prm),
+             self.mass.data_ptr(), self.rep.data_ptr(), self.body_cap, self.sys_cap, ctypes.byref(self.prm),
              self.th.data_ptr(), _stream())
 
-    def _snapshot_states(self) -> dict:
+    def _verlet_cap(self, s: _System) -> int:
+        return verlet_capacity(s.req.n, self.shape, s.req.phi, self.r_verlet)
+
+    def admit(self, new: list[_System]) -> None:
+        """Admit systems (their states from their requests); grows the buffers
+        (a new generation) when a capacity is short."""
+        if not new:
+            return
+        bodies = sum(m for _, m in self.free_bodies)
+        need_b = sum(s.req.n for s in new)
+        need_s = len(self.systems) + len(new)
+        need_p = sum(self._verlet_cap(s) for s in self.systems + new)
+        fits = need_s <= self.sys_cap and need_p <= self.cap and bodies >= need_b
+        if fits:  # a contiguous range for each new system, tried on a copy of the free list
+            trial = list(self.free_bodies)
+            for s in new:
+                k = next((k for k, (_, m) in enumerate(trial) if m >= s.req.n), None)
+                if k is None:
+                    fits = False
+                    break
+                a, m = trial[k]
+                trial[k] = (a + s.req.n, m - s.req.n)
+        if not fits:
+            used = sum(s.req.n for s in self.systems)
+            bc, sc, pc = self.body_cap, self.sys_cap, self.cap
+            while bc < 2 * (used + need_b):  # headroom against fragmentation
+                bc *= 2
+            while sc < need_s:
+                sc *= 2
+            while pc < need_p:
+                pc *= 2
+            self._alloc(bc, sc, pc)
+        self._place([(s, s.state, b"") for s in new])
+
+    def retire(self, gone: list[_System]) -> dict:
+        """Remove systems; returns their host states {rid: State}."""
+        if not gone:
+            return {}
+        states = self._snapshot_states([s.req.rid for s in gone])
+        rsz = ctypes.sizeof(Replica)
+        for s in gone:
+            r, a = self.where.pop(s.req.rid)
+            self.rep[a:a + s.req.n] = -1
+            self.rp[r * rsz:(r + 1) * rsz].zero_()  # n_dof = 0: a free system slot
+            self.free_sys.append(r)
+            self._give_bodies(a, s.req.n)
+        self.free_sys.sort()
+        ids = {s.req.rid for s in gone}
+        self.systems = [s for s in self.systems if s.req.rid not in ids]
+        return states
+
+    def _snapshot_states(self, rids=None) -> dict:
         out = {}
         if not self.systems:
             return out
         pos, quat, vel, ang, mass = (t.cpu().numpy() for t in (self.pos, self.quat, self.vel, self.angmom, self.mass))
-        thb = self.th.cpu().numpy().tobytes()
-        tsz = ctypes.sizeof(Thermostat)
-        for r, s in enumerate(self.systems):
-            a, b = int(self.first[r]), int(self.first[r]) + s.req.n
-            s.th = thb[r * tsz:(r + 1) * tsz]
-            out[s.req.rid] = type(s.state)(pos=pos[a:b], orient=quat[a:b], vel=vel[a:b], angmom=ang[a:b],
-                                           mass=mass[a:b], moi=s.state.moi, L=s.state.L)
+        for s in self.systems:
+            if rids is not None and s.req.rid not in rids:
+                continue
+            _, a = self.where[s.req.rid]
+            b = a + s.req.n
+            out[s.req.rid] = type(s.state)(pos=pos[a:b].copy(), orient=quat[a:b].copy(), vel=vel[a:b].copy(),
+                                           angmom=ang[a:b].copy(), mass=mass[a:b].copy(), moi=s.state.moi,
+                                           L=s.state.L)
         return out
 
     def unpack(self, s: _System):
         """Host copy of system s's state (positions, orientations, velocities, angular momenta)."""
-        return self._snapshot_states()[s.req.rid]
+        return self._snapshot_states([s.req.rid])[s.req.rid]
 
     # -------------------------------------------------------------- stepping
     def rebuild_lists(self) -> None:
         """Verlet list of every system (``amlp_nlist_build`` per system into its
         own slot), then one contiguous list with global body indices."""
         if not self.systems:
+            self.nv.zero_()
             return
         st = _stream()
-        slot = np.concatenate([[0], np.cumsum(self.caps)[:-1]]).astype(np.int64)
-        for r, s in enumerate(self.systems):
-            a, n = int(self.first[r]), s.req.n
-            call("amlp_nlist_build", self.pos[a:a + n].data_ptr(), n, float(s.state.L), self.r_verlet,
-                 self.vgap[int(slot[r]):].data_ptr(), self.caps[r], self.counts[r:r + 1].data_ptr(),
+        caps = [self._verlet_cap(s) for s in self.systems]
+        slot = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+        ws = max(size_query("amlp_nlist_workspace_bytes", s.req.n, float(s.state.L), self.r_verlet)
+                 for s in self.systems)
+        if self.nl_ws.numel() < ws:
+            self.nl_ws = torch.empty(ws, dtype=torch.uint8, device=self.device)
+        firsts = []
+        for k, s in enumerate(self.systems):
+            _, a = self.where[s.req.rid]
+            firsts.append(a)
+            call("amlp_nlist_build", self.pos[a:a + s.req.n].data_ptr(), s.req.n, float(s.state.L), self.r_verlet,
+                 self.vgap[int(slot[k]):].data_ptr(), caps[k], self.counts[k:k + 1].data_ptr(),
                  self.nl_ws.data_ptr(), self.nl_ws.numel(), st)
-        counts = self.counts.cpu().numpy()
-        if np.any(counts > np.asarray(self.caps)):
+        counts = self.counts[:len(self.systems)].cpu().numpy()
+        if np.any(counts > np.asarray(caps)):
             raise RuntimeError("Verlet list of a served system exceeds its capacity")
-        parts = [self.vgap[int(slot[r]):int(slot[r]) + int(counts[r])] + int(self.first[r])
-                 for r in range(len(self.systems)) if counts[r]]
+        parts = [self.vgap[int(slot[k]):int(slot[k]) + int(counts[k])] + int(firsts[k])
+                 for k in range(len(self.systems)) if counts[k]]
         total = int(counts.sum())
         if parts:
             torch.cat(parts, out=self.vpairs[:total])
         self.nv.fill_(total)
 
     def step_kernels(self) -> None:
-        if not self.systems:
-            return
+        """One step of every system of the bucket: the same launches whatever the active set."""
         st = _stream()
         self.F.zero_()
         self.T.zero_()
@@ -230,11 +339,11 @@ class _Bucket:
             call("amlp_multi_forces_adjoint_wide", *args, self.adj_ws.data_ptr(), self.adj_ws.numel(), st)
         call("amlp_multi_nvt_step_two", self.vel.data_ptr(), self.accel.data_ptr(), self.F.data_ptr(),
              self.mass.data_ptr(), self.quat.data_ptr(), self.T.data_ptr(), self.angmom.data_ptr(),
-             self.dp.data_ptr(), self.rep.data_ptr(), self.N, len(self.systems), self.rp.data_ptr(),
+             self.dp.data_ptr(), self.rep.data_ptr(), self.body_cap, self.sys_cap, self.rp.data_ptr(),
              ctypes.byref(self.prm), self.th.data_ptr(), st)
         call("amlp_multi_nvt_step_one", self.pos.data_ptr(), self.vel.data_ptr(), self.accel.data_ptr(),
              self.quat.data_ptr(), self.angmom.data_ptr(), self.dp.data_ptr(), self.mass.data_ptr(),
-             self.rep.data_ptr(), self.N, self.rp.data_ptr(), ctypes.byref(self.prm), self.th.data_ptr(), st)
+             self.rep.data_ptr(), self.body_cap, self.rp.data_ptr(), ctypes.byref(self.prm), self.th.data_ptr(), st)
 
 
 @dataclass
@@ -246,11 +355,16 @@ class ServeStats:
     max_active: int = 0
     graphs_captured: int = 0
 
+    segments_wall_ms: list = field(default_factory=list)
+
     def summary(self) -> dict:
         seg = np.asarray(self.segments_ms) if self.segments_ms else np.zeros(1)
+        wall = np.asarray(self.segments_wall_ms) if self.segments_wall_ms else np.zeros(1)
         lat = np.asarray([c[1] for c in self.completions]) if self.completions else np.zeros(1)
         return {"particle_steps_per_s": self.body_steps / self.wall_s if self.wall_s else 0.0,
                 "segment_ms_p50": float(np.percentile(seg, 50)), "segment_ms_p99": float(np.percentile(seg, 99)),
+                "segment_wall_ms_p50": float(np.percentile(wall, 50)),
+                "segment_wall_ms_p99": float(np.percentile(wall, 99)),
                 "request_latency_s_p50": float(np.percentile(lat, 50)),
                 "request_latency_s_p99": float(np.percentile(lat, 99)),
                 "segments": len(self.segments_ms), "requests": len(self.completions),
@@ -279,21 +393,21 @@ class Server:
         st = make_state(req.n, shape, req.phi, kT=req.kT, seed=req.seed)
         return _System(req=req, state=st, admitted_at=now, mem=system_bytes(req.n, shape, req.phi))
 
-    def _segment(self, steps: int) -> float:
-        """Run `steps` steps of every bucket; returns device milliseconds."""
-        for b in self.buckets.values():
-            b.rebuild_lists()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        key = tuple((k, tuple(s.req.rid for s in b.systems)) for k, b in self.buckets.items()) + (steps,)
+    def _segment(self, steps: int) -> tuple[float, float]:
+        """Run `steps` steps of every bucket: the Verlet lists, then one graph
+        replay. Returns (device ms of the replay, wall ms of lists + replay). The
+        graph is captured again only when a bucket's buffers were reallocated."""
+        key = tuple(b.generation for b in self.buckets.values()) + (steps,)
         if self.use_graphs and key != self._graph_key:
             self._graph = None
+            for b in self.buckets.values():
+                b.rebuild_lists()
             for b in self.buckets.values():   # warm-up launch sets kernel attributes outside capture
-                if b.systems:
-                    snap = [t.clone() for t in (b.pos, b.quat, b.vel, b.angmom, b.th)]
-                    b.step_kernels()
-                    torch.cuda.synchronize()
-                    for t, v in zip((b.pos, b.quat, b.vel, b.angmom, b.th), snap):
-                        t.copy_(v)
+                snap = [t.clone() for t in (b.pos, b.quat, b.vel, b.angmom, b.th)]
+                b.step_kernels()
+                torch.cuda.synchronize()
+                for t, v in zip((b.pos, b.quat, b.vel, b.angmom, b.th), snap):
+                    t.copy_(v)
             g = torch.cuda.CUDAGraph()
             s = torch.cuda.Stream()
             s.wait_stream(torch.cuda.current_stream())
@@ -303,8 +417,13 @@ class Server:
                         for b in self.buckets.values():
                             b.step_kernels()
             torch.cuda.current_stream().wait_stream(s)
+            torch.cuda.synchronize()
             self._graph, self._graph_key = g, key
             self.stats.graphs_captured += 1
+        t0 = time.perf_counter()
+        for b in self.buckets.values():
+            b.rebuild_lists()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         if self.use_graphs:
             self._graph.replay()
@@ -314,7 +433,7 @@ class Server:
                     b.step_kernels()
         ev1.record()
         torch.cuda.synchronize()
-        return ev0.elapsed_time(ev1)
+        return ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3
 
     def run(self, requests: list[Request], keep_states: bool = False) -> ServeStats:
         """Serve `requests` (arrival times in seconds from now) to completion."""
@@ -342,15 +461,14 @@ class Server:
                 admitted.append(sysm)
             if admitted:
                 for name, b in self.buckets.items():
-                    new = [s for s in admitted if s.req.shape == name]
-                    if new:
-                        b.pack(b.systems + new)
+                    b.admit([s for s in admitted if s.req.shape == name])
             if not active:
                 continue
             self.stats.max_active = max(self.stats.max_active, len(active))
             steps = min(self.segment, min(s.req.steps - s.done for s in active))
-            ms = self._segment(steps)
+            ms, wall_ms = self._segment(steps)
             self.stats.segments_ms.append(ms * self.segment / steps)
+            self.stats.segments_wall_ms.append(wall_ms * self.segment / steps)
             self.stats.body_steps += steps * sum(s.req.n for s in active)
             finished = []
             for s in active:
@@ -362,14 +480,13 @@ class Server:
                 for name, b in self.buckets.items():
                     gone = [s for s in b.systems if s in finished]
                     if gone:
-                        states = b._snapshot_states()
+                        states = b.retire(gone)
                         for s in gone:
                             s.finished_at = now
                             self.stats.completions.append((s.req.rid, now - s.req.arrival))
                             if keep_states:
                                 self.results[s.req.rid] = states[s.req.rid]
                             self.used -= s.mem
-                        b.pack([s for s in b.systems if s not in finished])
                 active = [s for s in active if s not in finished]
         self.stats.wall_s = time.perf_counter() - t0
         return self.stats

@@ -298,7 +298,7 @@ __global__ void k_multi_nvt_init(const float *vel, const float *quat, const floa
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double kt = 0.0, kr = 0.0;
     int key = -1 - (int)(threadIdx.x & 31);
-    if (i < n) {
+    if (i < n && rep[i] >= 0) {  // rep < 0: a free body slot
         float v[3] = {vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
         float a[4] = {angmom[4 * i], angmom[4 * i + 1], angmom[4 * i + 2], angmom[4 * i + 3]};
         kt = (double)trans_ke(v, mass[i]);
@@ -314,6 +314,7 @@ __global__ void k_multi_thermo_update(int nrep, const amlp_replica *rp, amlp_nvt
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrep) return;
     const amlp_replica q = rp[r];
+    if (!(q.n_dof > 0.f)) return;  // a free system slot
     thermo_update(p.dt, p.tau, q.kT, q.n_dof, q.rn_dof, q.nve, th + r);
     th[r].ke_t = 0.0;
     th[r].ke_r = 0.0;
@@ -323,7 +324,7 @@ __global__ void k_multi_step_two(float *vel, float *accel, const float *F, const
                                  const float *T, float *angmom, float *dp, const int *rep, int n, amlp_nvt p,
                                  const amlp_thermostat *th) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || rep[i] < 0) return;  // rep < 0: a free body slot
     const amlp_thermostat *t = th + rep[i];
     step_two_body(i, vel, accel, F, mass, quat, T, angmom, dp, p.dt, t->thermo_fac, t->xi_rot);
 }
@@ -336,7 +337,7 @@ __global__ void __launch_bounds__(kIntThreads) k_multi_step_one(float *pos, floa
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double kt = 0.0, kr = 0.0;
     int key = -1 - (int)(threadIdx.x & 31);
-    if (i < n) {
+    if (i < n && rep[i] >= 0) {  // rep < 0: a free body slot
         key = rep[i];
         const amlp_thermostat *t = th + key;
         step_one_body(i, pos, vel, accel, quat, angmom, dp, mass, p.dt, t->thermo_fac, t->xi_rot, rp[key].box, p.moi,

@@ -64,7 +64,15 @@ WORKLOADS = {
     "cube1000": dict(n=1000, shape="cube26", phi=0.30, seed=0, widths=(64, 64), act="tanh", net="xavier"),
     "tetra16": dict(n=65536, shape="tetra16", phi=0.40, seed=2, widths=(128, 128, 128), act="silu", net="trained"),
     "cyl24": dict(n=262144, shape="cyl24", phi=0.35, seed=3, widths=(128, 128), act="silu", net="trained"),
+    # the reference's own trained models (TheEnergyNet(150, 3, D), ReLU) on its th_v1 tetrahedra, at the
+    # number density of its init files (200 bodies in a box of 33) and its temperature kT 0.5
+    "th_C104": dict(n=262144, shape="th_v1", L=33.0 * (262144 / 200) ** (1 / 3), seed=4, widths=(150,) * 4,
+                    act="relu", net="model_th_C104", hypers=(10, 8, 4), kT=0.5),
+    "th_C100": dict(n=262144, shape="th_v1", L=33.0 * (262144 / 200) ** (1 / 3), seed=4, widths=(150,) * 4,
+                    act="relu", net="model_th_C100", hypers=(10, 10, 10), kT=0.5),
 }
+HYPERS = (10, 8, 4)
+BOX = None  # explicit box edge (workloads at a given number density instead of a packing fraction)
 
 # kernels launched by each libamlp entry point (for the gpu_launches count)
 LAUNCHES = {"amlp_nlist_build": 11, "amlp_pair_filter": 2, "amlp_forces_fd": 1, "amlp_forces_adjoint": 1,
@@ -84,18 +92,32 @@ DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.141824e6 + 350.520064e6 + 79.480064e6 +
                                        + 5.303552e6) / 381342
 
 
-def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS):
+def descriptor_flops(nd: int, hypers=(10, 8, 4), adjoint: bool = False) -> float:
+    """Algorithmic FLOPs of one descriptor evaluation of an Nd-point cloud.
+    Spherical-harmonic form (the plain path, and the adjoint path for (10, 8, 4)):
+    per point the 2 (nang+1) K contraction over K = lmax (lmax + 2) harmonics plus
+    their recurrences and the radial basis, 573 Nd + 432 for (10, 8, 4) and
+    3,050 Nd + 250 for (10, 10, 10). Direct form (the adjoint path for (10, 10,
+    10)): per point pair the Legendre recurrences and (nang+1) lmax
+    multiply-adds, 246 Nd^2 + 60 Nd."""
+    if tuple(hypers) == (10, 8, 4):
+        return 573.0 * nd + 432.0
+    if adjoint:
+        return 246.0 * nd * nd + 60.0 * nd
+    return 3050.0 * nd + 250.0
+
+
+def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WIDTHS, hypers=(10, 8, 4)):
     """Algorithmic FLOPs per filtered pair as (FP32 SIMT part, tensor-core part):
-    descriptor F_d = 573 Nd + 432 per cloud evaluation (spherical-harmonic form),
-    net F_n = 2 (sum of layer in x out). The plain method evaluates 10 clouds and
-    10 nets per pair, all in FP32 SIMT; the adjoint one cloud + its backward
-    (3 F_d, FP32 SIMT) and the net forward + backward (2 F_n) on the tensor cores."""
+    descriptor F_d per cloud evaluation (descriptor_flops), net F_n = 2 (sum of
+    layer in x out). The plain methods evaluate 10 clouds and 10 nets per pair,
+    all in FP32 SIMT; the adjoint one cloud + its backward (3 F_d, FP32 SIMT) and
+    the net forward + backward (2 F_n) on the tensor cores."""
     dims = [D] + list(widths) + [1]
     fn = 2.0 * sum(dims[k] * dims[k + 1] for k in range(len(dims) - 1))
-    fd = 573.0 * nd + 432.0
-    if method == "fd":
-        return 10.0 * (fd + fn), 0.0
-    return 3.0 * fd, 2.0 * fn
+    if method in ("fd", "fd_split"):
+        return 10.0 * (descriptor_flops(nd, hypers) + fn), 0.0
+    return 3.0 * descriptor_flops(nd, hypers, adjoint=True), 2.0 * fn
 
 
 class ClockSampler:
@@ -296,7 +318,7 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
     launches = [0]
     entry = "amlp_forces_" + ("fd" if method == "fd" else "adjoint")
-    wide = method != "fd" and system.adj_ws is not None  # nets wider than 64: the three-kernel adjoint
+    wide = method == "adjoint" and system.adj_ws is not None  # beyond the fused kernel: the wide adjoint
     if wide:
         entry = "amlp_forces_adjoint_wide"
 
@@ -324,14 +346,17 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
                 system.F.data_ptr(), system.T.data_ptr(), system._pe_ptr()]
         if wide:
             args += [system.adj_ws.data_ptr(), system.adj_ws.numel()]
-        _lib.call(entry, *args, stream.cuda_stream)
+        if method == "fd_split":  # the reference's data flow: g_all and e_all in HBM, one pair-count read
+            system._forces_split()
+        else:
+            _lib.call(entry, *args, stream.cuda_stream)
         if ev_force is not None:
             ev_force[1].record(stream)
         system.integrate_step_two()
         system.integrate_step_one()
         system.timestep += 1
-        launches[0] += (LAUNCHES["amlp_pair_filter"] + (4 if wide else 1) + LAUNCHES["amlp_nvt_step_two"] +
-                        LAUNCHES["amlp_nvt_step_one"])
+        launches[0] += (LAUNCHES["amlp_pair_filter"] + (4 if wide else 3 if method == "fd_split" else 1) +
+                        LAUNCHES["amlp_nvt_step_two"] + LAUNCHES["amlp_nvt_step_one"])
 
     for _ in range(warmup):
         one_step()
@@ -404,7 +429,7 @@ def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) 
     srv = Server(nets, hbm_budget=24 << 30, segment=100, device=dev)
     stats = srv.run(reqs).summary()
     seq_reqs = reqs
-    seq_steps = 20
+    seq_steps = steps  # the same steps per request as served
     body_steps, ms = 0, 0.0
     for r in seq_reqs:
         st = make_state(r.n, r.shape, r.phi, kT=r.kT, seed=r.seed)
@@ -422,6 +447,8 @@ def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) 
     seq_rate = body_steps / (ms / 1e3)
     return {"value": stats["particle_steps_per_s"], "unit": "particle-steps/s",
             "segment_ms_p50": stats["segment_ms_p50"], "segment_ms_p99": stats["segment_ms_p99"],
+            "segment_wall_ms_p50": stats["segment_wall_ms_p50"], "segment_wall_ms_p99": stats["segment_wall_ms_p99"],
+            "segment_ms_note": "per 100-step segment: device time of the graph replay; wall: Verlet lists + replay",
             "request_latency_s_p50": stats["request_latency_s_p50"],
             "request_latency_s_p99": stats["request_latency_s_p99"],
             "max_concurrent": stats["max_concurrent"], "requests": stats["requests"],
@@ -440,8 +467,9 @@ def make_net(dev):
     shape's trained soft-repulsion net."""
     import numpy as np
     from amlp.engine import EnergyNet
-    if NET == "trained":
-        z = np.load(os.path.join(REPO, "tests", "golden", f"model_{SHAPE}_soft.npz"))
+    if NET == "trained" or NET.startswith("model_"):
+        name = NET if NET.startswith("model_") else f"model_{SHAPE}_soft"
+        z = np.load(os.path.join(REPO, "tests", "golden", f"{name}.npz"))
         return EnergyNet([(z[f"W{k}"], z[f"b{k}"]) for k in range(len(z.files) // 2)], ACT, dev)
     net = EnergyNet.xavier(47, WIDTHS, ACT, seed=SEED, device="cpu")
     layers = list(net.layers)
@@ -463,18 +491,20 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    state = make_state(N_BODIES, SHAPE, PHI, kT=KT, seed=SEED)
+    state = make_state(N_BODIES, SHAPE, PHI if PHI else 0.1, kT=KT, seed=SEED, L=BOX)
     net = make_net(dev)
     methods = ["adjoint", "fd"] if args.method == "both" else [args.method]
-    if max(WIDTHS) > 64:
-        methods = ["adjoint"]  # the fused plain kernel takes widths up to 64
+    if max(WIDTHS) > 64 or HYPERS != (10, 8, 4):
+        # the fused plain kernel takes widths up to 64 and D = 47: the plain arm is the reference's
+        # own data flow (descriptors, net, differences as three kernels), where one is asked for
+        methods = ["adjoint", "fd_split"] if args.method == "both" and NET.startswith("model_") else ["adjoint"]
     peaks = measured_peaks()
     clk_mhz = peaks["sm_max_mhz"] or 1965.0
     fp32_peak = 148 * 128 * 2 * clk_mhz * 1e6 / 1e12
     results = {}
     clocks = ClockSampler(local_rank)
     for m in methods:
-        system = System(state, SHAPE, Hypers(), net, kT=KT, dt=DT, device=dev)
+        system = System(state, SHAPE, Hypers(*HYPERS), net, kT=KT, dt=DT, device=dev)
         r = _measure(system, m, args.steps, args.warmup, dist, dev)
         e2e_steps = max(3, min(args.steps, 20))
         r["e2e_ms"], r["e2e_bytes"] = _e2e(system, m, e2e_steps, dist, dev)
@@ -487,7 +517,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
     def summary(m):
         r = results[m]
         from amlp.shapes import get_shape
-        fl_pair, tc_pair = algorithmic_flops_per_pair(m, nd=get_shape(SHAPE).nd, widths=WIDTHS)
+        D = (HYPERS[0] + 1) + (HYPERS[1] + 1) * HYPERS[2]
+        fl_pair, tc_pair = algorithmic_flops_per_pair(m, nd=get_shape(SHAPE).nd, D=D, widths=WIDTHS, hypers=HYPERS)
         achieved = fl_pair * r["P"] / (r["force_ms"] / 1e3) / 1e12
         tensor = None
         if tc_pair:
@@ -495,11 +526,18 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
             tensor = {"algorithmic_tflops": tc_alg, "executed_tflops": 3.0 * tc_alg,
                       "peak": peaks["bf16_tflops"], "frac_executed": 3.0 * tc_alg / peaks["bf16_tflops"],
                       "note": "net on the tensor cores as three bf16 products per multiply-add (bf16x3)"}
+        wide = m == "adjoint" and (max(WIDTHS) > 64 or HYPERS != (10, 8, 4))
+        kernel = {"fd": "k_forces_fd", "fd_split": "k_descriptors + k_mlp + k_fd_scatter"}.get(
+            m, "k_adj_desc x2 + k_mlp_grad" if wide else "k_forces_adjoint")
+        if wide and HYPERS != (10, 8, 4):
+            kernel = "k_desc_direct_fwd + k_mlp_grad + k_desc_direct_bwd"
+        traffic_key = "adjoint_wide" if wide and HYPERS == (10, 8, 4) else m
+        traffic = DRAM_BYTES_PER_PAIR.get(traffic_key)
         return {"value": job_throughput(world, N_BODIES, args.steps, r["total_ms"]), "ms_per_step": r["total_ms"] / args.steps,
                 "roofline": {"bound": "fp32",
-                             "kernel": "k_forces_" + m if max(WIDTHS) <= 64 else "k_adj_desc x2 + k_mlp_grad", "achieved": achieved, "peak": fp32_peak,
+                             "kernel": kernel, "achieved": achieved, "peak": fp32_peak,
                              "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                             "traffic": DRAM_BYTES_PER_PAIR[m if max(WIDTHS) <= 64 else "adjoint_wide"] * r["P"],
+                             "traffic": traffic * r["P"] if traffic else None,
                              "traffic_unit": "bytes per force pass (ncu, scaled by pairs from 32,768 bodies)",
                              "flops_per_pair": fl_pair, "tensor_flops_per_pair": tc_pair, "tensor": tensor,
                              "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
@@ -530,8 +568,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                                   if head == "adjoint" else "FP32 throughout")},
             "roofline": hs["roofline"], "e2e": hs["e2e"], "gpu_launches": hs["gpu_launches"], "clocks": clk}
     if len(methods) > 1:
-        ps = summary("fd")
-        line["plain"] = {"method": "fd", "value": ps["value"], "ms_per_step": ps["ms_per_step"],
+        ps = summary(methods[1])
+        line["plain"] = {"method": methods[1], "value": ps["value"], "ms_per_step": ps["ms_per_step"],
                          "roofline": ps["roofline"], "e2e": ps["e2e"]}
         line["tuned_over_plain"] = hs["value"] / ps["value"]
         line["gpu_launches"] += ps["gpu_launches"]
@@ -656,10 +694,14 @@ def main():
     if args.workload != "cube26":
         w = WORKLOADS[args.workload]
         g = globals()
-        g.update(N_BODIES=w["n"], SHAPE=w["shape"], PHI=w["phi"], SEED=w["seed"], WIDTHS=w["widths"],
-                 ACT=w["act"], NET=w["net"], IS_BENCHMARK=False)
-        g["WORKLOAD"] = (f"nvt-step-{w['n']}-{w['shape']}-phi{w['phi']:.2f}-mlp47x" +
-                         "x".join(str(x) for x in w["widths"]) + f"x1-{w['act']}")
+        g.update(N_BODIES=w["n"], SHAPE=w["shape"], PHI=w.get("phi"), SEED=w["seed"], WIDTHS=w["widths"],
+                 ACT=w["act"], NET=w["net"], IS_BENCHMARK=False, HYPERS=w.get("hypers", (10, 8, 4)),
+                 BOX=w.get("L"), KT=w.get("kT", 1.0))
+        D = (HYPERS[0] + 1) + (HYPERS[1] + 1) * HYPERS[2]
+        dens = f"phi{w['phi']:.2f}" if w.get("phi") else f"L{w['L']:.1f}"
+        g["WORKLOAD"] = (f"nvt-step-{w['n']}-{w['shape']}-{dens}-mlp{D}x" +
+                         "x".join(str(x) for x in w["widths"]) + f"x1-{w['act']}" +
+                         (f"-{w['net']}" if w["net"].startswith("model_") else ""))
         if args.bodies == 131072:
             args.bodies = w["n"]
     if args.drift:

@@ -108,7 +108,11 @@ typedef struct amlp_nvt {
 } amlp_nvt;
 
 /* One system of a multi-system launch (serving): systems own contiguous body
- * ranges; the per-body int32 array `rep` gives each body's system. */
+ * ranges; the per-body int32 array `rep` gives each body's system. A body with
+ * rep < 0 is a free slot that every multi-system kernel skips, and a system
+ * with n_dof = 0 is a free system slot (its thermostat is left alone), so that
+ * buffers of a fixed capacity (and CUDA graphs over them) can serve a changing
+ * set of systems. */
 typedef struct amlp_replica {
     float kT, n_dof, rn_dof, box;
     int nve;
