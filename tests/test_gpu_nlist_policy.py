@@ -76,14 +76,19 @@ def test_same_trajectory_as_rebuilding_every_step():
 
 
 def test_cold_system_does_not_rebuild():
+    """Over 300 steps the float atomics' summation order alone lets two runs of
+    the same system drift apart; the displacement policy's trajectory may differ
+    from the fixed schedule's by no more than 10x that drift (plus 1e-5 of the scale)."""
     a = _system(0.01, "displacement")
     b = _system(0.01, "every", every=100)
-    a.run(300, "adjoint")
-    b.run(300, "adjoint")
+    c = _system(0.01, "every", every=100)
+    for s in (a, b, c):
+        s.run(300, "adjoint")
     torch.cuda.synchronize()
     assert a.rebuilds < 2
-    x, y = a.pos.cpu().numpy(), b.pos.cpu().numpy()
-    assert np.abs(x - y).max() <= 1e-4 * max(1.0, np.abs(y).max())
+    x, y, z = (s.pos.cpu().numpy() for s in (a, b, c))
+    floor = np.abs(z - y).max()
+    assert np.abs(x - y).max() <= 10 * floor + 1e-5 * max(1.0, np.abs(y).max())
 
 
 def test_overflowing_rebuild_reruns_with_a_larger_list():
