@@ -120,8 +120,10 @@ class Halo:
     test can pass the messages of several ranks by hand in one process."""
 
     def __init__(self, slab: Slab, width: float):
-        if slab.world > 1 and slab.L / slab.world < width:
-            raise ValueError(f"slabs of {slab.L / slab.world:.3g} are thinner than the halo of {width:.3g}")
+        # a body within the halo width of both boundaries would reach a two-rank
+        # neighbour twice, and a halo wider than a slab would need the slab beyond it
+        if slab.world > 1 and slab.L / slab.world < 2.0 * width:
+            raise ValueError(f"slabs of {slab.L / slab.world:.3g} are thinner than twice the halo of {width:.3g}")
         self.slab, self.width = slab, float(width)
         self.to_lower = self.to_upper = None
         self.n_from_upper = self.n_from_lower = 0
@@ -180,3 +182,185 @@ def migrate(comm: Comm, slab: Slab, owned: dict) -> dict:
     return {"pos": new[:, 0:3].float().contiguous(), "quat": new[:, 3:7].float().contiguous(),
             "vel": new[:, 7:10].float().contiguous(), "angmom": new[:, 10:14].float().contiguous(),
             "mass": new[:, 14].float().contiguous(), "ids": new[:, 15].round().long()}
+
+
+class OwnedForces:
+    """Forces and torques on the owned bodies from owned + halo bodies through
+    the library's kernels. At a rebuild the Verlet list of owned + halo bodies
+    is cut to its pairs with an owned first body (the prefix i < n_owned of the
+    (i, j)-sorted list) and split into owned-owned pairs and pairs with a halo
+    body; each step filters both and runs the force kernel on each. The pair
+    energy sums each owned-owned pair once and each cross pair with weight
+    1/2, so that the ranks' sums add up to the system's."""
+
+    def __init__(self, shape, hypers, net, L: float, device, method: str = "adjoint", skin: float = 2.0):
+        import ctypes
+        from ._lib import Nep
+        self.ctypes = ctypes
+        self.shape, self.hypers, self.net, self.L = shape, hypers, net, float(np.float32(L))
+        self.device, self.method = torch.device(device), method
+        self.r = float(shape.cutoff) + float(skin)
+        self.pts = torch.tensor(shape.pts, dtype=torch.float32, device=self.device)
+        n = Nep()
+        n.nrad, n.nang, n.lmax = hypers.nrad, hypers.nang, hypers.lmax
+        n.npts, n.d_pts = shape.npts, self.pts.data_ptr()
+        n.cutoff, n.nep_cutoff = float(shape.cutoff), float(shape.nep_cutoff)
+        n.en_min, n.en_max, n.dx, n.dteta = float(shape.en_min), float(shape.en_max), 1e-5, 1e-5
+        self.nep = n
+        self.lists = []
+        self.pe = torch.zeros(2, dtype=torch.float64, device=self.device)
+
+    def _stream(self):
+        return torch.cuda.current_stream().cuda_stream
+
+    def rebuild(self, ext_pos: torch.Tensor, n_owned: int) -> None:
+        from ._lib import call, size_query
+        n = int(ext_pos.shape[0])
+        ws = torch.empty(size_query("amlp_nlist_workspace_bytes", n, self.L, self.r), dtype=torch.uint8,
+                         device=self.device)
+        cnt = torch.zeros(1, dtype=torch.int64, device=self.device)
+        cap = max(1024, 64 * n)
+        while True:
+            out = torch.empty(cap, 2, dtype=torch.int32, device=self.device)
+            call("amlp_nlist_build", ext_pos.data_ptr(), n, self.L, self.r, out.data_ptr(), cap, cnt.data_ptr(),
+                 ws.data_ptr(), ws.numel(), self._stream())
+            k = int(cnt.item())
+            if k <= cap:
+                break
+            cap = k
+        vl = out[:k]
+        vl = vl[vl[:, 0] < n_owned]                       # a pair of two halo bodies is another rank's
+        cross = vl[:, 1] >= n_owned
+        self.lists = []
+        for part in (vl[~cross], vl[cross]):
+            part = part.contiguous()
+            m = max(1, int(part.shape[0]))
+            self.lists.append(dict(
+                v=part if part.shape[0] else torch.zeros(1, 2, dtype=torch.int32, device=self.device),
+                nv=torch.tensor([int(part.shape[0])], dtype=torch.int64, device=self.device),
+                f=torch.empty(m, 2, dtype=torch.int32, device=self.device),
+                nf=torch.zeros(1, dtype=torch.int64, device=self.device), cap=m,
+                ws=torch.empty(max(1, size_query("amlp_filter_workspace_bytes", m)), dtype=torch.uint8,
+                               device=self.device),
+                adj=(torch.empty(size_query("amlp_adjoint_workspace_bytes", m), dtype=torch.uint8,
+                                 device=self.device)
+                     if self.method == "adjoint" and (self.net.max_hidden > 64 or self.hypers.D > 48) else None)))
+
+    def forces(self, ext_pos: torch.Tensor, ext_quat: torch.Tensor, n_owned: int):
+        """(F, T) of the owned bodies, and this rank's share of the pair energy."""
+        from ._lib import call
+        c = self.ctypes
+        n = int(ext_pos.shape[0])
+        F = torch.zeros(n, 3, dtype=torch.float32, device=self.device)
+        T = torch.zeros(n, 3, dtype=torch.float32, device=self.device)
+        self.pe.zero_()
+        st = self._stream()
+        for k, lst in enumerate(self.lists):
+            call("amlp_pair_filter", ext_pos.data_ptr(), self.L, float(self.shape.cutoff), lst["v"].data_ptr(),
+                 lst["nv"].data_ptr(), lst["cap"], lst["f"].data_ptr(), lst["nf"].data_ptr(), lst["ws"].data_ptr(),
+                 lst["ws"].numel(), st)
+            args = [ext_pos.data_ptr(), ext_quat.data_ptr(), self.L, lst["f"].data_ptr(), lst["nf"].data_ptr(),
+                    lst["cap"], c.byref(self.nep), c.byref(self.net.struct), F.data_ptr(), T.data_ptr(),
+                    self.pe[k:k + 1].data_ptr()]
+            if self.method == "fd":
+                call("amlp_forces_fd", *args, st)
+            elif lst["adj"] is None:
+                call("amlp_forces_adjoint", *args, st)
+            else:
+                call("amlp_forces_adjoint_wide", *args, lst["adj"].data_ptr(), lst["adj"].numel(), st)
+        return F[:n_owned], T[:n_owned], self.pe[0] + 0.5 * self.pe[1]
+
+
+class DomainSystem:
+    """One rank's part of a periodic system decomposed into slabs (see the module
+    docstring): owned bodies, halo exchange, forces, the NVT halves of the owned
+    bodies and the global thermostat. Every rank calls ``step`` in lockstep."""
+
+    def __init__(self, comm: Comm, state, shape, hypers, net, kT: float, dt: float, device, method: str = "adjoint",
+                 nlist_every: int = 100, skin: float = 2.0):
+        import ctypes
+        from ._lib import Nvt, Thermostat, call, size_query
+        from .engine import THERMOSTAT_SEED
+        self.ctypes, self.call, self.size_query, self.Thermostat = ctypes, call, size_query, Thermostat
+        self.comm, self.device = comm, torch.device(device)
+        self.L = float(np.float32(state.L))
+        self.slab = Slab(self.L, comm.world, comm.rank)
+        self.halo = Halo(self.slab, float(shape.cutoff) + float(skin))
+        self.forces_of = OwnedForces(shape, hypers, net, self.L, device, method, skin)
+        self.nlist_every, self.timestep, self.N = int(nlist_every), 0, int(state.N)
+        mine = np.nonzero(self.slab.owner(np.asarray(state.pos)[:, 0]) == comm.rank)[0]
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.owned = {"pos": torch.tensor(np.asarray(state.pos)[mine], **f32),
+                      "quat": torch.tensor(np.asarray(state.orient)[mine], **f32),
+                      "vel": torch.tensor(np.asarray(state.vel)[mine], **f32),
+                      "angmom": torch.tensor(np.asarray(state.angmom)[mine], **f32),
+                      "mass": torch.tensor(np.asarray(state.mass)[mine], **f32),
+                      "ids": torch.tensor(mine, dtype=torch.long, device=self.device)}
+        self.nvt = Nvt()
+        self.nvt.dt, self.nvt.tau, self.nvt.kT = float(dt), float(np.float32(100.0 * dt)), float(kT)
+        self.nvt.n_dof, self.nvt.rn_dof = float((self.N - 1) * 3), float(3 * self.N)  # the whole system's
+        for k in range(3):
+            self.nvt.moi[k] = float(np.asarray(state.moi).reshape(-1)[k])
+        self.nvt.box, self.nvt.nve = self.L, 0
+        th = Thermostat()
+        th.xi, th.eta, th.xi_rot, th.eta_rot, th.thermo_fac = THERMOSTAT_SEED
+        self.th = torch.frombuffer(bytearray(bytes(th)), dtype=torch.uint8).to(self.device)
+        self.pe = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self._resize()
+        self.call("amlp_nvt_init", self.owned["vel"].data_ptr(), self.owned["quat"].data_ptr(),
+                  self.owned["angmom"].data_ptr(), self.owned["mass"].data_ptr(), self.n, ctypes.byref(self.nvt), 0,
+                  self.th.data_ptr(), self.ws.data_ptr(), self.ws.numel(), self._stream())
+        self._sum_kinetic()
+
+    @property
+    def n(self) -> int:
+        return int(self.owned["pos"].shape[0])
+
+    def _stream(self):
+        return torch.cuda.current_stream().cuda_stream
+
+    def _resize(self) -> None:
+        if self.n <= 0:
+            raise RuntimeError(f"rank {self.comm.rank} owns no body: too many slabs for this system")
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.accel = torch.zeros(self.n, 3, **f32)
+        self.dp = torch.zeros(self.n, 4, **f32)
+        self.ws = torch.empty(self.size_query("amlp_nvt_workspace_bytes", self.n), dtype=torch.uint8,
+                              device=self.device)
+
+    def _sum_kinetic(self) -> None:
+        off = self.Thermostat.ke_t.offset
+        ke = self.th[off:off + 16].view(torch.float64)  # ke_t, ke_r of the owned bodies -> of the system
+        self.comm.sum(ke)
+
+    def step(self) -> None:
+        o, c = self.owned, self.ctypes
+        if self.timestep % self.nlist_every == 0:
+            if self.timestep > 0:
+                self.owned = o = migrate(self.comm, self.slab, o)
+                self._resize()
+            self.halo.choose(o["pos"].cpu().numpy())
+            ext_pos, ext_quat = self.halo.exchange(self.comm, o["pos"], o["quat"])
+            self.forces_of.rebuild(ext_pos, self.n)
+        else:
+            ext_pos, ext_quat = self.halo.exchange(self.comm, o["pos"], o["quat"])
+        F, T, pe = self.forces_of.forces(ext_pos, ext_quat, self.n)
+        self.F, self.T = F, T = F.contiguous(), T.contiguous()  # forces and torques of the owned bodies
+        self.pe.copy_(pe.reshape(1))
+        st = self._stream()
+        self.call("amlp_nvt_step_two", o["vel"].data_ptr(), self.accel.data_ptr(), F.data_ptr(), o["mass"].data_ptr(),
+                  o["quat"].data_ptr(), T.data_ptr(), o["angmom"].data_ptr(), self.dp.data_ptr(), self.n,
+                  c.byref(self.nvt), self.th.data_ptr(), st)
+        self.call("amlp_nvt_step_one", o["pos"].data_ptr(), o["vel"].data_ptr(), self.accel.data_ptr(),
+                  o["quat"].data_ptr(), o["angmom"].data_ptr(), self.dp.data_ptr(), o["mass"].data_ptr(), self.n,
+                  c.byref(self.nvt), self.th.data_ptr(), self.ws.data_ptr(), self.ws.numel(), st)
+        self._sum_kinetic()
+        self.timestep += 1
+
+    def run(self, nsteps: int) -> None:
+        for _ in range(nsteps):
+            self.step()
+
+    def gather(self) -> dict:
+        """The owned bodies' arrays on the host, with their global indices."""
+        return {k: v.detach().cpu().numpy() for k, v in self.owned.items()}
