@@ -19,7 +19,31 @@ amlp_status check_launch() {
     return AMLP_OK;
 }
 
+// FP32 FMA throughput probe: 8 independent multiply-add chains per thread.
+constexpr int kProbeChains = 8;
+__global__ void __launch_bounds__(512) k_fma_probe(float *out, int iters, float mul, float add) {
+    float v[kProbeChains];
+#pragma unroll
+    for (int c = 0; c < kProbeChains; ++c) v[c] = (float)(threadIdx.x + c) * 1e-3f;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int c = 0; c < kProbeChains; ++c) v[c] = fmaf(v[c], mul, add);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < kProbeChains; ++c) s += v[c];
+    if (s == 12345.678f) out[0] = s;  // never true for these inputs; keeps the chains alive
+}
+
 }  // namespace amlp
+
+extern "C" amlp_status amlp_fp32_fma_probe(float *d_out, int iters, double *flops, void *stream) {
+    if (!d_out || iters <= 0 || !flops) return AMLP_ERR_INVALID_ARG;
+    const int blocks = 4 * amlp::kNumSM, threads = 512;
+    amlp::k_fma_probe<<<blocks, threads, 0, amlp::as_stream(stream)>>>(d_out, iters, 0.9999999f, 1e-7f);
+    *flops = 2.0 * amlp::kProbeChains * (double)iters * blocks * threads;
+    return amlp::check_launch();
+}
 
 extern "C" int amlp_version(void) { return 1; }
 

@@ -150,6 +150,27 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def measure_fp32_peak(dev) -> float:
+    """FP32 TFLOP/s of the library's multiply-add probe (amlp_fp32_fma_probe):
+    best of three ~0.1 s launches, CUDA events on the launching stream."""
+    import ctypes
+    import torch
+    from amlp import _lib
+    out = torch.zeros(1, device=dev)
+    stream = torch.cuda.current_stream()
+    flops = ctypes.c_double(0.0)
+    best = 0.0
+    _lib.call("amlp_fp32_fma_probe", out.data_ptr(), 20000, ctypes.byref(flops), stream.cuda_stream)  # warm-up
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.call("amlp_fp32_fma_probe", out.data_ptr(), 1500000, ctypes.byref(flops), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = max(best, flops.value / (e0.elapsed_time(e1) / 1e3) / 1e12)
+    return best
+
+
 def measured_peaks() -> dict:
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -500,7 +521,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         methods = ["adjoint", "fd_split"] if args.method == "both" and NET.startswith("model_") else ["adjoint"]
     peaks = measured_peaks()
     clk_mhz = peaks["sm_max_mhz"] or 1965.0
-    fp32_peak = 148 * 128 * 2 * clk_mhz * 1e6 / 1e12
+    fp32_nominal = 148 * 128 * 2 * clk_mhz * 1e6 / 1e12
+    fp32_peak = measure_fp32_peak(dev)  # the denominator: measured here, not the nominal figure
     results = {}
     clocks = ClockSampler(local_rank)
     for m in methods:
@@ -537,14 +559,16 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                 "roofline": {"bound": "fp32",
                              "kernel": kernel, "achieved": achieved, "peak": fp32_peak,
                              "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                             "peak_nominal": fp32_nominal, "frac_of_nominal": achieved / fp32_nominal,
                              "traffic": traffic * r["P"] if traffic else None,
                              "traffic_unit": "bytes per force pass (ncu, scaled by pairs from 32,768 bodies)",
                              "flops_per_pair": fl_pair, "tensor_flops_per_pair": tc_pair, "tensor": tensor,
                              "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
                              "force_share_of_step": r["force_share"],
-                             "peak_source": f"nominal FP32 SIMT 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz (no measured "
-                                            f"FP32 peak; HBM {peaks['hbm_gbs']} GB/s, bf16 {peaks['bf16_tflops']} TFLOP/s "
-                                            f"{peaks['source']})",
+                             "peak_source": (f"measured FP32 FMA throughput of amlp_fp32_fma_probe in this run (best of 3, "
+                                             f"CUDA events); nominal 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz beside it; "
+                                             f"HBM {peaks['hbm_gbs']} GB/s, bf16 {peaks['bf16_tflops']} TFLOP/s "
+                                             f"{peaks['source']}"),
                              "work": ("achieved counts the FP32 SIMT work only (descriptor forward and backward); "
                                       "the net's tensor-core work is reported under 'tensor'") if tc_pair else
                                      "achieved counts all the work (descriptors and net, FP32 SIMT)"},

@@ -123,6 +123,13 @@ typedef struct amlp_replica {
 int amlp_version(void);
 const char *amlp_status_string(amlp_status s);
 const char *amlp_last_cuda_error(void);
+/* Measurement utility (no reference counterpart): launches a kernel of
+ * independent FP32 multiply-add chains on every SM and returns in *flops the
+ * floating-point operations it performs (2 per multiply-add), for timing with
+ * events around it on the same stream: the measured FP32 peak that the FP32
+ * roofline of the force kernels divides by. d_out: one float, never written in
+ * practice. */
+amlp_status amlp_fp32_fma_probe(float *d_out, int iters, double *flops, void *stream);
 
 /* --------------------------------------------------------------- Verlet list
  * All pairs i < j with |x_i - x_j|_periodic <= r, computed exactly as scipy's
