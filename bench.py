@@ -437,9 +437,10 @@ def _e2e(system, method, steps, dist, dev):
     return ms, nbytes
 
 
-def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) -> dict:
+def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0, seq_requests: int = 0) -> dict:
     """Mixed request stream served by continuous batching, and the same requests
-    run one after another with the plain FP32 method (a subsample, timed)."""
+    run one after another with the plain FP32 method for the same number of
+    steps each (all of them, or the first `seq_requests` of the stream)."""
     import torch
     from amlp.configs import make_state
     from amlp.engine import EnergyNet, Hypers, System
@@ -449,7 +450,7 @@ def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) 
     reqs = request_stream(n_requests, seed=SEED, steps=steps, rate=rate)
     srv = Server(nets, hbm_budget=24 << 30, segment=100, device=dev)
     stats = srv.run(reqs).summary()
-    seq_reqs = reqs
+    seq_reqs = reqs[:seq_requests] if 0 < seq_requests < len(reqs) else reqs
     seq_steps = steps  # the same steps per request as served
     body_steps, ms = 0, 0.0
     for r in seq_reqs:
@@ -478,8 +479,9 @@ def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0) 
                       f"[500, 50000], shape uniform {{cube26, tetra16, cyl24}}, phi U[0.25, 0.45], kT U[0.5, 2.0], "
                       f"seed {SEED}; adjoint forces, bf16x3 tensor-core net, 100-step segments, 24 GiB budget",
             "sequential_plain": {"value": seq_rate, "unit": "particle-steps/s",
-                                 "sample": f"all {len(seq_reqs)} requests x {seq_steps} steps, one after "
-                                           f"another, plain FP32 finite differences, CUDA graphs"},
+                                 "sample": (f"{'all ' if len(seq_reqs) == len(reqs) else 'the first '}"
+                                            f"{len(seq_reqs)} requests x {seq_steps} steps, one after "
+                                            f"another, plain FP32 finite differences, CUDA graphs")},
             "served_over_sequential_plain": stats["particle_steps_per_s"] / seq_rate}
 
 
@@ -598,7 +600,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
         line["tuned_over_plain"] = hs["value"] / ps["value"]
         line["gpu_launches"] += ps["gpu_launches"]
     if rank == 0 and world == 1 and not args.no_serving and IS_BENCHMARK:
-        line["serving"] = run_serving(dev, args.serving_requests, args.serving_steps, args.serving_rate)
+        line["serving"] = run_serving(dev, args.serving_requests, args.serving_steps, args.serving_rate,
+                                      args.serving_seq_requests)
     if rank == 0 and not args.no_cpu_baseline and world == 1 and SHAPE == "cube26":
         line["cpu_baseline"] = cpu_step_sample()
     if rank == 0:
@@ -701,6 +704,10 @@ def main():
     ap.add_argument("--serving-steps", type=int, default=300,
                     help="NVT steps per request (2000 in the full serving configuration)")
     ap.add_argument("--serving-rate", type=float, default=8.0, help="Poisson arrival rate, requests per second")
+    ap.add_argument("--serving-seq-requests", type=int, default=0,
+                    help="requests of the stream run one after another with the plain method (0: all)")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="only the serving leg (one JSON line with its results)")
     ap.add_argument("--bodies", type=int, default=N_BODIES,
                     help="system size (the benchmark workload is 131072; smaller sizes are for profiling)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cube26",
@@ -739,6 +746,13 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", args.gpus))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.serving_only:
+        import torch
+        dev = torch.device("cuda", local_rank)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"metric": "served particle-steps/s", "serving": run_serving(
+            dev, args.serving_requests, args.serving_steps, args.serving_rate, args.serving_seq_requests)}))
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
     else:
