@@ -740,6 +740,8 @@ def main():
         return
     if args.bodies != N_BODIES:
         globals()["WORKLOAD"] = WORKLOAD.replace(str(N_BODIES), str(args.bodies))
+        if BOX:  # the same number density
+            globals()["BOX"] = BOX * (args.bodies / N_BODIES) ** (1.0 / 3.0)
         globals()["N_BODIES"] = args.bodies
     if args.warmup < 3:
         args.warmup = 3
