@@ -13,9 +13,10 @@ lies in its slab and, every step:
    indices stay valid; in between only the coordinates travel;
 2. evaluates the pair forces of every pair with at least one owned body over
    owned + halo bodies (owned bodies first, so that these pairs are the prefix
-   of the (i, j)-sorted Verlet list with i < n_owned) and keeps the forces and
-   torques of its owned bodies. A pair across a boundary is evaluated on both
-   sides ("Newton off"), which needs no reverse exchange of forces;
+   of the (i, j)-sorted Verlet list with i < n_owned; each pair then oriented by
+   global index, as in the single domain) and keeps the forces and torques of
+   its owned bodies. A pair across a boundary is evaluated on both sides
+   ("Newton off"), which needs no reverse exchange of forces;
 3. integrates its owned bodies; the thermostat, which needs the kinetic
    energies of the whole system, takes one all-reduce of two numbers.
 
@@ -188,8 +189,10 @@ class OwnedForces:
     """Forces and torques on the owned bodies from owned + halo bodies through
     the library's kernels. At a rebuild the Verlet list of owned + halo bodies
     is cut to its pairs with an owned first body (the prefix i < n_owned of the
-    (i, j)-sorted list) and split into owned-owned pairs and pairs with a halo
-    body; each step filters both and runs the force kernel on each. The pair
+    (i, j)-sorted list), each pair is oriented by global index as in the single
+    domain (the roles of the two bodies enter the rounding of a pair's forces),
+    and the list is split into owned-owned pairs and pairs with a halo body;
+    each step filters both and runs the force kernel on each. The pair
     energy sums each owned-owned pair once and each cross pair with weight
     1/2, so that the ranks' sums add up to the system's."""
 
@@ -213,7 +216,11 @@ class OwnedForces:
     def _stream(self):
         return torch.cuda.current_stream().cuda_stream
 
-    def rebuild(self, ext_pos: torch.Tensor, n_owned: int) -> None:
+    def rebuild(self, ext_pos: torch.Tensor, n_owned: int, ext_ids: torch.Tensor | None = None) -> None:
+        """Verlet lists of the owned bodies' pairs. With the global indices of
+        owned + halo bodies (`ext_ids`), every pair is oriented as in the single
+        domain (first body = smaller global index), so that each pair's forces
+        are computed with the same arithmetic as there."""
         from ._lib import call, size_query
         n = int(ext_pos.shape[0])
         ws = torch.empty(size_query("amlp_nlist_workspace_bytes", n, self.L, self.r), dtype=torch.uint8,
@@ -230,7 +237,13 @@ class OwnedForces:
             cap = k
         vl = out[:k]
         vl = vl[vl[:, 0] < n_owned]                       # a pair of two halo bodies is another rank's
-        cross = vl[:, 1] >= n_owned
+        if ext_ids is not None and vl.shape[0]:
+            g = ext_ids.to(self.device)[vl.long()]
+            swap = g[:, 0] > g[:, 1]
+            vl = torch.where(swap[:, None], vl.flip(1), vl)
+            key = vl[:, 0].long() * n + vl[:, 1].long()  # sorted by first body: the scatters merge per body
+            vl = vl[torch.argsort(key)].contiguous()
+        cross = (vl[:, 0] >= n_owned) | (vl[:, 1] >= n_owned)
         self.lists = []
         for part in (vl[~cross], vl[cross]):
             part = part.contiguous()
@@ -341,7 +354,11 @@ class DomainSystem:
                 self._resize()
             self.halo.choose(o["pos"].cpu().numpy())
             ext_pos, ext_quat = self.halo.exchange(self.comm, o["pos"], o["quat"])
-            self.forces_of.rebuild(ext_pos, self.n)
+            ids = o["ids"]
+            lo = torch.as_tensor(self.halo.to_lower, device=ids.device, dtype=torch.long)
+            hi = torch.as_tensor(self.halo.to_upper, device=ids.device, dtype=torch.long)
+            from_upper, from_lower = self.comm.shift(ids[lo], ids[hi])  # the halo's global indices
+            self.forces_of.rebuild(ext_pos, self.n, torch.cat([ids, from_upper, from_lower]))
         else:
             ext_pos, ext_quat = self.halo.exchange(self.comm, o["pos"], o["quat"])
         F, T, pe = self.forces_of.forces(ext_pos, ext_quat, self.n)

@@ -161,20 +161,19 @@ __global__ void __launch_bounds__(32 * kWarps) k_desc_direct_fwd(const float *po
             for (int l = 0; l < LM; ++l) acc[n][l] = 0.f;
 #pragma unroll
         for (int n = 0; n < NR; ++n) rad[n] = 0.f;
-        for (int a = lane; a < nd; a += 32) {
-            float fa[NR];
+        for (int a = lane; a < nd; a += 32)
 #pragma unroll
-            for (int n = 0; n < NR; ++n) fa[n] = C.f[a][n], rad[n] += fa[n];
-            const float ax = C.ux[a], ay = C.uy[a], az = C.uz[a];
-            for (int b = 0; b < nd; ++b) {
-                float Pl[LM];
-                legendre<false>(fmaf(ax, C.ux[b], fmaf(ay, C.uy[b], az * C.uz[b])), Pl, nullptr);
+            for (int n = 0; n < NR; ++n) rad[n] += C.f[a][n];
+        // the point pairs (a, b) spread over the lanes: every lane busy even for 8-point clouds
+        for (int ab = lane; ab < nd * nd; ab += 32) {
+            const int a = ab / nd, b = ab - a * nd;
+            float Pl[LM];
+            legendre<false>(fmaf(C.ux[a], C.ux[b], fmaf(C.uy[a], C.uy[b], C.uz[a] * C.uz[b])), Pl, nullptr);
 #pragma unroll
-                for (int n = 0; n < NA; ++n) {
-                    const float ff = fa[n] * C.f[b][n];
+            for (int n = 0; n < NA; ++n) {
+                const float ff = C.f[a][n] * C.f[b][n];
 #pragma unroll
-                    for (int l = 0; l < LM; ++l) acc[n][l] = fmaf(ff, Pl[l], acc[n][l]);
-                }
+                for (int l = 0; l < LM; ++l) acc[n][l] = fmaf(ff, Pl[l], acc[n][l]);
             }
         }
         // warp sums; lane k writes columns k, k + 32, ...
@@ -230,44 +229,9 @@ __global__ void __launch_bounds__(32 * kWarps) k_desc_direct_bwd(const float *po
         // per-lane partial sums over its points: sum_{a in i} G_a, sum_a G_a,
         // sum_{a in i} r_a x G_a, sum_{a in j} r_a x G_a (centred r_a)
         float Si[3] = {0, 0, 0}, Sa[3] = {0, 0, 0}, Xi[3] = {0, 0, 0}, Xj[3] = {0, 0, 0};
-        for (int a = lane; a < nd; a += 32) {
-            float fa[NR], dfa[NR];
-#pragma unroll
-            for (int n = 0; n < NR; ++n) fa[n] = C.f[a][n], dfa[n] = C.df[a][n];
-            const float ax = C.ux[a], ay = C.uy[a], az = C.uz[a], inv_da = 1.0f / C.d[a];
-            float ga = 0.f;  // coefficient of rhat_a
-#pragma unroll
-            for (int n = 0; n < NR; ++n) ga = fmaf(R[n], dfa[n], ga);
-            float gx = 0.f, gy = 0.f, gz = 0.f;  // sum_b beta_ab rhat_b
-            float bsum_c = 0.f;                  // sum_b beta_ab c_ab
-            float asum = 0.f;                    // sum_b alpha_ab
-            for (int b = 0; b < nd; ++b) {
-                const float bx = C.ux[b], by = C.uy[b], bz = C.uz[b];
-                const float c = fmaf(ax, bx, fmaf(ay, by, az * bz));
-                float Pl[LM], dPl[LM];
-                legendre<true>(c, Pl, dPl);
-                float al = 0.f, be = 0.f;
-#pragma unroll
-                for (int n = 0; n < NA; ++n) {
-                    const float fb = C.f[b][n];
-                    float sp = 0.f, sd = 0.f;
-#pragma unroll
-                    for (int l = 0; l < LM; ++l) {
-                        sp = fmaf(G[n][l], Pl[l], sp);
-                        sd = fmaf(G[n][l], dPl[l], sd);
-                    }
-                    al = fmaf(fb * dfa[n], sp, al);
-                    be = fmaf(fb * fa[n], sd, be);
-                }
-                asum += al;
-                if (b != a) {
-                    gx = fmaf(be, bx, gx), gy = fmaf(be, by, gy), gz = fmaf(be, bz, gz);
-                    bsum_c = fmaf(be, c, bsum_c);
-                }
-            }
-            // dE/dr_a = (ga + 2 asum - 2 bsum_c / d_a) rhat_a + 2 (sum_b beta rhat_b) / d_a
-            const float cu = ga + 2.0f * asum - 2.0f * bsum_c * inv_da, cb = 2.0f * inv_da;
-            const float Gx = fmaf(cu, ax, cb * gx), Gy = fmaf(cu, ay, cb * gy), Gz = fmaf(cu, az, cb * gz);
+        // the gradient dE/dr_a is linear in its terms, and so are the sums over a below: the
+        // point pairs (a, b) spread over the lanes, each lane adding the terms of its pairs
+        auto add_grad = [&](int a, float Gx, float Gy, float Gz) {
             const float rx = C.rx[a], ry = C.ry[a], rz = C.rz[a];
             const float cx = ry * Gz - rz * Gy, cy = rz * Gx - rx * Gz, cz = rx * Gy - ry * Gx;
             Sa[0] += Gx, Sa[1] += Gy, Sa[2] += Gz;
@@ -277,6 +241,37 @@ __global__ void __launch_bounds__(32 * kWarps) k_desc_direct_bwd(const float *po
             } else {
                 Xj[0] += cx, Xj[1] += cy, Xj[2] += cz;
             }
+        };
+        for (int a = lane; a < nd; a += 32) {  // radial part: (sum_n R_n f_n'(a)) rhat_a
+            float ga = 0.f;
+#pragma unroll
+            for (int n = 0; n < NR; ++n) ga = fmaf(R[n], C.df[a][n], ga);
+            add_grad(a, ga * C.ux[a], ga * C.uy[a], ga * C.uz[a]);
+        }
+        for (int ab = lane; ab < nd * nd; ab += 32) {
+            const int a = ab / nd, b = ab - a * nd;
+            const float ax = C.ux[a], ay = C.uy[a], az = C.uz[a];
+            const float bx = C.ux[b], by = C.uy[b], bz = C.uz[b];
+            const float c = fmaf(ax, bx, fmaf(ay, by, az * bz));
+            float Pl[LM], dPl[LM];
+            legendre<true>(c, Pl, dPl);
+            float al = 0.f, be = 0.f;
+#pragma unroll
+            for (int n = 0; n < NA; ++n) {
+                const float fb = C.f[b][n];
+                float sp = 0.f, sd = 0.f;
+#pragma unroll
+                for (int l = 0; l < LM; ++l) {
+                    sp = fmaf(G[n][l], Pl[l], sp);
+                    sd = fmaf(G[n][l], dPl[l], sd);
+                }
+                al = fmaf(fb * C.df[a][n], sp, al);
+                be = fmaf(fb * C.f[a][n], sd, be);
+            }
+            // 2 alpha_ab rhat_a + 2 beta_ab (rhat_b - c_ab rhat_a) / d_a (no beta term for b = a)
+            const float wb = b != a ? 2.0f * be / C.d[a] : 0.f;
+            const float cu = fmaf(-wb, c, 2.0f * al);
+            add_grad(a, fmaf(cu, ax, wb * bx), fmaf(cu, ay, wb * by), fmaf(cu, az, wb * bz));
         }
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
