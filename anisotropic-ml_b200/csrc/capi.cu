@@ -56,6 +56,7 @@ extern "C" const char *amlp_status_string(amlp_status s) {
         case AMLP_ERR_CUDA: return "CUDA error";
         case AMLP_ERR_CAPACITY: return "output capacity too small";
         case AMLP_ERR_TOO_LARGE: return "size beyond the fixed scratch of the allocation-free entry point";
+        case AMLP_ERR_DEVICE_WAIT: return "a bounded device-side wait gave up (see amlp_device_error)";
         default: return "unknown status";
     }
 }

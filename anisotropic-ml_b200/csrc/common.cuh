@@ -11,6 +11,7 @@ constexpr int kNumSM = 148;  // B200; grids are sized in multiples of it
 
 void set_cuda_error(cudaError_t e);
 amlp_status check_launch();
+amlp_status device_wait_status();  // AMLP_ERR_DEVICE_WAIT if a bounded device wait gave up
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 

@@ -1759,6 +1759,14 @@ extern "C" amlp_status amlp_test_first_wait_limit(int polls) {
     return AMLP_OK;
 }
 
+// The sticky flags as a status, for the handles' synchronisation points (reads
+// the flags without clearing them).
+amlp_status amlp::device_wait_status() {
+    unsigned int f = 0;
+    AMLP_CHECK_CUDA(cudaMemcpyFromSymbol(&f, g_amlp_device_error, sizeof(unsigned int)));
+    return f ? AMLP_ERR_DEVICE_WAIT : AMLP_OK;
+}
+
 extern "C" amlp_status amlp_device_error(unsigned int *flags, int clear) {
     if (!flags) return AMLP_ERR_INVALID_ARG;
     AMLP_CHECK_CUDA(cudaMemcpyFromSymbol(flags, g_amlp_device_error, sizeof(unsigned int)));

@@ -468,7 +468,10 @@ extern "C" amlp_status amlp_step(amlp_sim *h, int nsteps, int mode, void *stream
     if (!h->list_valid && (s = h->build_nlist(st))) return s;
     const long long every = h->cfg.nlist_every, end = h->timestep + nsteps;
     while (h->timestep < end) {
-        if (h->timestep % every == 0 && h->timestep > 0 && (s = h->build_nlist(st))) return s;
+        if (h->timestep % every == 0 && h->timestep > 0) {
+            if ((s = h->build_nlist(st))) return s;
+            if ((s = device_wait_status())) return h->fail(s, "a bounded device-side wait gave up");
+        }
         const int seg = (int)std::min(end - h->timestep, every - h->timestep % every);
         if ((s = h->run_segment(mode, seg, st))) return s;
         h->timestep += seg;
@@ -936,7 +939,9 @@ extern "C" amlp_status amlp_pool_step_segment(amlp_pool *p, int nsteps, void *st
     }
     if ((s = p->cuda(cudaGraphLaunch(g->exec, st), "graph launch"))) return s;
     for (auto &x : p->sys) x.steps_done += nsteps;
-    return p->cuda(cudaStreamSynchronize(st), "segment");
+    if ((s = p->cuda(cudaStreamSynchronize(st), "segment"))) return s;
+    if ((s = device_wait_status())) return p->fail(s, "a bounded device-side wait gave up");
+    return AMLP_OK;
 }
 
 extern "C" amlp_status amlp_pool_system_status(amlp_pool *p, int id, int *status, long long *steps_done,

@@ -59,6 +59,7 @@ typedef int amlp_status;
 #define AMLP_ERR_CUDA 4            /* a CUDA call failed (see amlp_last_cuda_error) */
 #define AMLP_ERR_CAPACITY 5        /* output capacity too small (count still written) */
 #define AMLP_ERR_TOO_LARGE 6       /* size beyond the fixed scratch of an allocation-free entry point */
+#define AMLP_ERR_DEVICE_WAIT 7     /* a bounded device-side wait gave up (amlp_device_error; clear it there) */
 
 #define AMLP_ACT_RELU 0
 #define AMLP_ACT_TANH 1
@@ -397,6 +398,9 @@ amlp_status amlp_sim_descriptors(amlp_sim *h, float *d_g, int *d_pairs, long lon
 /* One force pass (filter, forces, torques, pair-energy sum) on the current
  * state; d_F, d_T (N,3) receive copies when not NULL. */
 amlp_status amlp_forces(amlp_sim *h, float *d_F, float *d_T, int mode, void *stream);
+/* Returns AMLP_ERR_DEVICE_WAIT when, at one of its synchronisations (the
+ * Verlet rebuilds), a bounded device-side wait has given up since the flags
+ * were last cleared with amlp_device_error. */
 amlp_status amlp_step(amlp_sim *h, int nsteps, int mode, void *stream);
 /* Any of the outputs may be NULL. */
 amlp_status amlp_get_state(amlp_sim *h, float *d_pos, float *d_quat, float *d_vel, float *d_angmom,
@@ -451,7 +455,8 @@ amlp_status amlp_pool_admit(amlp_pool *p, const amlp_pool_system *sys, int *id);
  * NULL) and its thermostat to *h_th (may be NULL). */
 amlp_status amlp_pool_evict(amlp_pool *p, int id, float *h_pos, float *h_quat, float *h_vel, float *h_angmom,
                             amlp_thermostat *h_th);
-/* nsteps steps of every active system (adjoint forces). Synchronises the stream. */
+/* nsteps steps of every active system (adjoint forces). Synchronises the stream;
+ * AMLP_ERR_DEVICE_WAIT as for amlp_step. */
 amlp_status amlp_pool_step_segment(amlp_pool *p, int nsteps, void *stream);
 amlp_status amlp_pool_system_status(amlp_pool *p, int id, int *status, long long *steps_done,
                                     amlp_thermostat *h_th);

@@ -63,3 +63,26 @@ def test_wait_that_gives_up_is_reported_and_the_next_launch_is_clean():
         assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-3
     fresh.run(3, "adjoint")  # and a graph-captured segment after it
     assert torch.isfinite(fresh.pos).all()
+
+
+def test_simulation_handle_reports_the_wait_as_a_status():
+    """The C ABI's simulation handle checks the flags at its synchronisations
+    (the Verlet rebuilds) and returns AMLP_ERR_DEVICE_WAIT (7)."""
+    from amlp._lib import AmlpError
+    from amlp.native import NativeSystem
+    s, net, _ = _system(7)
+    _lib.device_error(clear=True)
+    nat = NativeSystem(s, "cube26", Hypers(), net, kT=1.0, dt=0.005, device=DEV)
+    _lib.call("amlp_test_first_wait_limit", 0)
+    try:
+        with pytest.raises(AmlpError) as info:
+            nat.run(150, "adjoint")  # a rebuild at step 100
+        assert info.value.status == 7
+    finally:
+        _lib.call("amlp_test_first_wait_limit", -1)
+        torch.cuda.synchronize()
+        _lib.device_error(clear=True)
+    nat.run(50, "adjoint")  # the flags cleared: the handle carries on
+    torch.cuda.synchronize()
+    assert _lib.device_error() == 0
+    nat.close()
