@@ -168,6 +168,83 @@ __global__ void __launch_bounds__(kMlpRows) k_mlp(const float *g, long long rows
     }
 }
 
+// Register-tiled FP32 net for widths up to 160 (the reference's 150-wide models
+// on its own finite-difference data flow): tiles of 64 rows, 256 threads, the
+// activations feature-major in shared memory and one layer's transposed
+// weights beside them (row stride npad + 1, odd, so that the transposing
+// stores do not collide in a bank). Thread t owns rows 4 (t % 16) .. + 3 and
+// columns cw (t / 16) .. + cw - 1 (cw = npad / 16 <= 10): 4 x cw outputs, one
+// 16-byte activation load and cw weight loads per 4 cw multiply-adds.
+constexpr int kTRows = 64, kTThreads = 256, kTMaxW = 160, kTMaxCw = kTMaxW / 16;
+
+__global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long long rows, MlpDesc m, const float *w,
+                                                         float *e_out) {
+    extern __shared__ __align__(16) float smem[];
+    float *A = smem, *B = A + kTMaxW * kTRows;
+    float *WT = B + kTMaxW * kTRows;  // (kmax) x (npad + 1), then the bias
+    const int t = threadIdx.x, rg = t & 15, cg = t >> 4;
+    for (long long r0 = (long long)blockIdx.x * kTRows; r0 < rows; r0 += (long long)gridDim.x * kTRows) {
+        const int D = m.dims[0];
+        for (int idx = t; idx < kTRows * D; idx += kTThreads) {
+            const int rr = idx / D, d = idx - rr * D;
+            A[d * kTRows + rr] = r0 + rr < rows ? g[(r0 + rr) * D + d] : 0.f;
+        }
+        float *X = A, *Y = B;
+        for (int L = 0; L < m.n_layers; ++L) {
+            const int K = m.dims[L], N = m.dims[L + 1];
+            const int npad = (N + 15) / 16 * 16, S = npad + 1, cw = npad / 16;
+            const float *W = w + m.woff[L], *b = W + (size_t)N * K;
+            __syncthreads();  // the previous layer is done with WT
+            for (int idx = t; idx < npad * K; idx += kTThreads) {  // coalesced reads of W (N x K)
+                const int n = idx / K, k = idx - n * K;
+                WT[k * S + n] = n < N ? W[idx] : 0.f;
+            }
+            for (int n = t; n < npad; n += kTThreads) WT[K * S + n] = n < N ? b[n] : 0.f;
+            __syncthreads();
+            const bool last = L == m.n_layers - 1;
+            float acc[4][kTMaxCw];
+#pragma unroll
+            for (int c = 0; c < kTMaxCw; ++c) {
+                const float bc = c < cw ? WT[K * S + cg * cw + c] : 0.f;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) acc[i][c] = bc;
+            }
+            for (int k = 0; k < K; ++k) {
+                const float4 x = *reinterpret_cast<const float4 *>(X + k * kTRows + 4 * rg);
+                const float *wk = WT + k * S + cg * cw;
+#pragma unroll
+                for (int c = 0; c < kTMaxCw; ++c) {
+                    if (c < cw) {
+                        const float wv = wk[c];
+                        acc[0][c] = fmaf(x.x, wv, acc[0][c]);
+                        acc[1][c] = fmaf(x.y, wv, acc[1][c]);
+                        acc[2][c] = fmaf(x.z, wv, acc[2][c]);
+                        acc[3][c] = fmaf(x.w, wv, acc[3][c]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < kTMaxCw; ++c) {
+                if (c < cw) {
+                    float4 o;
+                    o.x = last ? acc[0][c] : act_f(m.act, acc[0][c]);
+                    o.y = last ? acc[1][c] : act_f(m.act, acc[1][c]);
+                    o.z = last ? acc[2][c] : act_f(m.act, acc[2][c]);
+                    o.w = last ? acc[3][c] : act_f(m.act, acc[3][c]);
+                    *reinterpret_cast<float4 *>(Y + (cg * cw + c) * kTRows + 4 * rg) = o;
+                }
+            }
+            float *tmp = X;
+            X = Y;
+            Y = tmp;
+        }
+        __syncthreads();
+        for (int rr = t; rr < kTRows; rr += kTThreads)
+            if (r0 + rr < rows) e_out[r0 + rr] = X[rr];
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------- differences + scatter
 struct FdConst {
     float dx, dteta, en_min, en_range;
@@ -487,6 +564,14 @@ extern "C" amlp_status amlp_mlp_energy(const float *d_g, long long rows, const a
     for (int k = 0; k < mlp->n_layers; ++k) {
         m.woff[k] = off;
         off += (long long)mlp->dims[k + 1] * mlp->dims[k] + mlp->dims[k + 1];
+    }
+    if (amax <= kTMaxW) {  // the register-tiled kernel
+        size_t smem = sizeof(float) * (2 * (size_t)kTMaxW * kTRows + (size_t)(kTMaxW + 1) * (kTMaxW + 1));
+        if ((st = set_smem(k_mlp_tiled, smem))) return st;
+        long long tiles = (rows + kTRows - 1) / kTRows;
+        int grid = (int)std::min<long long>(tiles, kNumSM);  // one CTA per SM (184 KB of shared memory)
+        k_mlp_tiled<<<grid, kTThreads, smem, as_stream(stream)>>>(d_g, rows, m, mlp->d_w, d_e);
+        return check_launch();
     }
     size_t smem = 2 * sizeof(float) * (size_t)amax * kMlpRows;
     if ((st = set_smem(k_mlp, smem))) return st;
