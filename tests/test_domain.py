@@ -1,4 +1,4 @@
-"""Spatial domain decomposition (amlp.domain) on two gloo ranks on the CPU.
+"""Spatial domain decomposition (amlp.domain) on two and three gloo ranks on the CPU.
 
 Each rank owns the bodies of one slab of the box, receives the halo of its
 neighbours by send/recv, and evaluates the forces of every pair with an owned
@@ -18,13 +18,15 @@ import numpy as np
 import pytest
 import torch
 
-WORLD = 2
-L_BOX = 33.0  # the reference's th_v1 init box; slabs of 16.5 hold a halo of 7.75 twice
+# (ranks, bodies, box): the reference's th_v1 init box of 33 with two slabs of 16.5, and a box of 48
+# with three slabs of 16 (distinct lower and upper neighbours); each slab holds the halo of 7.75 twice
+SETUPS = {2: (400, 33.0), 3: (1200, 48.0)}
 
 
-def _state():
+def _state(world):
     from amlp.configs import make_state
-    return make_state(400, "th_v1", 0.1, kT=0.5, seed=31, L=L_BOX)
+    n, L = SETUPS[world]
+    return make_state(n, "th_v1", 0.1, kT=0.5, seed=31, L=L)
 
 
 def _layers():
@@ -42,7 +44,7 @@ def _forces(pos, quat, pairs_verlet, n_owned, L, shape, layers):
     return ex["forces"][:n_owned], ex["torques"][:n_owned], pe
 
 
-def _worker(rank, port, outdir):
+def _worker(rank, world, port, outdir):
     import datetime
     import sys
     here = os.path.dirname(os.path.abspath(__file__))
@@ -54,12 +56,12 @@ def _worker(rank, port, outdir):
     from oracle.shapes import SHAPES
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=WORLD, timeout=datetime.timedelta(seconds=60))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        s = _state()
+        s = _state(world)
         shape = SHAPES["th_v1"]
-        comm = Comm(dist, rank, WORLD, "cpu")
-        slab = Slab(s.L, WORLD, rank)
+        comm = Comm(dist, rank, world, "cpu")
+        slab = Slab(s.L, world, rank)
         mine = np.nonzero(slab.owner(s.pos[:, 0]) == rank)[0]
         pos, quat = torch.tensor(s.pos[mine]), torch.tensor(s.orient[mine])
         halo = Halo(slab, shape["cutoff"] + 2.0)
@@ -88,22 +90,24 @@ def _free_port():
         return sk.getsockname()[1]
 
 
-@pytest.fixture(scope="module")
-def ranks(tmp_path_factory):
+@pytest.fixture(scope="module", params=sorted(SETUPS))
+def ranks(request, tmp_path_factory):
     import torch.multiprocessing as mp
-    out = tmp_path_factory.mktemp("domain")
-    mp.start_processes(_worker, args=(_free_port(), str(out)), nprocs=WORLD, start_method="spawn", join=True)
+    world = request.param
+    out = tmp_path_factory.mktemp(f"domain{world}")
+    mp.start_processes(_worker, args=(world, _free_port(), str(out)), nprocs=world, start_method="spawn", join=True)
     res = []
-    for r in range(WORLD):
+    for r in range(world):
         with open(out / f"rank{r}.pkl", "rb") as fh:
             res.append(pickle.load(fh))
-    return res
+    return world, res
 
 
-def test_two_domain_forces_equal_single_domain(ranks):
+def test_domain_forces_equal_single_domain(ranks):
     from oracle import nlist
     from oracle.shapes import SHAPES
-    s = _state()
+    world, ranks = ranks
+    s = _state(world)
     shape = SHAPES["th_v1"]
     vl = nlist.sorted_pairs(nlist.reference_pairs(s.pos, s.L, shape["cutoff"] + 2.0))
     F, T, pe = _forces(s.pos, s.orient, vl, s.N, s.L, shape, _layers())
@@ -118,7 +122,8 @@ def test_two_domain_forces_equal_single_domain(ranks):
 
 
 def test_migration_hands_every_body_to_its_new_owner(ranks):
-    s = _state()
+    world, ranks = ranks
+    s = _state(world)
     ids = np.concatenate([r["after"]["ids"] for r in ranks])
     assert np.array_equal(np.sort(ids), np.arange(s.N))
     for r in ranks:
