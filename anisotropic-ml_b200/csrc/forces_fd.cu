@@ -65,18 +65,11 @@ __device__ void load_tile(const float *pos, const float *quat, float L, const in
     }
 }
 
-// Variant evaluated by each warp of a tile. The warps of a CTA sit on the four
-// schedulers as w % 4, so 10 warps make loads of 3, 3, 2 and 2; the variants
-// 4..9 rotate half of the cloud's points and cost more than 0..3, so the two
-// schedulers with three warps get two cheap variants each.
-__constant__ int c_variant_of_warp[10] = {0, 2, 6, 8, 1, 3, 7, 9, 4, 5};
-
-// Descriptor of row (v = the warp's variant, p = lane) of the staged tile into gT[d*ld + col].
+// Descriptor of row (v = warp, p = lane) of the staged tile into gT[d*ld + col].
 template <class Cfg>
 __device__ __forceinline__ void tile_descriptor_row(const float *R, const float *t, const TileGeom &g, float dx,
-                                                    float dteta, float inv_rc, float *gT, int ld, int col,
-                                                    bool permute) {
-    const int v = permute ? c_variant_of_warp[threadIdx.x >> 5] : threadIdx.x >> 5, p = threadIdx.x & 31;
+                                                    float dteta, float inv_rc, float *gT, int ld, int col) {
+    const int v = threadIdx.x >> 5, p = threadIdx.x & 31;
     VariantPoints vp;
     vp.Ri = R + p * g.rs;
     vp.Rj = vp.Ri + 3 * g.npts;
@@ -110,7 +103,7 @@ __global__ void __launch_bounds__(kTileThreads) k_descriptors(const float *pos, 
         long long p0 = tile * kPT;
         load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
         __syncthreads();
-        tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld, threadIdx.x, false);
+        tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld, threadIdx.x);
         __syncthreads();
         int valid = (int)min((long long)kPT, P - p0);
         // rows v*P + p0 .. p0+valid-1 of variant v are contiguous in g_all
@@ -442,7 +435,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
         const int valid = (int)min((long long)kPT, P - p0);
         load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
         __syncthreads();
-        tile_descriptor_row<Cfg>(R, t, g, c.dx, c.dteta, inv_rc, bufA, kRows, act_col(threadIdx.x), true);
+        tile_descriptor_row<Cfg>(R, t, g, c.dx, c.dteta, inv_rc, bufA, kRows, act_col(threadIdx.x));
         __syncthreads();
         float *X = bufA, *Y = bufB;
         for (int L2 = 0; L2 + 1 < net.n_layers; ++L2) {
@@ -458,10 +451,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
             float acc = wt[net.b_off[Ll]];
             const int col = act_col(threadIdx.x);
             for (int k = 0; k < K; ++k) acc = fmaf(wl[k * net.npad[Ll]], X[k * kRows + col], acc);
-            const int v = c_variant_of_warp[threadIdx.x >> 5], pp = threadIdx.x & 31;
-            e[v * kPT + pp] = acc;
-            if (e_out && pp < valid)  // row (variant v, pair p) of e_all: e_out[v P + p0 + p]
-                e_out[(long long)v * P + p0 + pp] = acc;
+            e[threadIdx.x] = acc;
+            if (e_out && (threadIdx.x & 31) < valid)  // row (variant v, pair p) of e_all: e_out[v P + p0 + p]
+                e_out[(long long)(threadIdx.x >> 5) * P + p0 + (threadIdx.x & 31)] = acc;
         }
         __syncthreads();
         for (int idx = threadIdx.x; idx < 9 * kPT; idx += blockDim.x) {

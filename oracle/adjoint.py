@@ -91,6 +91,29 @@ def exact_pair_forces(pos, quat, pairs, L, shape, hypers, layers, act, chunk=512
     return dict(F_pair=F, T_i=Ti, T_j=Tj, forces=Fn, torques=Tn, E=E, pairs=pairs)
 
 
+def relu_margin(pos, quat, pairs, L, shape, hypers, layers, chunk=2048):
+    """Per pair, the smallest |z| over all hidden pre-activations of the net,
+    in units of that layer's mean |z| over all pairs (FP64).
+
+    A ReLU net's forces jump where a pre-activation crosses zero, so an FP32
+    evaluation matches the FP64 one only on pairs whose every z stays clear of
+    zero by more than the FP32 path's own error."""
+    nrad, nang, lmax = (int(h) for h in hypers[:3])
+    pairs = np.asarray(pairs, np.int64).reshape(-1, 2)
+    _, _, t = nep.min_image_filter(pos, pairs, L, 1e30, np.float64)
+    c1, _ = nep.pair_clouds(quat, pairs, t, shape["pts"], np.float64)
+    with torch.no_grad():
+        g = descriptor_torch(torch.tensor(c1, dtype=torch.float64), nrad, nang, lmax, float(shape["nep_cutoff"]))
+        h, margin = g, None
+        for W, b in layers[:-1]:
+            z = torch.nn.functional.linear(h, torch.as_tensor(np.asarray(W, np.float64)),
+                                           torch.as_tensor(np.asarray(b, np.float64)))
+            m = (z.abs() / z.abs().mean()).min(dim=1).values
+            margin = m if margin is None else torch.minimum(margin, m)
+            h = torch.relu(z)
+    return margin.numpy()
+
+
 def _qmul(a, b):
     w = a[..., 0] * b[..., 0] - np.sum(a[..., 1:] * b[..., 1:], axis=-1)
     v = a[..., :1] * b[..., 1:] + b[..., :1] * a[..., 1:] + np.cross(a[..., 1:], b[..., 1:])
