@@ -1635,8 +1635,17 @@ static amlp_status check_pair_args(const float *d_pos, const float *d_quat, cons
     return AMLP_OK;
 }
 
-// Grid of the direct-form descriptor kernels (one warp per pair, grid-stride).
-constexpr int kDirectBlocks = 8 * kNumSM;
+// Launch of a direct-form descriptor kernel: one thread per pair, grid-stride
+// over at most 16 blocks per SM, one float4 of shared memory per point and thread.
+template <class K, class... Args>
+static amlp_status launch_direct(K kernel, long long cap, int npts, cudaStream_t s, Args... args) {
+    const size_t smem = direct::smem_bytes(2 * npts);
+    if (smem > 48 * 1024)
+        AMLP_CHECK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long blocks = min((cap + direct::kThreads - 1) / direct::kThreads, (long long)kNumSM * 16);
+    kernel<<<(unsigned)blocks, direct::kThreads, smem, s>>>(args...);
+    return AMLP_OK;
+}
 
 static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
                                        const long long *d_npairs, long long cap, const amlp_nep *nep,
@@ -1664,13 +1673,16 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
         char *wsplit = c.take<char>(kWeightSplitBytes);
         if (!c.ok()) return AMLP_ERR_WORKSPACE;
         AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, net.smem));
-        direct::k_desc_direct_fwd<<<kDirectBlocks, 32 * direct::kWarps, 0, s>>>(
-            d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, nep->npts, inv_rc, g_rows, kGRow2);
+        const int npts = nep->npts;
+        if ((st = launch_direct(direct::k_desc_direct_fwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                (const float *)nep->d_pts, npts, inv_rc, g_rows, kGRow2)))
+            return st;
         k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
         k_mlp_grad<<<kNumSM, kMThreads, net.smem, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
-        direct::k_desc_direct_bwd<<<kDirectBlocks, 32 * direct::kWarps, 0, s>>>(
-            d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, nep->npts, inv_rc, nep->en_min, rng, dg_rows,
-            kGP2, y_rows, d_wt, clip, d_F, d_T, d_pe);
+        if ((st = launch_direct(direct::k_desc_direct_bwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                (const float *)nep->d_pts, npts, inv_rc, nep->en_min, rng, (const float *)dg_rows,
+                                kGP2, (const float *)y_rows, d_wt, clip, d_F, d_T, d_pe)))
+            return st;
         return check_launch();
     }
     if ((st = wide_net(mlp, kGP, kGRow, &net))) return st;
@@ -1736,8 +1748,10 @@ extern "C" amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_
     if (!d_g || ld_g < nep_D(nep)) return AMLP_ERR_INVALID_ARG;
     if (cap == 0) return AMLP_OK;
     if (hyper_kind(nep) == 2) {
-        direct::k_desc_direct_fwd<<<kDirectBlocks, 32 * direct::kWarps, 0, as_stream(stream)>>>(
-            d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, nep->npts, 1.0f / nep->nep_cutoff, d_g, ld_g);
+        if ((st = launch_direct(direct::k_desc_direct_fwd, cap, nep->npts, as_stream(stream), d_pos, d_quat, box,
+                                d_pairs, d_npairs, cap, (const float *)nep->d_pts, nep->npts,
+                                1.0f / nep->nep_cutoff, d_g, ld_g)))
+            return st;
         return check_launch();
     }
     const size_t smem = wide_desc_smem(nep->npts);
