@@ -98,12 +98,15 @@ def descriptor_flops(nd: int, hypers=(10, 8, 4), adjoint: bool = False) -> float
     per point the 2 (nang+1) K contraction over K = lmax (lmax + 2) harmonics plus
     their recurrences and the radial basis, 573 Nd + 432 for (10, 8, 4) and
     3,050 Nd + 250 for (10, 10, 10). Direct form (the adjoint path for (10, 10,
-    10)): per point pair the Legendre recurrences and (nang+1) lmax
-    multiply-adds, 246 Nd^2 + 60 Nd."""
+    10)): the sum over point pairs is symmetric, so per unordered pair a < b the
+    dot product (5), the Legendre recurrences (36), the (nang+1) products f_n(a)
+    f_n(b) (11) and the (nang+1) lmax multiply-adds (220), 272 FLOPs, and per
+    point the radial basis, its diagonal term and the radial sums (75):
+    136 Nd (Nd - 1) + 75 Nd."""
     if tuple(hypers) == (10, 8, 4):
         return 573.0 * nd + 432.0
     if adjoint:
-        return 246.0 * nd * nd + 60.0 * nd
+        return 136.0 * nd * (nd - 1) + 75.0 * nd
     return 3050.0 * nd + 250.0
 
 
