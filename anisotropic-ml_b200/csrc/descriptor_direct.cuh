@@ -1,12 +1,13 @@
-// Adjoint descriptor passes for the hypers (nrad, nang, lmax) = (10, 10, 10),
-// D = 121, of the reference's C100 models, in the reference's direct form
+// Adjoint descriptor passes in the reference's direct form
 // (NepDescriptorKernels.py:3-144, DescriptorGenerator.py:296-442):
-//   g_rad[n]   = sum_a f_n(a)
-//   g_ang[n,l] = sum_{a,b} f_n(a) f_n(b) P_l(c_ab),  c_ab = rhat_a . rhat_b,
-// diagonal included, over the Nd points of the pair's cloud centred on their
-// centroid. The shapes these models belong to have few points (th_v1 4, cube_v2
-// 6, pbp_v3 7 per body), so the O(Nd^2) sum is cheaper here than 11 x 120
-// harmonic sums per point.
+//   g_rad[n]   = sum_a f_n(a),                              n < NR = nrad + 1
+//   g_ang[n,l] = sum_{a,b} f_n(a) f_n(b) P_l(c_ab),         n < NA = nang + 1, 1 <= l <= LM = lmax
+// (c_ab = rhat_a . rhat_b), diagonal included, over the Nd points of the pair's
+// cloud centred on their centroid. Used for the hypers (10, 10, 10), D = 121, of
+// the reference's C100 models, whose 11 x 120 harmonic sums would not fit in
+// registers, and for (10, 8, 4), D = 47, when the clouds are small (Nd <= 12:
+// th_v1 and cube_v2, 4 and 6 points per body), where the O(Nd^2) sum costs less
+// than the harmonic form's per-point work.
 //
 // Gradient with respect to the centred point r_a (d_a = |r_a|, G = dE/dg_ang,
 // R = dE/dg_rad):
@@ -41,7 +42,6 @@
 namespace amlp {
 namespace direct {
 
-constexpr int NR = 11, NA = 11, LM = 10, D = NR + NA * LM;  // 121
 constexpr int kThreads = 64;  // pairs per block, one thread each
 constexpr int kMaxNd = 64;
 
@@ -52,7 +52,7 @@ inline size_t smem_bytes(int nd) { return (size_t)nd * kThreads * sizeof(float4)
 // the cutoff cosine from the hardware sine/cosine. The forward and the backward
 // pass run this same arithmetic, so that the forces are the exact derivative of
 // the energy the forward computed.
-template <bool DER>
+template <int NR, bool DER>
 __device__ __forceinline__ void radial(float dist, float inv_rc, float *f, float *df) {
     const float u = dist * inv_rc, um1 = u - 1.0f;
     const float x = fmaf(2.0f * um1, um1, -1.0f);
@@ -147,11 +147,14 @@ __device__ __forceinline__ void build_cloud(float4 *S, const float *pos, const f
 
 extern __shared__ float4 direct_smem[];
 
-// Forward: row q of g (121 values, then zeros up to g_ld) for every filtered pair.
+// Forward: row q of g (D values, then zeros up to g_ld) for every filtered pair.
+template <int NR, int NA, int LM>
 __global__ void __launch_bounds__(kThreads) k_desc_direct_fwd(const float *pos, const float *quat, float L,
                                                               const int *pairs, const long long *d_np, long long cap,
                                                               const float *pts, int npts, float inv_rc, float *g_rows,
                                                               int g_ld) {
+    static_assert(NA <= NR && LM >= 2, "angular radial functions are the first NA of the NR");
+    constexpr int D = NR + NA * LM;
     float4 *S = direct_smem + threadIdx.x;
     const int nd = 2 * npts;
     const float3 psum = point_sum(pts, npts);
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_desc_direct_fwd(const float *pos, 
         for (int a = 0; a < nd; ++a) {
             const float4 A = S[a * kThreads];
             float fa[NR];
-            radial<false>(A.w, inv_rc, fa, nullptr);
+            radial<NR, false>(A.w, inv_rc, fa, nullptr);
 #pragma unroll
             for (int n = 0; n < NR; ++n) rad[n] += fa[n];
 #pragma unroll
@@ -187,7 +190,7 @@ __global__ void __launch_bounds__(kThreads) k_desc_direct_fwd(const float *pos, 
 #pragma unroll
                 for (int l = 2; l < LM; ++l) Pl[l] = legendre_next(l, c, Pl[l - 1], Pl[l - 2]);
                 float fb[NR];
-                radial<false>(B.w, inv_rc, fb, nullptr);
+                radial<NR, false>(B.w, inv_rc, fb, nullptr);
 #pragma unroll
                 for (int n = 0; n < NA; ++n) {
                     const float ff = fa[n] * fb[n];
@@ -221,16 +224,19 @@ __global__ void __launch_bounds__(kThreads) k_desc_direct_fwd(const float *pos, 
     }
 }
 
-// Backward: dE/dg rows (stride gp, a multiple of 4 floats, 16-byte aligned) and
-// net outputs y in; forces, torques and pair energies out (the scaling, clip and
-// scatter of ForceEvaluator.py:119-142). wt (may be null) weights pair q's dE/dg
-// by wt[q]; clip = 0 leaves out the clip.
+// Backward: dE/dg rows (stride gp >= 4 ceil(D / 4), a multiple of 4 floats,
+// 16-byte aligned) and net outputs y in; forces, torques and pair energies out
+// (the scaling, clip and scatter of ForceEvaluator.py:119-142). wt (may be null)
+// weights pair q's dE/dg by wt[q]; clip = 0 leaves out the clip.
+template <int NR, int NA, int LM>
 __global__ void __launch_bounds__(kThreads) k_desc_direct_bwd(const float *pos, const float *quat, float L,
                                                               const int *pairs, const long long *d_np, long long cap,
                                                               const float *pts, int npts, float inv_rc, float en_min,
                                                               float en_range, const float *dg_rows, int gp,
                                                               const float *y_rows, const float *wt, int clip,
                                                               float *F, float *T, double *pe) {
+    static_assert(NA <= NR && LM >= 2, "angular radial functions are the first NA of the NR");
+    constexpr int D = NR + NA * LM;
     float4 *S = direct_smem + threadIdx.x;
     const int nd = 2 * npts;
     const float3 psum = point_sum(pts, npts);
@@ -281,7 +287,7 @@ __global__ void __launch_bounds__(kThreads) k_desc_direct_bwd(const float *pos, 
         for (int a = 0; a < nd; ++a) {
             const float4 A = S[a * kThreads];
             float fa[NR], dfa[NR];
-            radial<true>(A.w, inv_rc, fa, dfa);
+            radial<NR, true>(A.w, inv_rc, fa, dfa);
             // radial part and the diagonal: (sum_n R_n f_n'(a) + 2 sum_n f_n'(a) f_n(a) H_n(1)) rhat_a
             float ga = 0.f;
 #pragma unroll
@@ -313,7 +319,7 @@ __global__ void __launch_bounds__(kThreads) k_desc_direct_bwd(const float *pos, 
                     }
                 }
                 float fb[NR], dfb[NR];
-                radial<true>(B.w, inv_rc, fb, dfb);
+                radial<NR, true>(B.w, inv_rc, fb, dfb);
                 float al_ab = 0.f, al_ba = 0.f, be = 0.f;
 #pragma unroll
                 for (int n = 0; n < NA; ++n) {

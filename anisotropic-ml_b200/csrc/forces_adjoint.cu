@@ -1635,6 +1635,15 @@ static amlp_status check_pair_args(const float *d_pos, const float *d_quat, cons
     return AMLP_OK;
 }
 
+// The wide path and amlp_pair_descriptors take the direct-form descriptor
+// passes for the hypers (10, 10, 10) and, for (10, 8, 4), for clouds of at most
+// 12 points (th_v1, cube_v2), where the O(Nd^2) sum costs less than the
+// harmonic form; the multi-system path keeps the harmonic form.
+constexpr int kDirectMaxNd47 = 12;
+static bool use_direct(const amlp_nep *nep) {
+    return hyper_kind(nep) == 2 || (hyper_kind(nep) == 1 && 2 * nep->npts <= kDirectMaxNd47);
+}
+
 // Launch of a direct-form descriptor kernel: one thread per pair, grid-stride
 // over at most 16 blocks per SM, one float4 of shared memory per point and thread.
 template <class K, class... Args>
@@ -1663,25 +1672,29 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     cudaStream_t s = as_stream(stream);
     const float inv_rc = 1.0f / nep->nep_cutoff, rng = nep->en_max - nep->en_min;
     AdjNet net;
-    if (hyper_kind(nep) == 2) {  // D = 121: the direct-form descriptor passes around the same net kernel
+    if (hyper_kind(nep) == 2 || (use_direct(nep) && !d_rep)) {  // the direct-form passes around the same net kernel
         if (d_rep) return AMLP_ERR_UNSUPPORTED;
-        if ((st = wide_net(mlp, kGP2, kGRow2, &net))) return st;
+        const bool k2 = hyper_kind(nep) == 2;
+        const int gp = k2 ? kGP2 : kGP, grow = k2 ? kGRow2 : kGRow;
+        if ((st = wide_net(mlp, gp, grow, &net))) return st;
         Carver c(d_ws, ws_bytes);
-        float *g_rows = c.take<float>((size_t)cap * kGRow2);
-        float *dg_rows = c.take<float>((size_t)cap * kGP2);
+        float *g_rows = c.take<float>((size_t)cap * grow);
+        float *dg_rows = c.take<float>((size_t)cap * gp);
         float *y_rows = c.take<float>((size_t)cap);
         char *wsplit = c.take<char>(kWeightSplitBytes);
         if (!c.ok()) return AMLP_ERR_WORKSPACE;
         AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, net.smem));
         const int npts = nep->npts;
-        if ((st = launch_direct(direct::k_desc_direct_fwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
-                                (const float *)nep->d_pts, npts, inv_rc, g_rows, kGRow2)))
+        auto fwd = k2 ? direct::k_desc_direct_fwd<11, 11, 10> : direct::k_desc_direct_fwd<11, 9, 4>;
+        auto bwd = k2 ? direct::k_desc_direct_bwd<11, 11, 10> : direct::k_desc_direct_bwd<11, 9, 4>;
+        if ((st = launch_direct(fwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                (const float *)nep->d_pts, npts, inv_rc, g_rows, grow)))
             return st;
         k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
         k_mlp_grad<<<kNumSM, kMThreads, net.smem, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
-        if ((st = launch_direct(direct::k_desc_direct_bwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
-                                (const float *)nep->d_pts, npts, inv_rc, nep->en_min, rng, (const float *)dg_rows,
-                                kGP2, (const float *)y_rows, d_wt, clip, d_F, d_T, d_pe)))
+        if ((st = launch_direct(bwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                (const float *)nep->d_pts, npts, inv_rc, nep->en_min, rng, (const float *)dg_rows, gp,
+                                (const float *)y_rows, d_wt, clip, d_F, d_T, d_pe)))
             return st;
         return check_launch();
     }
@@ -1747,10 +1760,10 @@ extern "C" amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_
     if (st) return st;
     if (!d_g || ld_g < nep_D(nep)) return AMLP_ERR_INVALID_ARG;
     if (cap == 0) return AMLP_OK;
-    if (hyper_kind(nep) == 2) {
-        if ((st = launch_direct(direct::k_desc_direct_fwd, cap, nep->npts, as_stream(stream), d_pos, d_quat, box,
-                                d_pairs, d_npairs, cap, (const float *)nep->d_pts, nep->npts,
-                                1.0f / nep->nep_cutoff, d_g, ld_g)))
+    if (use_direct(nep)) {
+        auto fwd = hyper_kind(nep) == 2 ? direct::k_desc_direct_fwd<11, 11, 10> : direct::k_desc_direct_fwd<11, 9, 4>;
+        if ((st = launch_direct(fwd, cap, nep->npts, as_stream(stream), d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                (const float *)nep->d_pts, nep->npts, 1.0f / nep->nep_cutoff, d_g, ld_g)))
             return st;
         return check_launch();
     }

@@ -74,6 +74,22 @@ def descriptors(pos, quat, L, pairs, shape, hypers):
     return g.cpu().numpy()
 
 
+def pair_descriptors(pos, quat, L, pairs, shape, hypers, ld=None):
+    """amlp_pair_descriptors: one descriptor row per pair (the adjoint path's forward)."""
+    pts_t = t32(shape["pts"])
+    D = (hypers[0] + 1) + (hypers[1] + 1) * hypers[2]
+    ld = ld or D
+    P = len(pairs)
+    g = torch.full((max(P, 1), ld), float("nan"), dtype=torch.float32, device=DEV)
+    pr = torch.tensor(np.asarray(pairs, np.int32).reshape(-1, 2), device=DEV).contiguous()
+    npairs = torch.tensor([P], dtype=torch.int64, device=DEV)
+    n = nep_struct(shape, hypers, pts_t)
+    pos_t, quat_t = t32(pos), t32(quat)
+    call("amlp_pair_descriptors", pos_t.data_ptr(), quat_t.data_ptr(), float(L), pr.data_ptr(), npairs.data_ptr(),
+         max(P, 1), ctypes.byref(n), g.data_ptr(), ld, stream())
+    return g[:P].cpu().numpy()
+
+
 def mlp_energy(layers, act, g):
     net = EnergyNet(layers, act, DEV)
     gt = t32(g)

@@ -150,6 +150,29 @@ def test_descriptors_new_shapes(shape_name, phi, seed):
     _check_desc(g, g64)
 
 
+@pytest.mark.parametrize("shape_name,hyp,ld", [("th_v1", (10, 8, 4), 52), ("cube_v2", (10, 8, 4), 47),
+                                               ("pbp_v3", (10, 8, 4), 48), ("th_v1", (10, 10, 10), 132),
+                                               ("cube_v2", (10, 10, 10), 121)])
+def test_pair_descriptors_vs_fp64(shape_name, hyp, ld):
+    """amlp_pair_descriptors, the forward of the adjoint path: the direct form for
+    (10, 10, 10) and for (10, 8, 4) clouds of up to 12 points (th_v1, cube_v2), the
+    harmonic form for pbp_v3's 14; row strides with and without 16-byte rows and
+    zero padding past D."""
+    s = make_state(300, shape_name, 0.1, seed=5, L={"pbp_v3": 32.0}.get(shape_name, 24.0))  # ~20 neighbours each
+    shape = SHAPES[shape_name]
+    vp = nlist.sorted_pairs(nlist.reference_pairs(s.pos, s.L, shape["cutoff"] + 2.0))
+    _, pairs, _ = nep.min_image_filter(s.pos, vp, s.L, shape["cutoff"])
+    assert 1000 < len(pairs) < 10000
+    D = (hyp[0] + 1) + (hyp[1] + 1) * hyp[2]
+    g = gh.pair_descriptors(s.pos, s.orient, s.L, pairs, shape, hyp, ld=ld)
+    _, _, t = nep.min_image_filter(s.pos, pairs, s.L, shape["cutoff"], np.float64)
+    c1, _ = nep.pair_clouds(s.orient, pairs, t, shape["pts"], np.float64)
+    g64 = nep.descriptor(c1, hyp, shape["nep_cutoff"], np.float64)
+    _check_desc(g[:, :D], g64)
+    if ld > D:
+        assert np.all(g[:, D:] == 0.0)
+
+
 # ----------------------------------------------------------------------------- net energies
 @pytest.mark.parametrize("widths,act", [((64, 64), "tanh"), ((128, 128, 128), "silu"), ((150, 150, 150, 150), "relu")])
 def test_mlp_energy_vs_torch(widths, act):
