@@ -129,6 +129,8 @@ SIGNATURES = {
     "amlp_mlp_backward": [_P, _P, _LL, ctypes.POINTER(Mlp), _P, _P],
     "amlp_device_error": [ctypes.POINTER(ctypes.c_uint), _I],
     "amlp_test_first_wait_limit": [_I],
+    "amlp_stage_timing": [_I],
+    "amlp_stage_times": [ctypes.POINTER(_F)],
     "amlp_fp32_fma_probe": [_P, _I, ctypes.POINTER(_D), _P],
     "amlp_nvt_workspace_bytes": [_I, _PSZ],
     "amlp_nvt_init": [_P, _P, _P, _P, _I, ctypes.POINTER(Nvt), _I, _P, _P, _SZ, _P],

@@ -1656,6 +1656,17 @@ static amlp_status launch_direct(K kernel, long long cap, int npts, cudaStream_t
     return AMLP_OK;
 }
 
+// Stage events of the wide path (amlp_stage_timing): one set for the library,
+// recorded by the last call on its stream.
+static bool g_stage_timing = false;
+static bool g_stage_recorded = false;
+static cudaEvent_t g_stage_ev[4];
+
+static void stage_mark(int k, cudaStream_t s) {
+    if (g_stage_timing) cudaEventRecord(g_stage_ev[k], s);
+    if (g_stage_timing && k == 3) g_stage_recorded = true;
+}
+
 static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
                                        const long long *d_npairs, long long cap, const amlp_nep *nep,
                                        const amlp_mlp *mlp, const float *d_wt, int clip, float *d_F, float *d_T,
@@ -1687,15 +1698,19 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
         const int npts = nep->npts;
         auto fwd = k2 ? direct::k_desc_direct_fwd<11, 11, 10> : direct::k_desc_direct_fwd<11, 9, 4>;
         auto bwd = k2 ? direct::k_desc_direct_bwd<11, 11, 10> : direct::k_desc_direct_bwd<11, 9, 4>;
+        stage_mark(0, s);
         if ((st = launch_direct(fwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
                                 (const float *)nep->d_pts, npts, inv_rc, g_rows, grow)))
             return st;
+        stage_mark(1, s);
         k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
         k_mlp_grad<<<kNumSM, kMThreads, net.smem, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
+        stage_mark(2, s);
         if ((st = launch_direct(bwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
                                 (const float *)nep->d_pts, npts, inv_rc, nep->en_min, rng, (const float *)dg_rows, gp,
                                 (const float *)y_rows, d_wt, clip, d_F, d_T, d_pe)))
             return st;
+        stage_mark(3, s);
         return check_launch();
     }
     if ((st = wide_net(mlp, kGP, kGRow, &net))) return st;
@@ -1716,14 +1731,18 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mlp));
+    stage_mark(0, s);
     fwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, g_rows, kGRow, nullptr, nullptr, nullptr, clip, d_F,
                                              d_T, d_pe, d_rep, d_rp, a_rows);
+    stage_mark(1, s);
     k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
     k_mlp_grad<<<kNumSM, kMThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
+    stage_mark(2, s);
     bwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, nullptr, kGP, dg_rows, y_rows, d_wt, clip, d_F, d_T,
                                              d_pe, d_rep, d_rp, a_rows);
+    stage_mark(3, s);
     return check_launch();
 }
 
@@ -1778,6 +1797,22 @@ extern "C" amlp_status amlp_pair_descriptors(const float *d_pos, const float *d_
                                                         nullptr, 1, nullptr, nullptr, nullptr, nullptr, nullptr,
                                                         nullptr);
     return check_launch();
+}
+
+extern "C" amlp_status amlp_stage_timing(int enable) {
+    if (enable && !g_stage_ev[0]) {
+        for (auto &e : g_stage_ev) AMLP_CHECK_CUDA(cudaEventCreate(&e));
+    }
+    g_stage_timing = enable != 0;
+    return AMLP_OK;
+}
+
+extern "C" amlp_status amlp_stage_times(float *h_ms3) {
+    if (!h_ms3) return AMLP_ERR_INVALID_ARG;
+    if (!g_stage_recorded) return AMLP_ERR_INVALID_ARG;  // no call recorded its stages yet
+    AMLP_CHECK_CUDA(cudaEventSynchronize(g_stage_ev[3]));
+    for (int k = 0; k < 3; ++k) AMLP_CHECK_CUDA(cudaEventElapsedTime(h_ms3 + k, g_stage_ev[k], g_stage_ev[k + 1]));
+    return AMLP_OK;
 }
 
 extern "C" amlp_status amlp_test_first_wait_limit(int polls) {

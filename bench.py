@@ -90,23 +90,41 @@ DRAM_BYTES_PER_PAIR = {"adjoint": 5.340928e6 / 436636, "fd": 5.318912e6 / 436636
 # net, so the figure serves every wide workload.
 DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.141824e6 + 350.520064e6 + 79.480064e6 + 26.586624e6 + 409.184e6
                                        + 5.303552e6) / 381342
+# Per stage of the wide path, keyed by (kernel, D): ncu dram__bytes_read.sum + dram__bytes_write.sum per
+# pair at 32,768 th_v1 bodies (87,256 pairs; the profiles give the commands). The descriptor rows
+# depend on D, not on the net or the shape.
+STAGE_DRAM_BYTES_PER_PAIR = {
+    ("k_mlp_grad", 47): 18.56128e6 / 87256,
+    ("k_desc_direct_fwd", 121): (2.888960e6 + 1.725440e6) / 87257,
+    ("k_desc_direct_bwd", 121): (47.458304e6 + 0.022528e6) / 87257,
+}
 
 
-def descriptor_flops(nd: int, hypers=(10, 8, 4), adjoint: bool = False) -> float:
+def uses_direct_form(nd: int, hypers=(10, 8, 4)) -> bool:
+    """Whether the adjoint wide path runs the direct-form descriptor kernels: the
+    hypers (10, 10, 10), and (10, 8, 4) clouds of at most 12 points (the
+    library's own choice, kDirectMaxNd47)."""
+    return tuple(hypers) != (10, 8, 4) or nd <= 12
+
+
+def descriptor_flops(nd: int, hypers=(10, 8, 4), direct: bool = False) -> float:
     """Algorithmic FLOPs of one descriptor evaluation of an Nd-point cloud.
-    Spherical-harmonic form (the plain path, and the adjoint path for (10, 8, 4)):
-    per point the 2 (nang+1) K contraction over K = lmax (lmax + 2) harmonics plus
-    their recurrences and the radial basis, 573 Nd + 432 for (10, 8, 4) and
-    3,050 Nd + 250 for (10, 10, 10). Direct form (the adjoint path for (10, 10,
-    10)): the sum over point pairs is symmetric, so per unordered pair a < b the
-    dot product (5), the Legendre recurrences (36), the (nang+1) products f_n(a)
-    f_n(b) (11) and the (nang+1) lmax multiply-adds (220), 272 FLOPs, and per
-    point the radial basis, its diagonal term and the radial sums (75):
-    136 Nd (Nd - 1) + 75 Nd."""
+    Spherical-harmonic form (the plain path, and the adjoint path for (10, 8, 4)
+    and larger clouds): per point the 2 (nang+1) K contraction over K = lmax
+    (lmax + 2) harmonics plus their recurrences and the radial basis, 573 Nd + 432
+    for (10, 8, 4) and 3,050 Nd + 250 for (10, 10, 10). Direct form: the sum over
+    point pairs is symmetric, so per unordered pair a < b the dot product (5), the
+    Legendre recurrences (4 (lmax - 1)), the (nang+1) products f_n(a) f_n(b) and
+    the (nang+1) lmax multiply-adds, 272 FLOPs for (10, 10, 10) and 98 for
+    (10, 8, 4); per point the radial basis (42), its diagonal term (2 (nang+1))
+    and the radial sums (nrad+1)."""
+    nrad, nang, lmax = (int(h) for h in hypers[:3])
+    if direct:
+        per_pair = 5 + 4 * (lmax - 1) + (nang + 1) + 2 * (nang + 1) * lmax
+        per_point = 42 + 2 * (nang + 1) + (nrad + 1)
+        return per_pair * nd * (nd - 1) / 2.0 + per_point * nd
     if tuple(hypers) == (10, 8, 4):
         return 573.0 * nd + 432.0
-    if adjoint:
-        return 136.0 * nd * (nd - 1) + 75.0 * nd
     return 3050.0 * nd + 250.0
 
 
@@ -120,7 +138,8 @@ def algorithmic_flops_per_pair(method: str, nd: int = 52, D: int = 47, widths=WI
     fn = 2.0 * sum(dims[k] * dims[k + 1] for k in range(len(dims) - 1))
     if method in ("fd", "fd_split"):
         return 10.0 * (descriptor_flops(nd, hypers) + fn), 0.0
-    return 3.0 * descriptor_flops(nd, hypers, adjoint=True), 2.0 * fn
+    wide = max(widths) > 64 or tuple(hypers) != (10, 8, 4)
+    return 3.0 * descriptor_flops(nd, hypers, direct=wide and uses_direct_form(nd, hypers)), 2.0 * fn
 
 
 class ClockSampler:
@@ -393,7 +412,9 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
     rebuilds[0] = 0
     origin[0] = system.timestep
     start = (system.timestep, system.snapshot_tensors())  # the end-to-end leg starts from the same state
-    step_ms, force_ms = [], []
+    step_ms, force_ms, stage_ms = [], [], []
+    if wide:  # events between the three kernels of the wide force pass, on the launching stream
+        _lib.call("amlp_stage_timing", 1)
     for _ in range(steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -404,12 +425,19 @@ def _measure(system, method: str, steps: int, warmup: int, dist, dev):
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
         force_ms.append(f0.elapsed_time(f1))
+        if wide:
+            st3 = (ctypes.c_float * 3)()
+            _lib.call("amlp_stage_times", st3)
+            stage_ms.append(list(st3))
+    if wide:
+        _lib.call("amlp_stage_timing", 0)
     total = max_over_ranks(sum(step_ms), dist, dev)
     assert _lib.device_error() == 0, "a bounded device wait gave up"
     finite = bool(torch.isfinite(system.pos).all() and torch.isfinite(system.vel).all())
     return {"total_ms": total, "force_ms": statistics.mean(force_ms), "force_share": sum(force_ms) / sum(step_ms),
             "P": P, "NV": NV, "launches": launches[0], "P_end": int(system.nf.item()), "finite": finite,
-            "rebuilds": rebuilds[0], "start": start}
+            "rebuilds": rebuilds[0], "start": start,
+            "stage_ms": [statistics.mean(col) for col in zip(*stage_ms)] if stage_ms else None}
 
 
 def _e2e(system, method, steps, dist, dev, start):
@@ -493,6 +521,44 @@ def run_serving(dev, n_requests: int = 48, steps: int = 300, rate: float = 8.0, 
             "served_over_sequential_plain": stats["particle_steps_per_s"] / seq_rate}
 
 
+def wide_roofline(roof: dict, r: dict, D: int, fp32_peak: float, bf16_peak: float) -> dict:
+    """Roofline of the wide adjoint force pass from its three stages, each timed
+    with CUDA events on the launching stream inside the timed window
+    (amlp_stage_timing): the descriptor forward (one evaluation, FP32), the net
+    forward and backward on the tensor cores (2 F_n per pair, algorithmic: one
+    product per multiply-add, executed as three bf16 products), the descriptor
+    backward (two evaluations' worth, FP32). The line's roofline is the stage
+    that takes the most time; all three are listed."""
+    from amlp.shapes import get_shape
+    nd = get_shape(SHAPE).nd
+    direct = uses_direct_form(nd, HYPERS)
+    fd1 = descriptor_flops(nd, HYPERS, direct=direct)
+    _, tc_pair = algorithmic_flops_per_pair("adjoint", nd=nd, D=D, widths=WIDTHS, hypers=HYPERS)
+    names = (["k_desc_direct_fwd", "k_mlp_grad", "k_desc_direct_bwd"] if direct else
+             ["k_adj_desc (forward)", "k_mlp_grad", "k_adj_desc (backward)"])
+    P = r["P"]
+    stages = []
+    for name, ms, (fl, bound) in zip(names, r["stage_ms"], ((fd1, "fp32"), (tc_pair, "tensor"), (2 * fd1, "fp32"))):
+        ach = fl * P / (ms / 1e3) / 1e12
+        peak = bf16_peak if bound == "tensor" else fp32_peak
+        tb = STAGE_DRAM_BYTES_PER_PAIR.get((name, D))
+        st = {"kernel": name, "ms": ms, "bound": bound, "flops_per_pair": fl, "achieved": ach, "peak": peak,
+              "frac": ach / peak, "traffic": tb * P if tb else None}
+        if bound == "tensor":
+            st["executed_tflops"] = 3.0 * ach
+            st["frac_executed"] = 3.0 * ach / peak
+        stages.append(st)
+    dom = max(stages, key=lambda x: x["ms"])
+    out = dict(roof)
+    out.update({"bound": dom["bound"], "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": dom["peak"],
+                "frac": dom["frac"], "traffic": dom["traffic"], "stages": stages,
+                "work": ("the stage that takes the most time; tensor stages count one product per multiply-add "
+                         "against the measured bf16 peak (executed as three: frac_executed)")})
+    out.pop("peak_nominal", None)
+    out.pop("frac_of_nominal", None)
+    return out
+
+
 def make_net(dev):
     """The workload's net: seeded Xavier weights, the same with the output layer scaled by 0.05, or the
     shape's trained soft-repulsion net."""
@@ -559,29 +625,26 @@ def run_gpu(args, rank: int, world: int, local_rank: int) -> None:
                       "peak": peaks["bf16_tflops"], "frac_executed": 3.0 * tc_alg / peaks["bf16_tflops"],
                       "note": "net on the tensor cores as three bf16 products per multiply-add (bf16x3)"}
         wide = m == "adjoint" and (max(WIDTHS) > 64 or HYPERS != (10, 8, 4))
-        kernel = {"fd": "k_forces_fd", "fd_split": "k_descriptors + k_mlp + k_fd_scatter"}.get(
-            m, "k_adj_desc x2 + k_mlp_grad" if wide else "k_forces_adjoint")
-        if wide and HYPERS != (10, 8, 4):
-            kernel = "k_desc_direct_fwd + k_mlp_grad + k_desc_direct_bwd"
-        traffic_key = "adjoint_wide" if wide and HYPERS == (10, 8, 4) else m
-        traffic = DRAM_BYTES_PER_PAIR.get(traffic_key)
+        kernel = {"fd": "k_forces_fd", "fd_split": "k_descriptors + k_mlp + k_fd_scatter"}.get(m, "k_forces_adjoint")
+        traffic = DRAM_BYTES_PER_PAIR.get(m)
+        roof = {"bound": "fp32", "kernel": kernel, "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "peak_nominal": fp32_nominal, "frac_of_nominal": achieved / fp32_nominal,
+                "traffic": traffic * r["P"] if traffic else None,
+                "traffic_unit": "bytes per launch (ncu, scaled by pairs from 32,768 bodies)",
+                "flops_per_pair": fl_pair, "tensor_flops_per_pair": tc_pair, "tensor": tensor,
+                "pairs_per_launch": r["P"], "launch_ms": r["force_ms"], "force_share_of_step": r["force_share"],
+                "peak_source": (f"measured FP32 FMA throughput of amlp_fp32_fma_probe in this run (best of 3, "
+                                f"CUDA events); nominal 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz beside it; "
+                                f"HBM {peaks['hbm_gbs']} GB/s, bf16 {peaks['bf16_tflops']} TFLOP/s "
+                                f"{peaks['source']}"),
+                "work": ("achieved counts the FP32 SIMT work only (descriptor forward and backward); "
+                         "the net's tensor-core work is reported under 'tensor'") if tc_pair else
+                        "achieved counts all the work (descriptors and net, FP32 SIMT)"}
+        if wide and r.get("stage_ms"):
+            roof = wide_roofline(roof, r, D, fp32_peak, peaks["bf16_tflops"])
         return {"value": job_throughput(world, N_BODIES, args.steps, r["total_ms"]), "ms_per_step": r["total_ms"] / args.steps,
-                "roofline": {"bound": "fp32",
-                             "kernel": kernel, "achieved": achieved, "peak": fp32_peak,
-                             "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                             "peak_nominal": fp32_nominal, "frac_of_nominal": achieved / fp32_nominal,
-                             "traffic": traffic * r["P"] if traffic else None,
-                             "traffic_unit": "bytes per force pass (ncu, scaled by pairs from 32,768 bodies)",
-                             "flops_per_pair": fl_pair, "tensor_flops_per_pair": tc_pair, "tensor": tensor,
-                             "pairs_per_launch": r["P"], "launch_ms": r["force_ms"],
-                             "force_share_of_step": r["force_share"],
-                             "peak_source": (f"measured FP32 FMA throughput of amlp_fp32_fma_probe in this run (best of 3, "
-                                             f"CUDA events); nominal 148 SM x 128 lanes x 2 x {clk_mhz:.0f} MHz beside it; "
-                                             f"HBM {peaks['hbm_gbs']} GB/s, bf16 {peaks['bf16_tflops']} TFLOP/s "
-                                             f"{peaks['source']}"),
-                             "work": ("achieved counts the FP32 SIMT work only (descriptor forward and backward); "
-                                      "the net's tensor-core work is reported under 'tensor'") if tc_pair else
-                                     "achieved counts all the work (descriptors and net, FP32 SIMT)"},
+                "roofline": roof,
                 "e2e": {"value": job_throughput(world, N_BODIES, r["e2e_steps"], r["e2e_ms"]), "unit": "particle-steps/s",
                         "h2d_bytes_per_step": r["e2e_bytes"], "d2h_bytes_per_step": r["e2e_bytes"],
                         "steps": r["e2e_steps"]},

@@ -286,6 +286,15 @@ amlp_status amlp_device_error(unsigned int *flags, int clear);
  * memory. -1 restores the normal limit. It applies to later launches. */
 amlp_status amlp_test_first_wait_limit(int polls);
 
+/* Stage timing (no reference counterpart): with enable = 1, every later
+ * amlp_forces_adjoint_wide / amlp_pair_energy_vjp call records CUDA events on
+ * its stream around its three stages: descriptor forward, net forward and
+ * backward (k_mlp_grad, with the weight split), descriptor backward. Not for
+ * calls captured into a CUDA graph. amlp_stage_times waits for the last such
+ * call's events and writes the three durations in milliseconds. */
+amlp_status amlp_stage_timing(int enable);
+amlp_status amlp_stage_times(float *h_ms3);
+
 /* --------------------------------------------------------------- NVT integrator
  * d_th: one amlp_thermostat in device memory.
  * init: kinetic energies before the first step. With initial_ke_quirk = 1 the
