@@ -95,6 +95,9 @@ DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.141824e6 + 350.520064e6 + 79.480064e6 +
 # depend on D, not on the net or the shape.
 STAGE_DRAM_BYTES_PER_PAIR = {
     ("k_mlp_grad", 47): 18.56128e6 / 87256,
+    ("k_mlp_grad", 121): (46.54e6 + 0.39e6) / 87257,
+    ("k_desc_direct_fwd", 47): 1.64e6 / 87256,
+    ("k_desc_direct_bwd", 47): 19.54e6 / 87256,
     ("k_desc_direct_fwd", 121): (2.888960e6 + 1.725440e6) / 87257,
     ("k_desc_direct_bwd", 121): (47.458304e6 + 0.022528e6) / 87257,
 }
