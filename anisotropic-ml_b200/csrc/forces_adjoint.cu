@@ -458,13 +458,21 @@ __device__ __forceinline__ void mma3(uint32_t d_tmem, const char *a_hi, int K, c
 
 // Write 8 consecutive values of row p, columns c0..c0+7 into a K-major bf16
 // hi/lo tile of width K.
+// The splits are rounded two at a time (one packed conversion per pair, the
+// same round-to-nearest-even values as tc::split_bf16).
 __device__ __forceinline__ void store_split8(char *tile_hi, int K, int p, int c0, const float *v) {
-    __align__(16) __nv_bfloat16 hi[8], lo[8];
+    uint32_t hi[4], lo[4];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) tc::split_bf16(v[k], hi[k], lo[k]);
+    for (int k = 0; k < 4; ++k) {
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+        const float2 hf = __bfloat1622float2(h2);
+        const __nv_bfloat162 l2 = __floats2bfloat162_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
+        hi[k] = *reinterpret_cast<const uint32_t *>(&h2);
+        lo[k] = *reinterpret_cast<const uint32_t *>(&l2);
+    }
     uint32_t off = tc::kmajor_offset(p, c0, K);
-    *reinterpret_cast<uint4 *>(tile_hi + off) = *reinterpret_cast<uint4 *>(hi);
-    *reinterpret_cast<uint4 *>(tile_hi + kAP * K * 2 + off) = *reinterpret_cast<uint4 *>(lo);
+    *reinterpret_cast<uint4 *>(tile_hi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4 *>(tile_hi + kAP * K * 2 + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
 // Centroid of pair q's cloud into S.cen from its orientations and translation
@@ -1508,7 +1516,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
                                                                float *y_rows, float *dg_rows) {
     extern __shared__ __align__(128) char smem_raw[];
     constexpr int kSlots = kWideMax / kPC;  // 5
-    __shared__ uint64_t mbar, gbar, wfull[kSlots], chunk_ready[kSlots];
+    __shared__ uint64_t mbar, gbar, wfull[kSlots], chunk_ready[kSlots], slot_free[kSlots];
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
     char *tile = smem_raw;
@@ -1535,6 +1543,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
         for (int k = 0; k < kSlots; ++k) {
             tc::mbar_init(&wfull[k], 1);
             tc::mbar_init(&chunk_ready[k], kMThreads / 32);
+            tc::mbar_init(&slot_free[k], 1);
         }
     }
     tc::fence_before();
@@ -1549,33 +1558,56 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
     auto region = [&](int x) { return (uint32_t)((x & 1) * 256); };
     bool gave_up = false, aborted = false;
     uint32_t mphase = 0;
-    // thread 0's bookkeeping: phases of chunk_ready and wfull, slots with a copy in flight,
-    // a commit not yet waited for
-    uint32_t cr_phase = 0, wf_phase = 0, w_pending = 0;
+    // thread 0's bookkeeping: phases of chunk_ready, wfull and slot_free, slots with a copy in
+    // flight, slots whose last chunk MMA has a commit not yet waited for, a product commit not
+    // yet waited for
+    uint32_t cr_phase = 0, wf_phase = 0, sf_phase = 0, w_pending = 0, sf_pending = 0;
     bool commit_pending = false;
-    auto load_weights = [&](int x) {  // thread 0: every chunk of product x into its slot
-        if (aborted || gave_up) return;
-        const int K = in_w(x), nch = (K + kPC - 1) / kPC;
-        for (int j = 0; j < nch; ++j) {
-            const uint32_t dst = slots_u32 + (uint32_t)(j * net.slot_bytes), wb = tc::smem_u32(&wfull[j]);
-            if (x < nh) {
-                const int Np = net.nout[x];
-                const uint32_t bytes = (uint32_t)(128 * Np);
-                tc::mbar_arrive_expect_tx(wb, bytes);
-                tc::bulk_g2s(dst, wchunks + net.wch_off[x] + (size_t)j * bytes, bytes, wb);
-            } else {
-                const int L2 = nprod - 1 - x, Np = net.nout[L2], Kp = net.kin[L2];
-                const int rows = min(kPC, Np - j * kPC);
-                const uint32_t bytes = (uint32_t)(rows * Kp * 2);
-                const char *hi = wsplit + net.wsm_off[L2] + (size_t)j * kPC * Kp * 2;
-                tc::mbar_arrive_expect_tx(wb, 2 * bytes);
-                tc::bulk_g2s(dst, hi, bytes, wb);
-                tc::bulk_g2s(dst + (uint32_t)(kPC * Kp * 2), hi + (size_t)Np * Kp * 2, bytes, wb);
+    auto nchunks = [&](int x) { return (in_w(x) + kPC - 1) / kPC; };
+    // thread 0: slot j is free once the chunk MMA that last read it has completed (each
+    // chunk's MMAs commit to slot_free[j]; every such commit is waited for, in order, before
+    // the next copy into the slot)
+    auto free_slot = [&](int j) {
+        if (!((sf_pending >> j) & 1u)) return true;
+        if (!tc::mbar_wait(tc::smem_u32(&slot_free[j]), (sf_phase >> j) & 1u)) return false;
+        sf_phase ^= 1u << j;
+        sf_pending &= ~(1u << j);
+        return true;
+    };
+    // thread 0: chunk j of product x into slot j (free)
+    auto load_one = [&](int x, int j) {
+        const uint32_t dst = slots_u32 + (uint32_t)(j * net.slot_bytes), wb = tc::smem_u32(&wfull[j]);
+        if (x < nh) {
+            const int Np = net.nout[x];
+            const uint32_t bytes = (uint32_t)(128 * Np);
+            tc::mbar_arrive_expect_tx(wb, bytes);
+            tc::bulk_g2s(dst, wchunks + net.wch_off[x] + (size_t)j * bytes, bytes, wb);
+        } else {
+            const int L2 = nprod - 1 - x, Np = net.nout[L2], Kp = net.kin[L2];
+            const int rows = min(kPC, Np - j * kPC);
+            const uint32_t bytes = (uint32_t)(rows * Kp * 2);
+            const char *hi = wsplit + net.wsm_off[L2] + (size_t)j * kPC * Kp * 2;
+            tc::mbar_arrive_expect_tx(wb, 2 * bytes);
+            tc::bulk_g2s(dst, hi, bytes, wb);
+            tc::bulk_g2s(dst + (uint32_t)(kPC * Kp * 2), hi + (size_t)Np * Kp * 2, bytes, wb);
+        }
+        w_pending |= 1u << j;
+    };
+    // thread 0: chunks j0 .. of product x, each once its slot is free
+    auto load_weights = [&](int x, int j0) {
+        if (aborted || gave_up || x < 0) return;
+        for (int j = j0; j < nchunks(x); ++j) {
+            if (!free_slot(j)) {
+                gave_up = true;
+                return;
             }
-            w_pending |= 1u << j;
+            load_one(x, j);
         }
     };
-    auto issue_chunk = [&](int x, int j) {  // thread 0: chunk j of product x, once its operand columns are written
+    // thread 0: chunk j of product x, once its operand columns are written; then the
+    // slot of chunk j - 1 takes chunk j - 1 of product y (the one after x, or -1) as
+    // soon as chunk j - 1's MMAs are done, one product ahead
+    auto issue_chunk = [&](int x, int j, int y) {
         if (gave_up || aborted) return;  // nothing more is issued; the stage barrier ends the kernel
         if (!tc::mbar_wait(tc::smem_u32(&chunk_ready[j]), (cr_phase >> j) & 1u)) {
             gave_up = true;
@@ -1611,15 +1643,24 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
             tc::mma_bf16(d, da, db1, idesc, 1u);
             tc::mma_bf16(d, da1, db, idesc, 1u);
         }
+        tc::commit(tc::smem_u32(&slot_free[j]));
+        sf_pending |= 1u << j;
+        if (j > 0) {
+            if (!free_slot(j - 1)) {
+                gave_up = true;
+                return;
+            }
+            if (y >= 0 && j - 1 < nchunks(y)) load_one(y, j - 1);
+        }
     };
     // the end of an epilogue chunk: the operand columns written by this warp are
     // visible to the tensor cores; thread 0 then issues the chunk
-    auto chunk_done = [&](int x_next, int j) {
+    auto chunk_done = [&](int x_next, int j, int y) {
         tc::fence_async_smem();
         tc::fence_before();
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(tc::smem_u32(&chunk_ready[j]));
-        if (tid == 0) issue_chunk(x_next, j);
+        if (tid == 0) issue_chunk(x_next, j, y);
         __syncwarp();  // warp 0 converged again before its next tcgen05.ld
     };
     auto finish_product = [&](int x) {  // thread 0, after its last chunk: one commit for the whole product
@@ -1641,7 +1682,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
         tc::bulk_g2s(gbuf_u32, g_rows + r0 * net.g_ld, bytes, gbar_u32);
         g_pending = true;
     };
-    if (tid == 0 && blockIdx.x < ntiles) load_weights(0);
+    if (tid == 0 && blockIdx.x < ntiles) load_weights(0, 0);
     request_g(blockIdx.x);
     uint64_t m0 = 0, m1 = 0, m2 = 0;  // ReLU: act'(z) bits of hidden layers 0, 1, 2 (this thread's chunks)
     for (long long tl = blockIdx.x; tl < ntiles && !aborted; tl += gridDim.x) {
@@ -1667,7 +1708,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
                 v[4] = hi4.x, v[5] = hi4.y, v[6] = hi4.z, v[7] = hi4.w;
                 store_split8(tile, Kg, p, c0, v);
             }
-            chunk_done(0, j);
+            chunk_done(0, j, 1);
         }
         if (tid == 0) finish_product(0);
         for (int x = 0; x < nprod; ++x) {
@@ -1679,11 +1720,13 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
             aborted = __syncthreads_or(gave_up) != 0;
             if (aborted) break;
             if (x == 0) request_g(tl + gridDim.x);  // every thread has read gbuf
+            const bool more = tl + gridDim.x < ntiles;
             const int xn = x + 1 < nprod ? x + 1 : -1;  // the product this epilogue feeds (none after the last)
-            if (tid == 0) {
-                if (xn >= 0) load_weights(xn);
-                else if (tl + gridDim.x < ntiles) load_weights(0);  // the next tile's first product
-            }
+            // the product after xn (the next tile's first after the last), whose chunks go into
+            // their slots while xn runs
+            const int yn = xn < 0 ? -1 : (xn + 1 < nprod ? xn + 1 : (more ? 0 : -1));
+            // the chunks of the product after x that did not go in while x ran: from x's last on
+            if (tid == 0) load_weights(xn >= 0 ? xn : (more ? 0 : -1), nchunks(x) - 1);
             __syncwarp();
             if (x == nh && tid < kAP && p < valid)
                 y_rows[r0 + p] = (eps[p] + eps[kAP + p]) + (eps[2 * kAP + p] + eps[3 * kAP + p]) +
@@ -1699,23 +1742,31 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
                 for (int j = 0; j * kPC < Nx; ++j) {
                     const int c0 = j * kPC + 8 * h;
                     if (c0 < Nx) {
-                        float z[8], v[8];
+                        float z[8], v[8], bb[8], ww[8];
                         tc::tmem_ld8(dcol + c0, z);
+                        *reinterpret_cast<float4 *>(bb) = *reinterpret_cast<const float4 *>(bias + c0);
+                        *reinterpret_cast<float4 *>(bb + 4) = *reinterpret_cast<const float4 *>(bias + c0 + 4);
+                        if (last) {
+                            *reinterpret_cast<float4 *>(ww) = *reinterpret_cast<const float4 *>(wl + c0);
+                            *reinterpret_cast<float4 *>(ww + 4) = *reinterpret_cast<const float4 *>(wl + c0 + 4);
+                        }
+                        uint32_t b8 = 0;
 #pragma unroll
                         for (int k = 0; k < 8; ++k) {
-                            const float zz = z[k] + bias[c0 + k];
+                            const float zz = z[k] + bb[k];
                             const float fz = fmaxf(zz, 0.0f);
                             if (last) {
-                                esum = fmaf(wl[c0 + k], fz, esum);
-                                v[k] = zz > 0.0f ? wl[c0 + k] : 0.0f;
+                                esum = fmaf(ww[k], fz, esum);
+                                v[k] = zz > 0.0f ? ww[k] : 0.0f;
                             } else {
                                 v[k] = fz;
-                                if (zz > 0.0f) bits |= 1ull << (8 * j + k);
+                                b8 |= (zz > 0.0f ? 1u : 0u) << k;
                             }
                         }
+                        if (!last) bits |= (uint64_t)b8 << (8 * j);
                         store_split8(tile, Nx, p, c0, v);
                     }
-                    chunk_done(xn, j);
+                    chunk_done(xn, j, yn);
                 }
                 if (last) eps[h * kAP + p] = esum;
                 else if (x == 0) m0 = bits;
@@ -1731,8 +1782,9 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
                         tc::tmem_ld8(dcol + c0, dz);
                         if (L2 > 0) {
                             float v[8];
+                            const uint32_t b8 = (uint32_t)(bits >> (8 * j));
 #pragma unroll
-                            for (int k = 0; k < 8; ++k) v[k] = (bits >> (8 * j + k)) & 1ull ? dz[k] : 0.f;
+                            for (int k = 0; k < 8; ++k) v[k] = (b8 >> k) & 1u ? dz[k] : 0.f;
                             store_split8(tile, Nx, p, c0, v);
                         } else if (p < valid) {
                             float4 *dst = reinterpret_cast<float4 *>(dg_rows + (r0 + p) * net.gp + c0);
@@ -1740,7 +1792,7 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
                             dst[1] = make_float4(dz[4], dz[5], dz[6], dz[7]);
                         }
                     }
-                    if (xn >= 0) chunk_done(xn, j);
+                    if (xn >= 0) chunk_done(xn, j, yn);
                 }
             }
             if (tid == 0 && xn >= 0) finish_product(xn);
@@ -1751,8 +1803,10 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_r
     if (tid == 0) {
         bool drained = true;
         if (commit_pending) drained &= tc::mbar_wait(bar, mphase);  // no MMA may still be running
-        for (int j = 0; j < kSlots; ++j)  // no copy may still write shared memory
+        for (int j = 0; j < kSlots; ++j) {  // no copy, MMA or commit may still write shared memory
             if ((w_pending >> j) & 1u) drained &= tc::mbar_wait(tc::smem_u32(&wfull[j]), (wf_phase >> j) & 1u);
+            if ((sf_pending >> j) & 1u) drained &= tc::mbar_wait(tc::smem_u32(&slot_free[j]), (sf_phase >> j) & 1u);
+        }
         if (g_pending) drained &= tc::mbar_wait(gbar_u32, gphase);
         if (aborted || !drained) atomicOr(&g_amlp_device_error, kErrMbarTimeout);
     }
