@@ -61,10 +61,6 @@ struct AdjNet {
     // shared-memory carve-up and whether the next tile's g rows are prefetched
     int g_ld, gp, wmax, zbw, relu_bits;
     int wbuf_off, par_off, eps_off, gbuf_off, prefetch_g, smem;
-    // k_mlp_grad_pipe only (ReLU nets): bytes of one weight slot, and the offset of each
-    // layer's chunk-major forward image (k_split_weights) in the second weight copy
-    int pipe, slot_bytes;
-    int wch_off[kMaxHiddenWide];
 };
 
 // Activation and its derivative from one exponential, for the tensor-core
@@ -1210,16 +1206,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_adj_desc(const float *pos, con
 // The hidden layers' weights split into bf16 hi/lo once per launch, in the
 // K-major layout of the shared-memory operand (per layer: hi, then lo), so that
 // k_mlp_grad loads a layer with one bulk copy.
-// Input columns per chunk of k_mlp_grad_pipe's products.
-constexpr int kPC = 32;
-
-// bf16 hi/lo splits of the hidden layers' weights in the shared-memory image
-// of the MMA B operand: per layer the Np x Kp K-major tile (hi plane, then lo)
-// at dst + wsm_off. With dst_chunks, also the chunk-major image of
-// k_mlp_grad_pipe's forward products: per layer and chunk j of 32 input
-// columns an Np x 32 K-major tile (hi, then lo; columns past Kp zero) at
-// dst_chunks + wch_off + j * 128 * Np.
-__global__ void k_split_weights(AdjNet net, const float *w, char *dst, char *dst_chunks) {
+__global__ void k_split_weights(AdjNet net, const float *w, char *dst) {
     for (int L2 = 0; L2 < net.nh; ++L2) {
         const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
         const float *W = w + net.woff[L2];
@@ -1232,18 +1219,6 @@ __global__ void k_split_weights(AdjNet net, const float *w, char *dst, char *dst
             uint32_t o = tc::kmajor_offset(n, k, Kp);
             *reinterpret_cast<__nv_bfloat16 *>(hi + o) = a;
             *reinterpret_cast<__nv_bfloat16 *>(lo + o) = bb;
-        }
-        if (!dst_chunks) continue;
-        const int kc = (Kp + kPC - 1) / kPC * kPC;
-        for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < Np * kc; idx += gridDim.x * blockDim.x) {
-            const int n = idx / kc, k = idx - n * kc, j = k / kPC, kl = k - j * kPC;
-            const float v = (n < N && k < K) ? W[(size_t)n * K + k] : 0.f;
-            __nv_bfloat16 a, bb;
-            tc::split_bf16(v, a, bb);
-            char *ch = dst_chunks + net.wch_off[L2] + (size_t)j * 128 * Np;
-            const uint32_t o = tc::kmajor_offset(n, kl, kPC);
-            *reinterpret_cast<__nv_bfloat16 *>(ch + o) = a;
-            *reinterpret_cast<__nv_bfloat16 *>(ch + (size_t)Np * kPC * 2 + o) = bb;
         }
     }
 }
@@ -1396,21 +1371,29 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             float esum = 0.f;
             uint64_t bits = 0;
             for (int j = 0, c0 = 8 * h; c0 < Np; ++j, c0 += 8 * kMQ) {
-                float z[8], v[8], dv[8];
+                float z[8], v[8], dv[8], bb[8], ww[8];
                 tc::tmem_ld8(tmem + lane_base + c0, z);
+                *reinterpret_cast<float4 *>(bb) = *reinterpret_cast<const float4 *>(bias + c0);
+                *reinterpret_cast<float4 *>(bb + 4) = *reinterpret_cast<const float4 *>(bias + c0 + 4);
+                if (last) {
+                    *reinterpret_cast<float4 *>(ww) = *reinterpret_cast<const float4 *>(wl + c0);
+                    *reinterpret_cast<float4 *>(ww + 4) = *reinterpret_cast<const float4 *>(wl + c0 + 4);
+                }
+                uint32_t b8 = 0;
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    float zz = z[k] + bias[c0 + k], fz, dfz;
+                    float zz = z[k] + bb[k], fz, dfz;
                     act_pair(net.act, zz, fz, dfz);
                     if (last) {
-                        esum = fmaf(wl[c0 + k], fz, esum);
-                        v[k] = wl[c0 + k] * dfz;
+                        esum = fmaf(ww[k], fz, esum);
+                        v[k] = ww[k] * dfz;
                     } else {
                         v[k] = fz;
                         dv[k] = dfz;
-                        if (dfz != 0.f) bits |= 1ull << (8 * j + k);
+                        b8 |= (dfz != 0.f ? 1u : 0u) << k;
                     }
                 }
+                if (!last) bits |= (uint64_t)b8 << (8 * j);
                 store_split8(tile, Np, p, c0, v);  // the MMA that read the tile is complete
                 if (!last && !relu) tc::tmem_st8(tmem + lane_base + dfcol(L2) + c0, dv);  // for the backward
             }
@@ -1452,8 +1435,9 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
                     float dz[8], df[8], v[8];
                     tc::tmem_ld8(tmem + lane_base + c0, dz);
                     if (relu) {
+                        const uint32_t b8 = (uint32_t)(bits >> (8 * j));
 #pragma unroll
-                        for (int k = 0; k < 8; ++k) v[k] = (bits >> (8 * j + k)) & 1ull ? dz[k] : 0.f;
+                        for (int k = 0; k < 8; ++k) v[k] = (b8 >> k) & 1u ? dz[k] : 0.f;
                     } else {
                         tc::tmem_ld8(tmem + lane_base + dfcol(L2 - 1) + c0, df);
 #pragma unroll
@@ -1483,330 +1467,6 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
         // the last MMA issued (commit number `commits`, parity (commits - 1) & 1) may still be in flight
         if (commits > 0) drained &= tc::mbar_wait(bar, (uint32_t)((commits - 1) & 1));
         if (w_pending) drained &= tc::mbar_wait(wbar_u32, wphase);  // no copy may still write shared memory
-        if (g_pending) drained &= tc::mbar_wait(gbar_u32, gphase);
-        if (aborted || !drained) atomicOr(&g_amlp_device_error, kErrMbarTimeout);
-    }
-    __syncthreads();
-    if (warp == 0) {
-        tc::fence_after();
-        tc::tmem_dealloc(tmem, 512);
-    }
-}
-
-// k_mlp_grad for ReLU nets with the products pipelined against the epilogues.
-// A tile runs 2 nh products in order, x = 0 .. nh - 1 the forward layers and
-// x = nh .. 2 nh - 1 the backward ones (layer 2 nh - 1 - x); the input of
-// product x is the operand tile written by the epilogue of product x - 1 (for
-// x = 0 the staged descriptor rows). Each product is issued in chunks of kPC
-// input columns: as soon as every warp has written chunk j of the operand
-// (chunk_ready[j], one arrival per warp), thread 0 issues chunk j's MMAs, so
-// the tensor cores work while the rest of the epilogue is still running. The
-// products alternate between two TMEM regions (an epilogue reads one while the
-// next product accumulates into the other), and chunk j's weights sit in slot
-// j: their bulk copies start when the previous product completes, one
-// epilogue ahead. Forward chunks come from the chunk-major image (Np x kPC,
-// K-major); backward chunks are kPC-row blocks of the layer's K-major image,
-// read as the MN-major transpose. ReLU derivatives stay as bits in registers,
-// so TMEM holds the two product regions only. Same inputs and outputs as
-// k_mlp_grad; every wait is bounded and an expired one ends the kernel the
-// same way.
-__global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad_pipe(const float *g_rows, const long long *d_np,
-                                                               long long cap, AdjNet net, const float *w,
-                                                               const char *wsplit, const char *wchunks,
-                                                               float *y_rows, float *dg_rows) {
-    extern __shared__ __align__(128) char smem_raw[];
-    constexpr int kSlots = kWideMax / kPC;  // 5
-    __shared__ uint64_t mbar, gbar, wfull[kSlots], chunk_ready[kSlots], slot_free[kSlots];
-    __shared__ uint32_t tmem_slot;
-    const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
-    char *tile = smem_raw;
-    char *slots = smem_raw + net.wbuf_off;
-    float *par = reinterpret_cast<float *>(smem_raw + net.par_off);
-    float *eps = reinterpret_cast<float *>(smem_raw + net.eps_off);
-    float *gbuf = reinterpret_cast<float *>(smem_raw + net.gbuf_off);
-    const int nh = net.nh, nprod = 2 * nh;
-    for (int L2 = 0; L2 < nh; ++L2) {
-        const int N = net.dims[L2 + 1], Np = net.nout[L2];
-        const float *b = w + net.woff[L2] + (size_t)N * net.dims[L2];
-        for (int n = tid; n < Np; n += kMThreads) par[net.bias_off[L2] + n] = n < N ? b[n] : 0.f;
-    }
-    {
-        const int K = net.dims[nh];
-        const float *Wl = w + net.woff[nh];
-        for (int k = tid; k < kWideMax; k += kMThreads) par[net.bias_off[nh] + k] = k < K ? Wl[k] : 0.f;
-        if (tid == 0) par[net.bias_off[nh] + kWideMax] = Wl[K];
-    }
-    if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);
-    if (tid == 0) {
-        tc::mbar_init(&mbar, 1);
-        tc::mbar_init(&gbar, 1);
-        for (int k = 0; k < kSlots; ++k) {
-            tc::mbar_init(&wfull[k], 1);
-            tc::mbar_init(&chunk_ready[k], kMThreads / 32);
-            tc::mbar_init(&slot_free[k], 1);
-        }
-    }
-    tc::fence_before();
-    __syncthreads();
-    tc::fence_after();
-    const uint32_t tmem = tmem_slot, bar = tc::smem_u32(&mbar);
-    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
-    const uint32_t slots_u32 = tc::smem_u32(slots), tile_u32 = tc::smem_u32(tile);
-    // product x: input width, output width, forward layer or backward layer
-    auto in_w = [&](int x) { return x < nh ? net.kin[x] : net.nout[nprod - 1 - x]; };
-    auto out_w = [&](int x) { return x < nh ? net.nout[x] : net.kin[nprod - 1 - x]; };
-    auto region = [&](int x) { return (uint32_t)((x & 1) * 256); };
-    bool gave_up = false, aborted = false;
-    uint32_t mphase = 0;
-    // thread 0's bookkeeping: phases of chunk_ready, wfull and slot_free, slots with a copy in
-    // flight, slots whose last chunk MMA has a commit not yet waited for, a product commit not
-    // yet waited for
-    uint32_t cr_phase = 0, wf_phase = 0, sf_phase = 0, w_pending = 0, sf_pending = 0;
-    bool commit_pending = false;
-    auto nchunks = [&](int x) { return (in_w(x) + kPC - 1) / kPC; };
-    // thread 0: slot j is free once the chunk MMA that last read it has completed (each
-    // chunk's MMAs commit to slot_free[j]; every such commit is waited for, in order, before
-    // the next copy into the slot)
-    auto free_slot = [&](int j) {
-        if (!((sf_pending >> j) & 1u)) return true;
-        if (!tc::mbar_wait(tc::smem_u32(&slot_free[j]), (sf_phase >> j) & 1u)) return false;
-        sf_phase ^= 1u << j;
-        sf_pending &= ~(1u << j);
-        return true;
-    };
-    // thread 0: chunk j of product x into slot j (free)
-    auto load_one = [&](int x, int j) {
-        const uint32_t dst = slots_u32 + (uint32_t)(j * net.slot_bytes), wb = tc::smem_u32(&wfull[j]);
-        if (x < nh) {
-            const int Np = net.nout[x];
-            const uint32_t bytes = (uint32_t)(128 * Np);
-            tc::mbar_arrive_expect_tx(wb, bytes);
-            tc::bulk_g2s(dst, wchunks + net.wch_off[x] + (size_t)j * bytes, bytes, wb);
-        } else {
-            const int L2 = nprod - 1 - x, Np = net.nout[L2], Kp = net.kin[L2];
-            const int rows = min(kPC, Np - j * kPC);
-            const uint32_t bytes = (uint32_t)(rows * Kp * 2);
-            const char *hi = wsplit + net.wsm_off[L2] + (size_t)j * kPC * Kp * 2;
-            tc::mbar_arrive_expect_tx(wb, 2 * bytes);
-            tc::bulk_g2s(dst, hi, bytes, wb);
-            tc::bulk_g2s(dst + (uint32_t)(kPC * Kp * 2), hi + (size_t)Np * Kp * 2, bytes, wb);
-        }
-        w_pending |= 1u << j;
-    };
-    // thread 0: chunks j0 .. of product x, each once its slot is free
-    auto load_weights = [&](int x, int j0) {
-        if (aborted || gave_up || x < 0) return;
-        for (int j = j0; j < nchunks(x); ++j) {
-            if (!free_slot(j)) {
-                gave_up = true;
-                return;
-            }
-            load_one(x, j);
-        }
-    };
-    // thread 0: chunk j of product x, once its operand columns are written; then the
-    // slot of chunk j - 1 takes chunk j - 1 of product y (the one after x, or -1) as
-    // soon as chunk j - 1's MMAs are done, one product ahead
-    auto issue_chunk = [&](int x, int j, int y) {
-        if (gave_up || aborted) return;  // nothing more is issued; the stage barrier ends the kernel
-        if (!tc::mbar_wait(tc::smem_u32(&chunk_ready[j]), (cr_phase >> j) & 1u)) {
-            gave_up = true;
-            return;
-        }
-        cr_phase ^= 1u << j;
-        if (!tc::mbar_wait(tc::smem_u32(&wfull[j]), (wf_phase >> j) & 1u)) {
-            gave_up = true;
-            return;
-        }
-        wf_phase ^= 1u << j;
-        w_pending &= ~(1u << j);
-        tc::fence_after();
-        const int K = in_w(x), N = out_w(x), ksteps = min(2, (K - j * kPC) / 16);
-        const uint32_t a0 = tile_u32, a1 = a0 + (uint32_t)(kAP * K * 2), sb = slots_u32 + (uint32_t)(j * net.slot_bytes);
-        const bool fwd = x < nh;
-        const uint32_t idesc = tc::idesc_bf16(N, fwd ? 0 : 1);
-        const uint32_t b_lo = fwd ? (uint32_t)(N * kPC * 2) : (uint32_t)(kPC * N * 2);
-        for (int s = 0; s < ksteps; ++s) {
-            const int ks = j * (kPC / 16) + s;
-            const uint64_t da = tc::smem_desc(a0 + ks * 256, 128, (uint32_t)K * 16);
-            const uint64_t da1 = tc::smem_desc(a1 + ks * 256, 128, (uint32_t)K * 16);
-            uint64_t db, db1;
-            if (fwd) {  // Np x kPC K-major block
-                db = tc::smem_desc(sb + s * 256, 128, kPC * 16);
-                db1 = tc::smem_desc(sb + b_lo + s * 256, 128, kPC * 16);
-            } else {  // kPC rows of the Np x Kp K-major tile read as its transpose (N = Kp)
-                db = tc::smem_desc(sb + s * 2 * N * 16, (uint32_t)N * 16, 128);
-                db1 = tc::smem_desc(sb + b_lo + s * 2 * N * 16, (uint32_t)N * 16, 128);
-            }
-            const uint32_t d = tmem + region(x);
-            tc::mma_bf16(d, da, db, idesc, (j > 0 || s > 0) ? 1u : 0u);
-            tc::mma_bf16(d, da, db1, idesc, 1u);
-            tc::mma_bf16(d, da1, db, idesc, 1u);
-        }
-        tc::commit(tc::smem_u32(&slot_free[j]));
-        sf_pending |= 1u << j;
-        if (j > 0) {
-            if (!free_slot(j - 1)) {
-                gave_up = true;
-                return;
-            }
-            if (y >= 0 && j - 1 < nchunks(y)) load_one(y, j - 1);
-        }
-    };
-    // the end of an epilogue chunk: the operand columns written by this warp are
-    // visible to the tensor cores; thread 0 then issues the chunk
-    auto chunk_done = [&](int x_next, int j, int y) {
-        tc::fence_async_smem();
-        tc::fence_before();
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive(tc::smem_u32(&chunk_ready[j]));
-        if (tid == 0) issue_chunk(x_next, j, y);
-        __syncwarp();  // warp 0 converged again before its next tcgen05.ld
-    };
-    auto finish_product = [&](int x) {  // thread 0, after its last chunk: one commit for the whole product
-        (void)x;
-        tc::commit(bar);
-        commit_pending = true;
-    };
-    const long long P = min(*d_np, cap);
-    const long long ntiles = (P + kAP - 1) / kAP;
-    const int Kg = net.kin[0];
-    bool g_pending = false;
-    uint32_t gphase = 0;
-    const uint32_t gbuf_u32 = tc::smem_u32(gbuf), gbar_u32 = tc::smem_u32(&gbar);
-    auto request_g = [&](long long tl) {
-        if (!net.prefetch_g || tid != 0 || aborted || gave_up || tl >= ntiles) return;
-        const long long r0 = tl * kAP;
-        const uint32_t bytes = (uint32_t)(min((long long)kAP, P - r0) * net.g_ld * 4);
-        tc::mbar_arrive_expect_tx(gbar_u32, bytes);
-        tc::bulk_g2s(gbuf_u32, g_rows + r0 * net.g_ld, bytes, gbar_u32);
-        g_pending = true;
-    };
-    if (tid == 0 && blockIdx.x < ntiles) load_weights(0, 0);
-    request_g(blockIdx.x);
-    uint64_t m0 = 0, m1 = 0, m2 = 0;  // ReLU: act'(z) bits of hidden layers 0, 1, 2 (this thread's chunks)
-    for (long long tl = blockIdx.x; tl < ntiles && !aborted; tl += gridDim.x) {
-        const long long r0 = tl * kAP;
-        const int valid = (int)min((long long)kAP, P - r0);
-        // staging: the descriptor rows are the operand of product 0
-        if (net.prefetch_g) {
-            if (!tc::mbar_wait(gbar_u32, gphase)) gave_up = true;
-            gphase ^= 1u;
-            if (tid == 0) g_pending = false;
-        }
-        aborted = __syncthreads_or(gave_up) != 0;
-        if (aborted) break;
-        for (int j = 0; j * kPC < Kg; ++j) {
-            const int c0 = j * kPC + 8 * h;
-            if (c0 < Kg) {
-                float v[8];
-                const float *src = net.prefetch_g ? gbuf + p * net.g_ld + c0 : g_rows + (r0 + p) * net.g_ld + c0;
-                const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-                const float4 lo4 = p < valid ? reinterpret_cast<const float4 *>(src)[0] : zero4;
-                const float4 hi4 = p < valid ? reinterpret_cast<const float4 *>(src)[1] : zero4;
-                v[0] = lo4.x, v[1] = lo4.y, v[2] = lo4.z, v[3] = lo4.w;
-                v[4] = hi4.x, v[5] = hi4.y, v[6] = hi4.z, v[7] = hi4.w;
-                store_split8(tile, Kg, p, c0, v);
-            }
-            chunk_done(0, j, 1);
-        }
-        if (tid == 0) finish_product(0);
-        for (int x = 0; x < nprod; ++x) {
-            // product x complete: its region holds this epilogue's input, every slot is free
-            if (!tc::mbar_wait(bar, mphase)) gave_up = true;
-            mphase ^= 1u;
-            if (tid == 0) commit_pending = false;
-            tc::fence_after();
-            aborted = __syncthreads_or(gave_up) != 0;
-            if (aborted) break;
-            if (x == 0) request_g(tl + gridDim.x);  // every thread has read gbuf
-            const bool more = tl + gridDim.x < ntiles;
-            const int xn = x + 1 < nprod ? x + 1 : -1;  // the product this epilogue feeds (none after the last)
-            // the product after xn (the next tile's first after the last), whose chunks go into
-            // their slots while xn runs
-            const int yn = xn < 0 ? -1 : (xn + 1 < nprod ? xn + 1 : (more ? 0 : -1));
-            // the chunks of the product after x that did not go in while x ran: from x's last on
-            if (tid == 0) load_weights(xn >= 0 ? xn : (more ? 0 : -1), nchunks(x) - 1);
-            __syncwarp();
-            if (x == nh && tid < kAP && p < valid)
-                y_rows[r0 + p] = (eps[p] + eps[kAP + p]) + (eps[2 * kAP + p] + eps[3 * kAP + p]) +
-                                 par[net.bias_off[nh] + kWideMax];
-            const int Nx = out_w(x);
-            const uint32_t dcol = tmem + lane_base + region(x);
-            if (x < nh) {  // forward epilogue of layer x
-                const bool last = x == nh - 1;
-                const float *bias = par + net.bias_off[x];
-                const float *wl = par + net.bias_off[nh];
-                float esum = 0.f;
-                uint64_t bits = 0;
-                for (int j = 0; j * kPC < Nx; ++j) {
-                    const int c0 = j * kPC + 8 * h;
-                    if (c0 < Nx) {
-                        float z[8], v[8], bb[8], ww[8];
-                        tc::tmem_ld8(dcol + c0, z);
-                        *reinterpret_cast<float4 *>(bb) = *reinterpret_cast<const float4 *>(bias + c0);
-                        *reinterpret_cast<float4 *>(bb + 4) = *reinterpret_cast<const float4 *>(bias + c0 + 4);
-                        if (last) {
-                            *reinterpret_cast<float4 *>(ww) = *reinterpret_cast<const float4 *>(wl + c0);
-                            *reinterpret_cast<float4 *>(ww + 4) = *reinterpret_cast<const float4 *>(wl + c0 + 4);
-                        }
-                        uint32_t b8 = 0;
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const float zz = z[k] + bb[k];
-                            const float fz = fmaxf(zz, 0.0f);
-                            if (last) {
-                                esum = fmaf(ww[k], fz, esum);
-                                v[k] = zz > 0.0f ? ww[k] : 0.0f;
-                            } else {
-                                v[k] = fz;
-                                b8 |= (zz > 0.0f ? 1u : 0u) << k;
-                            }
-                        }
-                        if (!last) bits |= (uint64_t)b8 << (8 * j);
-                        store_split8(tile, Nx, p, c0, v);
-                    }
-                    chunk_done(xn, j, yn);
-                }
-                if (last) eps[h * kAP + p] = esum;
-                else if (x == 0) m0 = bits;
-                else if (x == 1) m1 = bits;
-                else m2 = bits;
-            } else {  // backward epilogue of layer L2: dE/dh_{L2 - 1} masked by act'(z_{L2 - 1}), or dE/dg
-                const int L2 = nprod - 1 - x;
-                const uint64_t bits = L2 == 1 ? m0 : (L2 == 2 ? m1 : m2);
-                for (int j = 0; j * kPC < Nx; ++j) {
-                    const int c0 = j * kPC + 8 * h;
-                    if (c0 < Nx) {
-                        float dz[8];
-                        tc::tmem_ld8(dcol + c0, dz);
-                        if (L2 > 0) {
-                            float v[8];
-                            const uint32_t b8 = (uint32_t)(bits >> (8 * j));
-#pragma unroll
-                            for (int k = 0; k < 8; ++k) v[k] = (b8 >> k) & 1u ? dz[k] : 0.f;
-                            store_split8(tile, Nx, p, c0, v);
-                        } else if (p < valid) {
-                            float4 *dst = reinterpret_cast<float4 *>(dg_rows + (r0 + p) * net.gp + c0);
-                            dst[0] = make_float4(dz[0], dz[1], dz[2], dz[3]);
-                            dst[1] = make_float4(dz[4], dz[5], dz[6], dz[7]);
-                        }
-                    }
-                    if (xn >= 0) chunk_done(xn, j, yn);
-                }
-            }
-            if (tid == 0 && xn >= 0) finish_product(xn);
-            tc::fence_before();
-        }
-    }
-    aborted = __syncthreads_or(gave_up) != 0;
-    if (tid == 0) {
-        bool drained = true;
-        if (commit_pending) drained &= tc::mbar_wait(bar, mphase);  // no MMA may still be running
-        for (int j = 0; j < kSlots; ++j) {  // no copy, MMA or commit may still write shared memory
-            if ((w_pending >> j) & 1u) drained &= tc::mbar_wait(tc::smem_u32(&wfull[j]), (wf_phase >> j) & 1u);
-            if ((sf_pending >> j) & 1u) drained &= tc::mbar_wait(tc::smem_u32(&slot_free[j]), (sf_phase >> j) & 1u);
-        }
         if (g_pending) drained &= tc::mbar_wait(gbar_u32, gphase);
         if (aborted || !drained) atomicOr(&g_amlp_device_error, kErrMbarTimeout);
     }
@@ -1953,19 +1613,6 @@ static amlp_status wide_net(const amlp_mlp *mlp, int Kg, int g_ld, AdjNet *net) 
     net->relu_bits = mlp->act == AMLP_ACT_RELU ? 1 : 0;
     // smooth activations keep act'(z) of nh - 1 layers in TMEM beside the product region
     if (!net->relu_bits && net->zbw + (nh - 1) * net->wmax > 512) return AMLP_ERR_UNSUPPORTED;
-    // ReLU nets run k_mlp_grad_pipe: one weight slot per chunk of kPC input columns, each
-    // large enough for a forward chunk (Np x kPC) or a backward one (kPC x Kp), hi and lo
-    net->pipe = net->relu_bits;
-    if (net->pipe) {
-        net->slot_bytes = 128 * net->zbw;
-        wbytes = net->slot_bytes * ((net->zbw + kPC - 1) / kPC);
-        int wch = 0;
-        for (int k = 0; k < nh; ++k) {
-            net->wch_off[k] = wch;
-            wch += (net->kin[k] + kPC - 1) / kPC * 128 * net->nout[k];
-        }
-        if ((size_t)wch > kWeightSplitBytes) return AMLP_ERR_UNSUPPORTED;
-    }
     size_t o = align_up((size_t)2 * kAP * net->zbw * 2, 128);  // operand tile, bf16 hi + lo
     net->wbuf_off = (int)o;
     o += align_up((size_t)wbytes, 128);
@@ -1984,7 +1631,7 @@ static amlp_status wide_net(const amlp_mlp *mlp, int Kg, int g_ld, AdjNet *net) 
 extern "C" amlp_status amlp_adjoint_workspace_bytes(long long cap, size_t *bytes) {
     if (cap < 0 || !bytes) return AMLP_ERR_INVALID_ARG;
     *bytes = align_up((size_t)cap * kGRow * 4) + align_up((size_t)cap * kGP * 4) + align_up((size_t)cap * 4) +
-             2 * align_up(kWeightSplitBytes) + align_up(adj_a_bytes(cap)) + 256;
+             align_up(kWeightSplitBytes) + align_up(adj_a_bytes(cap)) + 256;
     return AMLP_OK;
 }
 
@@ -2026,24 +1673,6 @@ static amlp_status launch_direct(K kernel, long long cap, int npts, cudaStream_t
     return AMLP_OK;
 }
 
-// The net stage of the wide path: the weight splits, then k_mlp_grad_pipe for
-// ReLU nets or k_mlp_grad.
-static amlp_status launch_mlp_grad(const AdjNet &net, const amlp_mlp *mlp, const float *g_rows,
-                                   const long long *d_npairs, long long cap, char *wsplit, char *wchunks,
-                                   float *y_rows, float *dg_rows, cudaStream_t s) {
-    k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit, net.pipe ? wchunks : nullptr);
-    if (net.pipe) {
-        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, net.smem));
-        k_mlp_grad_pipe<<<kNumSM, kMThreads, net.smem, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, wchunks,
-                                                             y_rows, dg_rows);
-    } else {
-        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, net.smem));
-        k_mlp_grad<<<kNumSM, kMThreads, net.smem, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows,
-                                                        dg_rows);
-    }
-    return AMLP_OK;
-}
-
 // Stage events of the wide path (amlp_stage_timing): one set for the library,
 // recorded by the last call on its stream.
 static bool g_stage_timing = false;
@@ -2081,8 +1710,8 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
         float *dg_rows = c.take<float>((size_t)cap * gp);
         float *y_rows = c.take<float>((size_t)cap);
         char *wsplit = c.take<char>(kWeightSplitBytes);
-        char *wchunks = c.take<char>(kWeightSplitBytes);
         if (!c.ok()) return AMLP_ERR_WORKSPACE;
+        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, net.smem));
         const int npts = nep->npts;
         auto fwd = k2 ? direct::k_desc_direct_fwd<11, 11, 10> : direct::k_desc_direct_fwd<11, 9, 4>;
         auto bwd = k2 ? direct::k_desc_direct_bwd<11, 11, 10> : direct::k_desc_direct_bwd<11, 9, 4>;
@@ -2091,7 +1720,8 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
                                 (const float *)nep->d_pts, npts, inv_rc, g_rows, grow)))
             return st;
         stage_mark(1, s);
-        if ((st = launch_mlp_grad(net, mlp, g_rows, d_npairs, cap, wsplit, wchunks, y_rows, dg_rows, s))) return st;
+        k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
+        k_mlp_grad<<<kNumSM, kMThreads, net.smem, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
         stage_mark(2, s);
         if ((st = launch_direct(bwd, cap, npts, s, d_pos, d_quat, box, d_pairs, d_npairs, cap,
                                 (const float *)nep->d_pts, npts, inv_rc, nep->en_min, rng, (const float *)dg_rows, gp,
@@ -2106,10 +1736,10 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     float *dg_rows = c.take<float>((size_t)cap * kGP);
     float *y_rows = c.take<float>((size_t)cap);
     char *wsplit = c.take<char>(kWeightSplitBytes);
-    char *wchunks = c.take<char>(kWeightSplitBytes);
     float *a_rows = c.take<float>(adj_a_bytes(cap) / 4);
     const int npts = nep->npts;
     const size_t smem_desc = wide_desc_smem(npts);
+    const size_t smem_mlp = (size_t)net.smem;
     if (smem_desc > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
     const bool multi = d_rep != nullptr;
@@ -2117,12 +1747,14 @@ static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, 
     auto bwd = multi ? k_adj_desc<Cfg, true, true> : k_adj_desc<Cfg, false, true>;
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
     AMLP_CHECK_CUDA(cudaFuncSetAttribute(bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_desc));
+    AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mlp));
     stage_mark(0, s);
     fwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, g_rows, kGRow, nullptr, nullptr, nullptr, clip, d_F,
                                              d_T, d_pe, d_rep, d_rp, a_rows);
     stage_mark(1, s);
-    if ((st = launch_mlp_grad(net, mlp, g_rows, d_npairs, cap, wsplit, wchunks, y_rows, dg_rows, s))) return st;
+    k_split_weights<<<64, 256, 0, s>>>(net, mlp->d_w, wsplit);
+    k_mlp_grad<<<kNumSM, kMThreads, smem_mlp, s>>>(g_rows, d_npairs, cap, net, mlp->d_w, wsplit, y_rows, dg_rows);
     stage_mark(2, s);
     bwd<<<kNumSM, kAThreads, smem_desc, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts, npts, inv_rc,
                                              nep->en_min, rng, nullptr, kGP, dg_rows, y_rows, d_wt, clip, d_F, d_T,

@@ -139,11 +139,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int limi
     return false;
 }
 
-// One plain arrival on the mbarrier.
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
 // One arrival on the mbarrier that also expects `bytes` of asynchronous copies.
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
