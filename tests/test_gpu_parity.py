@@ -531,3 +531,37 @@ def test_adjoint_wide_nets_to_160_and_four_layers(widths, act):
         err = np.linalg.norm(got - want) / np.linalg.norm(want)
         assert err <= 1e-3, err
     assert abs(pe - ref["E"].sum()) <= 1e-4 * max(1.0, np.abs(ref["E"]).sum())
+
+
+@pytest.mark.parametrize("shape_name,hyp", [("th_v1", (10, 8, 4)), ("cube26", (10, 8, 4))])
+def test_stage_timing_of_the_wide_path(shape_name, hyp):
+    """amlp_stage_timing / amlp_stage_times: three positive stage times whose sum
+    stays within the whole call's event time, and the same forces with the
+    events on as without them."""
+    import ctypes
+    from amlp import _lib
+    from amlp.engine import EnergyNet
+    L = {"th_v1": 24.0}.get(shape_name)
+    s = make_state(400, shape_name, 0.1 if L else 0.45, seed=3, L=L)
+    shape = SHAPES[shape_name]
+    vp, _ = gh.nlist(s.pos, s.L, shape["cutoff"] + 2.0)
+    pairs = gh.pair_filter(s.pos, s.L, shape["cutoff"], vp)
+    net = EnergyNet.xavier(47, (150, 150), "relu", seed=4, device="cpu")
+    ref = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, hyp, net.layers, "relu",
+                          method="amlp_forces_adjoint_wide")
+    _lib.call("amlp_stage_timing", 1)
+    try:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        got = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, hyp, net.layers, "relu",
+                              method="amlp_forces_adjoint_wide")
+        e1.record()
+        torch.cuda.synchronize()
+        ms = (ctypes.c_float * 3)()
+        _lib.call("amlp_stage_times", ms)
+    finally:
+        _lib.call("amlp_stage_timing", 0)
+    assert all(m > 0.0 for m in ms)
+    assert sum(ms) <= e0.elapsed_time(e1)
+    for a, b in zip(got[:2], ref[:2]):
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-5 * max(1.0, np.abs(b).max()))
