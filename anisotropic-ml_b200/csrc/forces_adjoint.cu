@@ -1239,8 +1239,8 @@ __global__ void k_split_weights(AdjNet net, const float *w, char *dst) {
 // each hidden layer but the last for the backward: for ReLU (derivative 0 or
 // 1) as bits in registers, otherwise in TMEM after the product region.
 // Outputs per row: y = net(g) and dE/dg (net.gp floats).
-constexpr int kMQ = 4;                  // column groups of the k_mlp_grad epilogues
-constexpr int kMThreads = kMQ * kAP;    // 512
+constexpr int kMQ = 8;                  // column groups of the k_mlp_grad epilogues
+constexpr int kMThreads = kMQ * kAP;    // 1024
 static_assert(kWideMax <= 8 * kMQ * 8, "a thread's 8-column chunks of a layer fit one 64-bit mask");
 __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
                                                           AdjNet net, const float *w, const char *wsplit,
@@ -1411,8 +1411,12 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             aborted = __syncthreads_or(gave_up) != 0;
         }
         if (tid < kAP && p < valid)
-            y_rows[r0 + p] = (eps[p] + eps[kAP + p]) + (eps[2 * kAP + p] + eps[3 * kAP + p]) +
-                             par[net.bias_off[net.nh] + kWideMax];
+        {
+            float ysum = par[net.bias_off[net.nh] + kWideMax];
+#pragma unroll
+            for (int g = 0; g < kMQ; ++g) ysum += eps[g * kAP + p];
+            y_rows[r0 + p] = ysum;
+        }
         // backward: delta_{k-1} = (delta_k W_k) * act'(z_{k-1}); dE/dg = delta_0 W_0
         for (int L2 = net.nh - 1; L2 >= 0; --L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
