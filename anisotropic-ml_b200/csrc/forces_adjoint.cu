@@ -733,14 +733,21 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *po
                 for (int ch = 0; ch < 2; ++ch) {
                     if (g + ch < nch) {
                         const int c0 = cb + 8 * (g + ch);
-                        float v[8], dv[8];
+                        float v[8], dv[8], bb[8], ww[8];
+                        // bias_off is a multiple of 16 floats and c0 of 8: 16-byte loads
+                        *reinterpret_cast<float4 *>(bb) = *reinterpret_cast<const float4 *>(bias + c0);
+                        *reinterpret_cast<float4 *>(bb + 4) = *reinterpret_cast<const float4 *>(bias + c0 + 4);
+                        if (last) {
+                            *reinterpret_cast<float4 *>(ww) = *reinterpret_cast<const float4 *>(wl + c0);
+                            *reinterpret_cast<float4 *>(ww + 4) = *reinterpret_cast<const float4 *>(wl + c0 + 4);
+                        }
 #pragma unroll
                         for (int k = 0; k < 8; ++k) {
-                            float zz = z[8 * ch + k] + bias[c0 + k], fz, dfz;
+                            float zz = z[8 * ch + k] + bb[k], fz, dfz;
                             act_pair(net.act, zz, fz, dfz);
                             if (last) {
-                                esum = fmaf(wl[c0 + k], fz, esum);
-                                v[k] = wl[c0 + k] * dfz;
+                                esum = fmaf(ww[k], fz, esum);
+                                v[k] = ww[k] * dfz;
                             } else {
                                 v[k] = fz;
                                 dv[k] = dfz;
