@@ -1246,8 +1246,8 @@ __global__ void k_split_weights(AdjNet net, const float *w, char *dst) {
 // each hidden layer but the last for the backward: for ReLU (derivative 0 or
 // 1) as bits in registers, otherwise in TMEM after the product region.
 // Outputs per row: y = net(g) and dE/dg (net.gp floats).
-constexpr int kMQ = 8;                  // column groups of the k_mlp_grad epilogues
-constexpr int kMThreads = kMQ * kAP;    // 1024
+constexpr int kMQ = 4;                  // column groups of the k_mlp_grad epilogues
+constexpr int kMThreads = kMQ * kAP;    // 512
 static_assert(kWideMax <= 8 * kMQ * 8, "a thread's 8-column chunks of a layer fit one 64-bit mask");
 __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, const long long *d_np, long long cap,
                                                           AdjNet net, const float *w, const char *wsplit,
