@@ -18,7 +18,8 @@ Systems of one shape share a bucket, buffers of a fixed capacity:
 The server advances all buckets in segments of ``segment`` steps (100, the
 Verlet rebuild period of the reference, ``Sim.py:87``). Each segment:
 - rebuilds every system's Verlet list;
-- replays one CUDA graph holding all steps of all buckets. It is captured once
+- replays one CUDA graph holding all steps of all buckets, one branch per
+  bucket so that the buckets' kernels run concurrently. It is captured once
   and captured again only when a bucket's capacity grows, so admissions and
   departures cost a few small copies, not a capture;
 - then admits new arrivals and retires finished systems. This is the only time
@@ -386,7 +387,14 @@ class Server:
         self.used = 0
         self._graph = None
         self._graph_key = None
+        self._branches = {}
         self.results = {}
+
+    def _branch(self, b) -> torch.cuda.Stream:
+        """The side stream that bucket b's steps are captured on."""
+        if id(b) not in self._branches:
+            self._branches[id(b)] = torch.cuda.Stream(device=self.device)
+        return self._branches[id(b)]
 
     def _admit(self, req: Request, now: float) -> _System:
         shape = get_shape(req.shape)
@@ -413,9 +421,16 @@ class Server:
             s.wait_stream(torch.cuda.current_stream())
             with torch.cuda.stream(s):
                 with torch.cuda.graph(g, stream=s):
-                    for _ in range(steps):
-                        for b in self.buckets.values():
-                            b.step_kernels()
+                    # one branch per bucket: the buckets share no buffer, so their steps run
+                    # concurrently and fill each other's idle SMs (a persistent force kernel with
+                    # few tiles leaves most of the GPU free at its tail)
+                    for b in self.buckets.values():
+                        bs = self._branch(b)
+                        bs.wait_stream(s)
+                        with torch.cuda.stream(bs):
+                            for _ in range(steps):
+                                b.step_kernels()
+                        s.wait_stream(bs)
             torch.cuda.current_stream().wait_stream(s)
             torch.cuda.synchronize()
             self._graph, self._graph_key = g, key
