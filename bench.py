@@ -94,6 +94,9 @@ DRAM_BYTES_PER_PAIR["adjoint_wide"] = (4.141824e6 + 350.520064e6 + 79.480064e6 +
 # pair at 32,768 th_v1 bodies (87,256 pairs; the profiles give the commands). The descriptor rows
 # depend on D, not on the net or the shape.
 STAGE_DRAM_BYTES_PER_PAIR = {
+    # the harmonic-form passes (clouds of more than 12 points), 32,768 cyl24 bodies, 381,342 pairs
+    ("k_adj_desc (forward)", 47): (4.141824e6 + 350.520064e6) / 381342,
+    ("k_adj_desc (backward)", 47): (409.184e6 + 5.303552e6) / 381342,
     ("k_mlp_grad", 47): 18.56128e6 / 87256,
     ("k_mlp_grad", 121): (46.54e6 + 0.39e6) / 87257,
     ("k_desc_direct_fwd", 47): 1.64e6 / 87256,
