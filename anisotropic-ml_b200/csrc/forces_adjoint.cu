@@ -1360,9 +1360,11 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
         for (int L2 = 0; L2 < net.nh; ++L2) {
             const int Kp = net.kin[L2], Np = net.nout[L2];
             request(L2);
-            tc::fence_async_smem();
-            aborted = __syncthreads_or(gave_up) != 0;
-            if (L2 == 0) request_g(tl + gridDim.x);  // gbuf has been read: prefetch the next tile
+            if (L2 == 0) {  // later layers start right after the previous epilogue's barrier
+                tc::fence_async_smem();
+                aborted = __syncthreads_or(gave_up) != 0;
+                request_g(tl + gridDim.x);  // gbuf has been read: prefetch the next tile
+            }
             if (tid == 0) ensure();
             if (tid == 0 && !aborted && !gave_up) {
                 tc::fence_after();
@@ -1425,11 +1427,9 @@ __global__ void __launch_bounds__(kMThreads, 1) k_mlp_grad(const float *g_rows, 
             y_rows[r0 + p] = ysum;
         }
         // backward: delta_{k-1} = (delta_k W_k) * act'(z_{k-1}); dE/dg = delta_0 W_0
-        for (int L2 = net.nh - 1; L2 >= 0; --L2) {
+        for (int L2 = net.nh - 1; L2 >= 0; --L2) {  // each layer starts right after the previous barrier
             const int Kp = net.kin[L2], Np = net.nout[L2];
             request(L2);
-            tc::fence_async_smem();
-            aborted = __syncthreads_or(gave_up) != 0;
             if (tid == 0) ensure();
             if (tid == 0 && !aborted && !gave_up) {
                 tc::fence_after();
