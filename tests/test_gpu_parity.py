@@ -565,3 +565,30 @@ def test_stage_timing_of_the_wide_path(shape_name, hyp):
     assert sum(ms) <= e0.elapsed_time(e1)
     for a, b in zip(got[:2], ref[:2]):
         np.testing.assert_allclose(a, b, rtol=0, atol=1e-5 * max(1.0, np.abs(b).max()))
+
+
+def test_direct_form_large_clouds_and_empty_lists():
+    """The direct-form passes at the largest clouds they take (cube26 with the
+    hypers (10, 10, 10): 52 points, 52 KB of shared memory per block, above the
+    default 48 KB), against the FP64 exact derivative; and an empty pair list,
+    which leaves the forces zero."""
+    from amlp.engine import EnergyNet
+    from oracle import adjoint
+    s = make_state(200, "cube26", 0.45, seed=21)
+    shape = SHAPES["cube26"]
+    vp, _ = gh.nlist(s.pos, s.L, shape["cutoff"] + 2.0)
+    pairs = gh.pair_filter(s.pos, s.L, shape["cutoff"], vp)[:300]
+    hyp = (10, 10, 10)
+    g = gh.pair_descriptors(s.pos, s.orient, s.L, pairs, shape, hyp, ld=124)
+    _, _, t = nep.min_image_filter(s.pos, pairs, s.L, shape["cutoff"], np.float64)
+    c1, _ = nep.pair_clouds(s.orient, pairs, t, shape["pts"], np.float64)
+    _check_desc(g[:, :121], nep.descriptor(c1, hyp, shape["nep_cutoff"], np.float64))
+    net = EnergyNet.xavier(121, (64, 64), "tanh", seed=22, device="cpu")
+    F, T, pe = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, hyp, net.layers, "tanh",
+                               method="amlp_forces_adjoint_wide")
+    ref = adjoint.exact_pair_forces(s.pos, s.orient, pairs, s.L, shape, hyp, net.layers, "tanh")
+    for got, want in ((F, ref["forces"]), (T, ref["torques"])):
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-3
+    F0, T0, pe0 = gh.fused_forces(s.pos, s.orient, s.L, pairs[:0], shape, hyp, net.layers, "tanh",
+                                  method="amlp_forces_adjoint_wide")
+    assert not F0.any() and not T0.any() and pe0 == 0.0
