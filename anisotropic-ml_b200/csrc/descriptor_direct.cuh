@@ -328,7 +328,9 @@ __global__ void __launch_bounds__(kThreads) k_desc_direct_bwd(const float *pos, 
                     be = fmaf(fa[n] * fb[n], Hp[n], be);
                 }
                 // a: 2 alpha_ab rhat_a + 2 beta (rhat_b - c rhat_a) / d_a; b likewise
-                const float wa = 2.0f * be * inv_da, wb = 2.0f * be / B.w;
+                // 2 beta / d_b with the hardware reciprocal (a few ulp; the exact quotient costs an
+                // IEEE division per point pair)
+                const float wa = 2.0f * be * inv_da, wb = __fdividef(2.0f * be, B.w);
                 const float ca = fmaf(-wa, c, 2.0f * al_ab), cb = fmaf(-wb, c, 2.0f * al_ba);
                 gx += fmaf(ca, A.x, wa * B.x), gy += fmaf(ca, A.y, wa * B.y), gz += fmaf(ca, A.z, wa * B.z);
                 add_grad(b, B, fmaf(cb, B.x, wb * A.x), fmaf(cb, B.y, wb * A.y), fmaf(cb, B.z, wb * A.z));
