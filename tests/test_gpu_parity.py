@@ -568,10 +568,14 @@ def test_stage_timing_of_the_wide_path(shape_name, hyp):
 
 
 def test_direct_form_large_clouds_and_empty_lists():
-    """The direct-form passes at the largest clouds they take (cube26 with the
-    hypers (10, 10, 10): 52 points, 52 KB of shared memory per block, above the
-    default 48 KB), against the FP64 exact derivative; and an empty pair list,
-    which leaves the forces zero."""
+    """The direct-form passes at large clouds (cube26 with the hypers (10, 10,
+    10): 52 points, 52 KB of shared memory per block, above the default 48 KB),
+    against the FP64 descriptor and exact derivative; and an empty pair list,
+    which leaves the forces zero. Each thread sums the 1,326 point pairs of a
+    52-point cloud in one FP32 register, and the Legendre terms cancel, so the
+    descriptor is checked against each row's largest entry (1e-5 of it) rather
+    than entry by entry (the reference's C100 shapes, 8 to 14 points, meet the
+    entry-wise bar in test_pair_descriptors_vs_fp64)."""
     from amlp.engine import EnergyNet
     from oracle import adjoint
     s = make_state(200, "cube26", 0.45, seed=21)
@@ -582,7 +586,10 @@ def test_direct_form_large_clouds_and_empty_lists():
     g = gh.pair_descriptors(s.pos, s.orient, s.L, pairs, shape, hyp, ld=124)
     _, _, t = nep.min_image_filter(s.pos, pairs, s.L, shape["cutoff"], np.float64)
     c1, _ = nep.pair_clouds(s.orient, pairs, t, shape["pts"], np.float64)
-    _check_desc(g[:, :121], nep.descriptor(c1, hyp, shape["nep_cutoff"], np.float64))
+    g64 = nep.descriptor(c1, hyp, shape["nep_cutoff"], np.float64)
+    row_scale = np.abs(g64).max(axis=1, keepdims=True)
+    assert (np.abs(g[:, :121] - g64) / row_scale).max() <= 1e-5
+    assert np.all(g[:, 121:] == 0.0)
     net = EnergyNet.xavier(121, (64, 64), "tanh", seed=22, device="cpu")
     F, T, pe = gh.fused_forces(s.pos, s.orient, s.L, pairs, shape, hyp, net.layers, "tanh",
                                method="amlp_forces_adjoint_wide")
