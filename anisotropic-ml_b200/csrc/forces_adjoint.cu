@@ -1691,8 +1691,11 @@ static bool g_stage_recorded = false;
 static cudaEvent_t g_stage_ev[4];
 
 static void stage_mark(int k, cudaStream_t s) {
-    if (g_stage_timing) cudaEventRecord(g_stage_ev[k], s);
-    if (g_stage_timing && k == 3) g_stage_recorded = true;
+    if (!g_stage_timing) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;  // not in graphs
+    cudaEventRecord(g_stage_ev[k], s);
+    if (k == 3) g_stage_recorded = true;
 }
 
 static amlp_status launch_adjoint_wide(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
