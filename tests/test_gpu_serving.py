@@ -91,3 +91,28 @@ def test_stream_runs_and_reports():
     s = srv.run(reqs).summary()
     assert s["requests"] == 8 and s["particle_steps"] == sum(r.n * 30 for r in reqs)
     assert s["segment_ms_p99"] >= s["segment_ms_p50"] > 0
+
+
+def test_wide_nets_same_alone_and_in_the_mix():
+    """Served systems whose nets are wider than the fused kernel takes (128 x 2
+    SiLU, the precision workload's size) run on the multi-system wide path
+    (amlp_multi_forces_adjoint_wide, harmonic-form descriptor passes); each
+    result equals the system run alone through System.step within the rounding
+    of the force atomics, after one step."""
+    nets = {}
+    for k, name in enumerate(("cube26", "tetra16", "cyl24")):
+        net = EnergyNet.xavier(47, (128, 128), "silu", seed=k + 30, device="cpu")
+        nets[name] = EnergyNet(net.layers, "silu", DEV)
+    reqs = _mix()
+    for r in reqs:
+        r.steps = 1
+    srv = Server(nets, hbm_budget=8 << 30, segment=1, device=DEV)
+    srv.run(reqs, keep_states=True)
+    assert all(b.adj_ws is not None for b in srv.buckets.values())  # the wide path
+    for r in reqs:
+        alone = _alone(r, nets[r.shape], 1)
+        mixed = srv.results[r.rid]
+        for got, ref in ((mixed.pos, alone.pos), (mixed.vel, alone.vel), (mixed.orient, alone.quat),
+                         (mixed.angmom, alone.angmom)):
+            ref = ref.cpu().numpy()
+            assert np.abs(got - ref).max() <= 2e-6 * max(1.0, np.abs(ref).max()), r.rid
