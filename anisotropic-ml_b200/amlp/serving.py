@@ -25,9 +25,11 @@ Verlet rebuild period of the reference, ``Sim.py:87``). Each segment:
 - then admits new arrivals and retires finished systems. This is the only time
   the set of systems can change.
 
-Throughput (particle-steps/s), per-segment latency percentiles (device time of
-the replay, and wall time of lists + replay) and per-request completion
-latencies are recorded.
+Throughput (particle-steps/s over the wall time), per-segment latency
+percentiles (device time of the replay, and wall time of lists + replay) and
+per-request completion latencies are recorded. Admissions and request latencies
+run on the device time of the segments (plus jumps over idle gaps), so a seeded
+stream is served the same way every run.
 """
 from __future__ import annotations
 
@@ -377,7 +379,10 @@ class Server:
     """Continuous-batching NVT server (see the module docstring)."""
 
     def __init__(self, nets: dict, hbm_budget: int, dt: float = 0.005, segment: int = 100, device="cuda",
-                 hypers: Hypers | None = None, use_graphs: bool = True):
+                 hypers: Hypers | None = None, use_graphs: bool = True, clock: str = "device"):
+        if clock not in ("device", "wall"):
+            raise ValueError(f"clock must be 'device' or 'wall', not {clock!r}")
+        self.clock = clock
         self.device = torch.device(device)
         self.hypers = hypers or Hypers()
         self.buckets = {k: _Bucket(k, v, self.hypers, dt, self.device) for k, v in nets.items()}
@@ -451,14 +456,26 @@ class Server:
         return ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3
 
     def run(self, requests: list[Request], keep_states: bool = False) -> ServeStats:
-        """Serve `requests` (arrival times in seconds from now) to completion."""
+        """Serve `requests` (arrival times in seconds from the start) to completion.
+
+        The server's clock (admissions, request latencies) is the device time of
+        the segments served so far, plus the jumps over idle gaps to the next
+        arrival: it does not see host work or graph captures, so the same stream
+        gives the same admissions, resident sets and segment sizes from run to
+        run. ``clock="wall"`` uses the host's clock instead. The aggregate
+        throughput is over the wall time either way."""
         self.stats = ServeStats()
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         active: list[_System] = []
         t0 = time.perf_counter()
         shift = 0.0
+        device_s = 0.0
+
+        def clock() -> float:
+            return (device_s if self.clock == "device" else time.perf_counter() - t0) + shift
+
         while pending or active:
-            now = time.perf_counter() - t0 + shift
+            now = clock()
             if not active and pending and pending[0].arrival > now:
                 shift += pending[0].arrival - now    # idle: jump to the next arrival
                 now = pending[0].arrival
@@ -482,6 +499,7 @@ class Server:
             self.stats.max_active = max(self.stats.max_active, len(active))
             steps = min(self.segment, min(s.req.steps - s.done for s in active))
             ms, wall_ms = self._segment(steps)
+            device_s += ms / 1e3
             self.stats.segments_ms.append(ms * self.segment / steps)
             self.stats.segments_wall_ms.append(wall_ms * self.segment / steps)
             self.stats.body_steps += steps * sum(s.req.n for s in active)
@@ -491,7 +509,7 @@ class Server:
                 if s.done >= s.req.steps:
                     finished.append(s)
             if finished:
-                now = time.perf_counter() - t0 + shift
+                now = clock()
                 for name, b in self.buckets.items():
                     gone = [s for s in b.systems if s in finished]
                     if gone:
