@@ -359,12 +359,16 @@ class ServeStats:
     graphs_captured: int = 0
 
     segments_wall_ms: list = field(default_factory=list)
+    server_clock_s: float = 0.0
 
     def summary(self) -> dict:
         seg = np.asarray(self.segments_ms) if self.segments_ms else np.zeros(1)
         wall = np.asarray(self.segments_wall_ms) if self.segments_wall_ms else np.zeros(1)
         lat = np.asarray([c[1] for c in self.completions]) if self.completions else np.zeros(1)
         return {"particle_steps_per_s": self.body_steps / self.wall_s if self.wall_s else 0.0,
+                "particle_steps_per_s_server_clock": (self.body_steps / self.server_clock_s
+                                                      if self.server_clock_s else 0.0),
+                "server_clock_s": self.server_clock_s,
                 "segment_ms_p50": float(np.percentile(seg, 50)), "segment_ms_p99": float(np.percentile(seg, 99)),
                 "segment_wall_ms_p50": float(np.percentile(wall, 50)),
                 "segment_wall_ms_p99": float(np.percentile(wall, 99)),
@@ -522,6 +526,7 @@ class Server:
                             self.used -= s.mem
                 active = [s for s in active if s not in finished]
         self.stats.wall_s = time.perf_counter() - t0
+        self.stats.server_clock_s = clock()
         return self.stats
 
 
