@@ -66,13 +66,6 @@ class Replica(ctypes.Structure):
                 ("box", ctypes.c_float), ("nve", ctypes.c_int), ("pad", ctypes.c_int * 3)]
 
 
-class ShapeBatch(ctypes.Structure):
-    _fields_ = [("d_pos", ctypes.c_void_p), ("d_quat", ctypes.c_void_p), ("d_rep", ctypes.c_void_p),
-                ("d_rp", ctypes.c_void_p), ("d_pairs", ctypes.c_void_p), ("d_npairs", ctypes.c_void_p),
-                ("cap", ctypes.c_longlong), ("nep", ctypes.POINTER(Nep)), ("mlp", ctypes.POINTER(Mlp)),
-                ("d_F", ctypes.c_void_p), ("d_T", ctypes.c_void_p), ("d_pe", ctypes.c_void_p)]
-
-
 class SimConfig(ctypes.Structure):
     """``amlp_sim_config``: parameters of a simulation handle."""
     _fields_ = [("n", ctypes.c_int), ("nrad", ctypes.c_int), ("nang", ctypes.c_int), ("lmax", ctypes.c_int),
@@ -128,7 +121,6 @@ SIGNATURES = {
     "amlp_adjoint_workspace_bytes": [_LL, _PSZ],
     "amlp_forces_adjoint_wide": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp), _P, _P, _P,
                                  _P, _SZ, _P],
-    "amlp_multi_forces_adjoint_shapes": [ctypes.POINTER(ShapeBatch), _I, _P],
     "amlp_multi_forces_adjoint_wide": [_P, _P, _P, _P, _P, _P, _LL, ctypes.POINTER(Nep), ctypes.POINTER(Mlp),
                                        _P, _P, _P, _P, _SZ, _P],
     "amlp_pair_descriptors": [_P, _P, _F, _P, _P, _LL, ctypes.POINTER(Nep), _P, _I, _P],

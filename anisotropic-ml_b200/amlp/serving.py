@@ -13,17 +13,13 @@ Systems of one shape share a bucket, buffers of a fixed capacity:
 - one time step of a bucket is: the pair filter, the adjoint force kernel
   (net on the tensor cores), and the two NVT halves, each a single launch over
   the bucket's capacity (``amlp_multi_*``), with the same arguments whatever
-  systems are resident;
-- when every bucket's net fits the fused kernel, one adjoint launch serves all
-  buckets (``amlp_multi_forces_adjoint_shapes``: each tile of 128 pairs is
-  dispatched to its bucket's shape and net), so a step is the buckets' filters,
-  one force launch and the buckets' NVT halves.
+  systems are resident.
 
 The server advances all buckets in segments of ``segment`` steps (100, the
 Verlet rebuild period of the reference, ``Sim.py:87``). Each segment:
 - rebuilds every system's Verlet list;
-- replays one CUDA graph holding all steps of all buckets, the buckets' own
-  kernels on parallel branches so that they run concurrently. It is captured once
+- replays one CUDA graph holding all steps of all buckets, one branch per
+  bucket so that the buckets' kernels run concurrently. It is captured once
   and captured again only when a bucket's capacity grows, so admissions and
   departures cost a few small copies, not a capture;
 - then admits new arrivals and retires finished systems. This is the only time
@@ -330,12 +326,6 @@ class _Bucket:
 
     def step_kernels(self) -> None:
         """One step of every system of the bucket: the same launches whatever the active set."""
-        self.pre_forces()
-        self.forces()
-        self.post_forces()
-
-    def pre_forces(self) -> None:
-        """Zeroed force, torque and energy sums, then the pair filter."""
         st = _stream()
         self.F.zero_()
         self.T.zero_()
@@ -343,10 +333,6 @@ class _Bucket:
         call("amlp_multi_pair_filter", self.pos.data_ptr(), self.rep.data_ptr(), self.rp.data_ptr(),
              float(self.shape.cutoff), self.vpairs.data_ptr(), self.nv.data_ptr(), self.cap, self.fpairs.data_ptr(),
              self.nf.data_ptr(), self.f_ws.data_ptr(), self.f_ws.numel(), st)
-
-    def forces(self) -> None:
-        """This bucket's adjoint force pass alone."""
-        st = _stream()
         args = [self.pos.data_ptr(), self.quat.data_ptr(), self.rep.data_ptr(), self.rp.data_ptr(),
                 self.fpairs.data_ptr(), self.nf.data_ptr(), self.cap, ctypes.byref(self.nep),
                 ctypes.byref(self.net.struct), self.F.data_ptr(), self.T.data_ptr(), self.pe.data_ptr()]
@@ -354,17 +340,6 @@ class _Bucket:
             call("amlp_multi_forces_adjoint", *args, st)
         else:
             call("amlp_multi_forces_adjoint_wide", *args, self.adj_ws.data_ptr(), self.adj_ws.numel(), st)
-
-    def shape_batch(self) -> "_lib.ShapeBatch":
-        """This bucket as one entry of amlp_multi_forces_adjoint_shapes."""
-        return _lib.ShapeBatch(self.pos.data_ptr(), self.quat.data_ptr(), self.rep.data_ptr(), self.rp.data_ptr(),
-                               self.fpairs.data_ptr(), self.nf.data_ptr(), self.cap, ctypes.pointer(self.nep),
-                               ctypes.pointer(self.net.struct), self.F.data_ptr(), self.T.data_ptr(),
-                               self.pe.data_ptr())
-
-    def post_forces(self) -> None:
-        """Both NVT halves."""
-        st = _stream()
         call("amlp_multi_nvt_step_two", self.vel.data_ptr(), self.accel.data_ptr(), self.F.data_ptr(),
              self.mass.data_ptr(), self.quat.data_ptr(), self.T.data_ptr(), self.angmom.data_ptr(),
              self.dp.data_ptr(), self.rep.data_ptr(), self.body_cap, self.sys_cap, self.rp.data_ptr(),
@@ -408,12 +383,10 @@ class Server:
     """Continuous-batching NVT server (see the module docstring)."""
 
     def __init__(self, nets: dict, hbm_budget: int, dt: float = 0.005, segment: int = 100, device="cuda",
-                 hypers: Hypers | None = None, use_graphs: bool = True, clock: str = "device",
-                 merge_forces: bool = True):
+                 hypers: Hypers | None = None, use_graphs: bool = True, clock: str = "device"):
         if clock not in ("device", "wall"):
             raise ValueError(f"clock must be 'device' or 'wall', not {clock!r}")
         self.clock = clock
-        self.merge_forces = merge_forces
         self.device = torch.device(device)
         self.hypers = hypers or Hypers()
         self.buckets = {k: _Bucket(k, v, self.hypers, dt, self.device) for k, v in nets.items()}
@@ -425,27 +398,6 @@ class Server:
         self._graph_key = None
         self._branches = {}
         self.results = {}
-
-    def _merged(self) -> bool:
-        """Whether one adjoint launch serves every bucket (all on the fused kernel, at most four)."""
-        return self.merge_forces and 1 < len(self.buckets) <= 4 and all(
-            b.adj_ws is None for b in self.buckets.values())
-
-    def _merged_forces(self) -> None:
-        """The adjoint force pass of every bucket in one launch (amlp_multi_forces_adjoint_shapes)."""
-        bl = list(self.buckets.values())
-        arr = (_lib.ShapeBatch * len(bl))(*[b.shape_batch() for b in bl])
-        call("amlp_multi_forces_adjoint_shapes", arr, len(bl), _stream())
-
-    def _on_branches(self, s: torch.cuda.Stream, fn) -> None:
-        """fn(bucket) for every bucket, each on its own side stream forked from and joined back into s."""
-        for b in self.buckets.values():
-            bs = self._branch(b)
-            bs.wait_stream(s)
-            with torch.cuda.stream(bs):
-                fn(b)
-        for b in self.buckets.values():
-            s.wait_stream(self._branch(b))
 
     def _branch(self, b) -> torch.cuda.Stream:
         """The side stream that bucket b's steps are captured on."""
@@ -467,45 +419,27 @@ class Server:
             self._graph = None
             for b in self.buckets.values():
                 b.rebuild_lists()
-            # warm-up step: sets the kernels' attributes outside the capture; the state is put back
-            snaps = {id(b): [t.clone() for t in (b.pos, b.quat, b.vel, b.angmom, b.th)] for b in self.buckets.values()}
-            if self._merged():
-                for b in self.buckets.values():
-                    b.pre_forces()
-                self._merged_forces()
-                for b in self.buckets.values():
-                    b.post_forces()
-            else:
-                for b in self.buckets.values():
-                    b.step_kernels()
-            torch.cuda.synchronize()
-            for b in self.buckets.values():
-                for t, v in zip((b.pos, b.quat, b.vel, b.angmom, b.th), snaps[id(b)]):
+            for b in self.buckets.values():   # warm-up launch sets kernel attributes outside capture
+                snap = [t.clone() for t in (b.pos, b.quat, b.vel, b.angmom, b.th)]
+                b.step_kernels()
+                torch.cuda.synchronize()
+                for t, v in zip((b.pos, b.quat, b.vel, b.angmom, b.th), snap):
                     t.copy_(v)
             g = torch.cuda.CUDAGraph()
             s = torch.cuda.Stream()
             s.wait_stream(torch.cuda.current_stream())
             with torch.cuda.stream(s):
                 with torch.cuda.graph(g, stream=s):
-                    if self._merged():
-                        # per step: the buckets' filters on parallel branches, one adjoint launch
-                        # for all buckets (their tiles spread over every SM), the NVT halves on
-                        # parallel branches again
-                        for _ in range(steps):
-                            self._on_branches(s, lambda b: b.pre_forces())
-                            self._merged_forces()
-                            self._on_branches(s, lambda b: b.post_forces())
-                    else:
-                        # one branch per bucket: the buckets share no buffer, so their steps run
-                        # concurrently and fill each other's idle SMs (a persistent force kernel
-                        # with few tiles leaves most of the GPU free at its tail)
-                        for b in self.buckets.values():
-                            bs = self._branch(b)
-                            bs.wait_stream(s)
-                            with torch.cuda.stream(bs):
-                                for _ in range(steps):
-                                    b.step_kernels()
-                            s.wait_stream(bs)
+                    # one branch per bucket: the buckets share no buffer, so their steps run
+                    # concurrently and fill each other's idle SMs (a persistent force kernel with
+                    # few tiles leaves most of the GPU free at its tail)
+                    for b in self.buckets.values():
+                        bs = self._branch(b)
+                        bs.wait_stream(s)
+                        with torch.cuda.stream(bs):
+                            for _ in range(steps):
+                                b.step_kernels()
+                        s.wait_stream(bs)
             torch.cuda.current_stream().wait_stream(s)
             torch.cuda.synchronize()
             self._graph, self._graph_key = g, key
@@ -519,15 +453,8 @@ class Server:
             self._graph.replay()
         else:
             for _ in range(steps):
-                if self._merged():
-                    for b in self.buckets.values():
-                        b.pre_forces()
-                    self._merged_forces()
-                    for b in self.buckets.values():
-                        b.post_forces()
-                else:
-                    for b in self.buckets.values():
-                        b.step_kernels()
+                for b in self.buckets.values():
+                    b.step_kernels()
         ev1.record()
         torch.cuda.synchronize()
         return ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3

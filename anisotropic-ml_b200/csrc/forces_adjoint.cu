@@ -526,42 +526,16 @@ __device__ __forceinline__ void add_centroid_terms(const AdjShared &S, int q, co
     Xj[2] += e[0] * Sj[1] - e[1] * Sj[0];
 }
 
-// One bucket of the fused kernel's work: a pair list with its bodies, shape,
-// net and outputs. One launch takes up to kMaxBuckets of them (the serving
-// path's shapes) and spreads all their tiles over its CTAs.
-struct AdjBucket {
-    const float *pos, *quat;
-    const int *pairs;
-    const long long *d_np;
-    const float *pts, *w;
-    float *F, *T;
-    double *pe;
-    const int *rep;
-    const amlp_replica *rp;
-    long long cap;
-    float L, inv_rc, en_min, en_range;
-    int npts, rs;
-    AdjNet net;
-};
-constexpr int kMaxBuckets = 4;
-struct AdjBuckets {
-    int n, npts_max, wsm_max, par_max;  // the shared-memory layout fits the largest of each
-    AdjBucket b[kMaxBuckets];
-};
-static_assert(sizeof(AdjBucket) % 4 == 0, "buckets are copied as 32-bit words");
-
-// The buckets' tiles in one sequence (bucket 0's, then bucket 1's, ...), tile t
-// on CTA t % gridDim.x: a CTA reloads points, weights and biases only when its
-// next tile is in another bucket, and every bucket's tail is filled by the
-// others' tiles.
 // MULTI: the pairs come from many systems in one launch; body i's system is
 // rep[i], its box rp[rep[i]].box, and the pair energies are summed per system
 // into pe[rep[i]].
-// SINGLE: one bucket, whose arguments are read from the kernel's parameter
-// space like plain arguments (no registers held for them across the tile loop).
-#define BK(f) (SINGLE ? bs.b[0].f : sB.f)
-template <class Cfg, bool MULTI, bool SINGLE>
-__global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_constant__ AdjBuckets bs, int keep_r) {
+template <class Cfg, bool MULTI>
+__global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const float *pos, const float *quat, float L,
+                                                                const int *pairs, const long long *d_np, long long cap,
+                                                                const float *pts, int npts, float inv_rc, float en_min,
+                                                                float en_range, AdjNet net, const float *w, float *F,
+                                                                float *T, double *pe, const int *rep,
+                                                                const amlp_replica *rp, int keep_r) {
     constexpr int KC = Half<Cfg>::KC;
     constexpr int DP = kGS;  // row stride of the fp32 descriptor staging
     extern __shared__ __align__(128) char smem_raw[];
@@ -569,11 +543,10 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
     __shared__ uint32_t tmem_slot;
     __shared__ double pe_s[kAThreads / 32];
     __shared__ float psum_s[3];
-    __shared__ AdjBucket sB;  // the bucket being worked on
 
     const int tid = threadIdx.x, p = tid & (kAP - 1), h = tid >> 7, warp = tid >> 5, lane = tid & 31;
-    const int rs_max = 6 * bs.npts_max + 1 - ((6 * bs.npts_max) & 1);
-    const int Kg = 48;  // kin[0] of every bucket (D = 47 padded, set by the launcher)
+    const int rs = 6 * npts + 1 - ((6 * npts) & 1);
+    const int Kg = net.kin[0];
     const int first_limit = g_amlp_first_wait_limit;
 
     // ---- shared memory carve-up (offsets are multiples of 128 bytes)
@@ -584,7 +557,7 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
     // the partials are), so R survives the net and is rotated once per tile.
     // Otherwise (when that does not fit) R shares its area with the operand
     // tiles and is rotated again after the net.
-    const size_t r_bytes = (size_t)kAP * rs_max * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
+    const size_t r_bytes = (size_t)kAP * rs * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
     if (keep_r) {
         S.R = reinterpret_cast<float *>(smem_raw);
         off = align_up(r_bytes, 128);
@@ -596,9 +569,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
         off = align_up(r_bytes > ops_bytes ? r_bytes : ops_bytes, 128);
     }
     S.wts = smem_raw + off;
-    off += align_up(bs.wsm_max, 128);
+    off += align_up(net.wsm_total, 128);
     S.par = reinterpret_cast<float *>(smem_raw + off);
-    off += align_up((size_t)bs.par_max * 4, 128);
+    off += align_up((size_t)net.par_total * 4, 128);
     if (keep_r) {
         S.g0 = reinterpret_cast<float *>(op_tile(S.ops, 0));
         S.g1 = reinterpret_cast<float *>(op_tile(S.ops, 1));
@@ -621,12 +594,40 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
     S.ij = reinterpret_cast<int *>(smem_raw + off);
     off += (size_t)kAP * 2 * 4;
     S.pts = reinterpret_cast<float *>(smem_raw + off);
-    off = align_up(off + (size_t)3 * bs.npts_max * 4, 16);
+    off = align_up(off + (size_t)3 * npts * 4, 16);
     S.q = reinterpret_cast<float4 *>(smem_raw + off);
     S.psum = psum_s;
 
+    // ---- one-time set-up: weights (bf16 hi/lo, K-major), biases, TMEM, mbarrier
+    for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = pts[k];
+    __syncthreads();
+    body_point_sum(S, npts);
+    for (int L2 = 0; L2 < net.nh; ++L2) {
+        const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
+        const float *W = w + net.woff[L2];
+        char *hi = S.wts + net.wsm_off[L2];
+        char *lo = hi + Np * Kp * 2;
+        for (int idx = tid; idx < Np * Kp; idx += kAThreads) {
+            int n = idx / Kp, k = idx - n * Kp;
+            float v = (n < N && k < K) ? W[(size_t)n * K + k] : 0.f;
+            __nv_bfloat16 a, b;
+            tc::split_bf16(v, a, b);
+            uint32_t o = tc::kmajor_offset(n, k, Kp);
+            *reinterpret_cast<__nv_bfloat16 *>(hi + o) = a;
+            *reinterpret_cast<__nv_bfloat16 *>(lo + o) = b;
+        }
+        const float *b = W + (size_t)N * K;
+        for (int n = tid; n < Np; n += kAThreads) S.par[net.bias_off[L2] + n] = n < N ? b[n] : 0.f;
+    }
+    {
+        const int K = net.dims[net.nh];
+        const float *Wl = w + net.woff[net.nh];
+        for (int k = tid; k < kWpad; k += kAThreads) S.par[net.bias_off[net.nh] + k] = k < K ? Wl[k] : 0.f;
+        if (tid == 0) S.par[net.bias_off[net.nh] + kWpad] = Wl[K];  // last bias
+    }
     if (warp == 0) tc::tmem_alloc(&tmem_slot, 512);
     if (tid == 0) tc::mbar_init(&mbar, 1);
+    tc::fence_async_smem();
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
@@ -654,66 +655,22 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
         tc::fence_after();
     };
 
-    long long first_tile = 0;  // index of the current bucket's first tile in the launch's sequence
-    for (int bi = 0; bi < bs.n && !aborted; ++bi) {
-    __syncthreads();  // every thread is done with the previous bucket's arguments
-    for (int k = tid; k < (int)(sizeof(AdjBucket) / 4); k += kAThreads)
-        reinterpret_cast<int *>(&sB)[k] = reinterpret_cast<const int *>(&bs.b[bi])[k];
-    __syncthreads();
-    const long long P = min(*BK(d_np), BK(cap));
+    const long long P = min(*d_np, cap);
     const long long ntiles = (P + kAP - 1) / kAP;
-    long long t0 = ((long long)blockIdx.x - first_tile) % (long long)gridDim.x;
-    if (t0 < 0) t0 += gridDim.x;
-    first_tile += ntiles;
-    if (t0 >= ntiles) continue;  // no tile of this bucket on this CTA (the same for all its threads)
-    const AdjNet &net = BK(net);
-    const int npts = BK(npts), rs = BK(rs), nd = 2 * npts;
-    const float inv_rc = BK(inv_rc);
-
-    // ---- the bucket's set-up: body points, weights (bf16 hi/lo, K-major), biases
-    for (int k = tid; k < 3 * npts; k += kAThreads) S.pts[k] = BK(pts)[k];
-    __syncthreads();
-    body_point_sum(S, npts);
-    for (int L2 = 0; L2 < net.nh; ++L2) {
-        const int K = net.dims[L2], N = net.dims[L2 + 1], Kp = net.kin[L2], Np = net.nout[L2];
-        const float *W = BK(w) + net.woff[L2];
-        char *hi = S.wts + net.wsm_off[L2];
-        char *lo = hi + Np * Kp * 2;
-        for (int idx = tid; idx < Np * Kp; idx += kAThreads) {
-            int n = idx / Kp, k = idx - n * Kp;
-            float v = (n < N && k < K) ? W[(size_t)n * K + k] : 0.f;
-            __nv_bfloat16 a, b;
-            tc::split_bf16(v, a, b);
-            uint32_t o = tc::kmajor_offset(n, k, Kp);
-            *reinterpret_cast<__nv_bfloat16 *>(hi + o) = a;
-            *reinterpret_cast<__nv_bfloat16 *>(lo + o) = b;
-        }
-        const float *b = W + (size_t)N * K;
-        for (int n = tid; n < Np; n += kAThreads) S.par[net.bias_off[L2] + n] = n < N ? b[n] : 0.f;
-    }
-    {
-        const int K = net.dims[net.nh];
-        const float *Wl = BK(w) + net.woff[net.nh];
-        for (int k = tid; k < kWpad; k += kAThreads) S.par[net.bias_off[net.nh] + k] = k < K ? Wl[k] : 0.f;
-        if (tid == 0) S.par[net.bias_off[net.nh] + kWpad] = Wl[K];  // last bias
-    }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    tc::fence_after();
     double pe_acc = 0.0;
+    const int nd = 2 * npts;
 
-    for (long long tile = t0; tile < ntiles; tile += gridDim.x) {
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long long p0 = tile * kAP;
         const int valid = (int)min((long long)kAP, P - p0);
         // ---- 1. pair indices, orientations, translations, then the rotated body points
         if (tid < kAP) {
             long long pr = min(p0 + tid, P - 1);
-            int i = BK(pairs)[2 * pr], j = BK(pairs)[2 * pr + 1];
-            S.q[2 * tid] = load_quat(BK(quat), i);
-            S.q[2 * tid + 1] = load_quat(BK(quat), j);
+            int i = pairs[2 * pr], j = pairs[2 * pr + 1];
+            S.q[2 * tid] = load_quat(quat, i);
+            S.q[2 * tid + 1] = load_quat(quat, j);
             float dd;
-            float3 tt = min_image(BK(pos), i, j, MULTI ? BK(rp)[BK(rep)[i]].box : BK(L), &dd);
+            float3 tt = min_image(pos, i, j, MULTI ? rp[rep[i]].box : L, &dd);
             S.t[3 * tid] = tt.x;
             S.t[3 * tid + 1] = tt.y;
             S.t[3 * tid + 2] = tt.z;
@@ -853,8 +810,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
         }
         if (aborted) break;  // the net's outputs are not to be trusted: no forces from this tile
         if (!MULTI && h == 0 && p < valid)
-            pe_acc += (double)BK(en_min) +
-                      (double)BK(en_range) * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
+            pe_acc += (double)en_min +
+                      (double)en_range * (double)(S.eps[p] + S.eps[kAP + p] + S.par[net.bias_off[net.nh] + kWpad]);
         // ---- 4. recompute the rotated points (their area held the MLP tiles)
         if (!keep_r) {
             rotate_tile(S, npts, rs);
@@ -893,9 +850,9 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
             Tj[2] = -(Xj[2] - (Qj[0] * Gm[1] - Qj[1] * Gm[0]));
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                S.fd[9 * p + k] = clip100(Fp[k] * BK(en_range));
-                S.fd[9 * p + 3 + k] = clip100(Ti[k] * BK(en_range));
-                S.fd[9 * p + 6 + k] = clip100(Tj[k] * BK(en_range));
+                S.fd[9 * p + k] = clip100(Fp[k] * en_range);
+                S.fd[9 * p + 3 + k] = clip100(Ti[k] * en_range);
+                S.fd[9 * p + 6 + k] = clip100(Tj[k] * en_range);
             }
         }
         __syncthreads();
@@ -913,8 +870,8 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
             if (ok) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    atomicAdd(BK(F) + 3 * j + k, -v[k]);
-                    atomicAdd(BK(T) + 3 * j + k, S.fd[9 * q + 6 + k]);
+                    atomicAdd(F + 3 * j + k, -v[k]);
+                    atomicAdd(T + 3 * j + k, S.fd[9 * q + 6 + k]);
                 }
             }
             const bool runs = warp_keys_sorted(i, ok);  // every lane takes part (warp vote)
@@ -932,15 +889,15 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
             if (ok && (lane == 31 || kn != key)) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
-                    atomicAdd(BK(F) + 3 * i + k, v[k]);
-                    atomicAdd(BK(T) + 3 * i + k, v[3 + k]);
+                    atomicAdd(F + 3 * i + k, v[k]);
+                    atomicAdd(T + 3 * i + k, v[3 + k]);
                 }
             }
-            if (MULTI && BK(pe)) {  // pair energies summed per system (systems own contiguous bodies)
-                double e = ok ? (double)BK(en_min) + (double)BK(en_range) *
+            if (MULTI && pe) {  // pair energies summed per system (systems own contiguous bodies)
+                double e = ok ? (double)en_min + (double)en_range *
                                     (double)(S.eps[q] + S.eps[kAP + q] + S.par[net.bias_off[net.nh] + kWpad])
                               : 0.0;
-                const int sys = ok ? BK(rep)[i] : 0;
+                const int sys = ok ? rep[i] : 0;
                 const bool sys_runs = warp_keys_sorted(sys, ok);
                 int rk = ok && sys_runs ? sys : -1 - lane;
 #pragma unroll
@@ -950,13 +907,13 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
                     if (lane >= o && ro == rk) e += y;
                 }
                 int rn = __shfl_down_sync(0xffffffffu, rk, 1);
-                if (ok && (lane == 31 || rn != rk)) atomicAdd(BK(pe) + sys, e);
+                if (ok && (lane == 31 || rn != rk)) atomicAdd(pe + sys, e);
             }
         }
         __syncthreads();
     }
-    // ---- the bucket's pair-energy sum
-    if (!MULTI && BK(pe)) {
+    // ---- pair-energy sum, TMEM release
+    if (!MULTI && pe) {
         double v = pe_acc;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -964,13 +921,11 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
     }
     tc::fence_before();
     __syncthreads();
-    if (!MULTI && BK(pe) && tid == 0) {
+    if (!MULTI && pe && tid == 0) {
         double s = 0.0;
         for (int k = 0; k < kAThreads / 32; ++k) s += pe_s[k];
-        if (s != 0.0) atomicAdd(BK(pe), s);
+        if (s != 0.0) atomicAdd(pe, s);
     }
-    }  // buckets
-    // ---- TMEM release
     if (aborted && tid == 0) {
         atomicOr(&g_amlp_device_error, kErrMbarTimeout);
         // the last MMA issued may still be in flight (thread 0 flipped `phase` after waiting for it):
@@ -983,7 +938,6 @@ __global__ void __launch_bounds__(kAThreads, 1) k_forces_adjoint(const __grid_co
         tc::tmem_dealloc(tmem, 512);
     }
 }
-#undef BK
 
 // ============================================================================
 // Wide nets (hidden widths up to 128): three kernels instead of one, since the
@@ -1545,17 +1499,16 @@ amlp_status check_mlp(const amlp_mlp *m, int D);
 
 using namespace amlp;
 
-// One bucket of the fused kernel from the C-ABI arguments: checks, the net's
-// padded layout and the shape.
-static amlp_status make_bucket(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
-                               const long long *d_npairs, long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
-                               float *d_F, float *d_T, double *d_pe, const int *d_rep, const amlp_replica *d_rp,
-                               AdjBucket *out) {
+static amlp_status launch_adjoint(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
+                                  const long long *d_npairs, long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
+                                  float *d_F, float *d_T, double *d_pe, const int *d_rep, const amlp_replica *d_rp,
+                                  void *stream) {
     amlp_status st = check_nep(nep);
     if (st) return st;
     const int D = nep_D(nep);
     if ((st = check_mlp(mlp, D))) return st;
     if (!d_pos || !d_quat || !d_npairs || !d_F || !d_T || cap < 0 || (cap > 0 && !d_pairs)) return AMLP_ERR_INVALID_ARG;
+    if (cap == 0) return AMLP_OK;
     if (hyper_kind(nep) != 1 || D > 48) return AMLP_ERR_UNSUPPORTED;
     const int nh = mlp->n_layers - 1;
     if (nh < 1 || nh > kMaxHidden) return AMLP_ERR_UNSUPPORTED;
@@ -1582,32 +1535,7 @@ static amlp_status make_bucket(const float *d_pos, const float *d_quat, float bo
     par += kWpad + 4;
     net.wsm_total = wsm;
     net.par_total = par;
-    AdjBucket &B = *out;
-    B = AdjBucket{};
-    B.pos = d_pos, B.quat = d_quat, B.pairs = d_pairs, B.d_np = d_npairs, B.cap = cap;
-    B.pts = nep->d_pts, B.w = mlp->d_w, B.F = d_F, B.T = d_T, B.pe = d_pe, B.rep = d_rep, B.rp = d_rp;
-    B.L = box, B.inv_rc = 1.0f / nep->nep_cutoff, B.en_min = nep->en_min, B.en_range = nep->en_max - nep->en_min;
-    B.npts = nep->npts, B.rs = 6 * nep->npts + 1 - ((6 * nep->npts) & 1);
-    B.net = net;
-    return AMLP_OK;
-}
-
-// The fused kernel over one or more buckets (all with or all without the
-// multi-system indices): one launch, the shared-memory layout sized for the
-// largest shape and net among them.
-static amlp_status launch_buckets(const AdjBucket *buckets, int n, bool multi, cudaStream_t s) {
-    if (n < 1 || n > kMaxBuckets) return AMLP_ERR_INVALID_ARG;
-    AdjBuckets bs{};
-    bs.n = 0;
-    for (int k = 0; k < n; ++k) {
-        if (buckets[k].cap == 0) continue;
-        bs.b[bs.n++] = buckets[k];
-        bs.npts_max = std::max(bs.npts_max, buckets[k].npts);
-        bs.wsm_max = std::max(bs.wsm_max, buckets[k].net.wsm_total);
-        bs.par_max = std::max(bs.par_max, buckets[k].net.par_total);
-    }
-    if (bs.n == 0) return AMLP_OK;
-    const int npts = bs.npts_max, wsm = bs.wsm_max, par = bs.par_max;
+    const int npts = nep->npts;
     const int rs = 6 * npts + 1 - ((6 * npts) & 1);
     size_t r_bytes = (size_t)kAP * rs * 4, ops_bytes = (size_t)2 * 2 * kAP * kWpad * 2;
     static_assert((size_t)kAP * kGS * 4 <= (size_t)2 * kAP * kWpad * 2, "descriptor partials fit an operand tile");
@@ -1622,22 +1550,23 @@ static amlp_status launch_buckets(const AdjBucket *buckets, int n, bool multi, c
     const size_t smem = keep_r ? smem_keep : smem_shared;
     if (smem > 220 * 1024) return AMLP_ERR_UNSUPPORTED;
     using Cfg = NepCfg<10, 8, 4, 12>;
-    auto kern = bs.n == 1 ? (multi ? k_forces_adjoint<Cfg, true, true> : k_forces_adjoint<Cfg, false, true>)
-                          : (multi ? k_forces_adjoint<Cfg, true, false> : k_forces_adjoint<Cfg, false, false>);
-    AMLP_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    kern<<<kNumSM, kAThreads, smem, s>>>(bs, keep_r);
+    cudaStream_t s = as_stream(stream);
+    const float inv_rc = 1.0f / nep->nep_cutoff, rng = nep->en_max - nep->en_min;
+    if (d_rep) {
+        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_forces_adjoint<Cfg, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+        k_forces_adjoint<Cfg, true><<<kNumSM, kAThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                                                    nep->d_pts, npts, inv_rc, nep->en_min, rng, net,
+                                                                    mlp->d_w, d_F, d_T, d_pe, d_rep, d_rp, keep_r);
+    } else {
+        AMLP_CHECK_CUDA(cudaFuncSetAttribute(k_forces_adjoint<Cfg, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem));
+        k_forces_adjoint<Cfg, false><<<kNumSM, kAThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap,
+                                                                     nep->d_pts, npts, inv_rc, nep->en_min, rng, net,
+                                                                     mlp->d_w, d_F, d_T, d_pe, nullptr, nullptr,
+                                                                     keep_r);
+    }
     return check_launch();
-}
-
-static amlp_status launch_adjoint(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
-                                  const long long *d_npairs, long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
-                                  float *d_F, float *d_T, double *d_pe, const int *d_rep, const amlp_replica *d_rp,
-                                  void *stream) {
-    AdjBucket B;
-    amlp_status st = make_bucket(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, d_rep, d_rp, &B);
-    if (st) return st;
-    if (cap == 0) return AMLP_OK;
-    return launch_buckets(&B, 1, d_rep != nullptr, as_stream(stream));
 }
 
 extern "C" amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_quat, float box, const int *d_pairs,
@@ -1646,19 +1575,6 @@ extern "C" amlp_status amlp_forces_adjoint(const float *d_pos, const float *d_qu
                                            void *stream) {
     return launch_adjoint(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep, mlp, d_F, d_T, d_pe, nullptr, nullptr,
                           stream);
-}
-
-extern "C" amlp_status amlp_multi_forces_adjoint_shapes(const amlp_shape_batch *batches, int n, void *stream) {
-    if (!batches || n < 1 || n > kMaxBuckets) return AMLP_ERR_INVALID_ARG;
-    AdjBucket B[kMaxBuckets];
-    for (int k = 0; k < n; ++k) {
-        const amlp_shape_batch &b = batches[k];
-        if (!b.d_rep || !b.d_rp) return AMLP_ERR_INVALID_ARG;
-        amlp_status st = make_bucket(b.d_pos, b.d_quat, 0.f, b.d_pairs, b.d_npairs, b.cap, b.nep, b.mlp, b.d_F,
-                                     b.d_T, b.d_pe, b.d_rep, b.d_rp, &B[k]);
-        if (st) return st;
-    }
-    return launch_buckets(B, n, true, as_stream(stream));
 }
 
 extern "C" amlp_status amlp_multi_forces_adjoint(const float *d_pos, const float *d_quat, const int *d_rep,

@@ -329,26 +329,6 @@ amlp_status amlp_multi_forces_adjoint(const float *d_pos, const float *d_quat, c
                                       const amlp_replica *d_rp, const int *d_pairs, const long long *d_npairs,
                                       long long cap, const amlp_nep *nep, const amlp_mlp *mlp,
                                       float *d_F, float *d_T, double *d_pe, void *stream);
-/* One shape bucket of amlp_multi_forces_adjoint_shapes: the arguments of
- * amlp_multi_forces_adjoint for one shape and net (nep and mlp on the host). */
-typedef struct amlp_shape_batch {
-    const float *d_pos, *d_quat;
-    const int *d_rep;
-    const amlp_replica *d_rp;
-    const int *d_pairs;
-    const long long *d_npairs;
-    long long cap;
-    const amlp_nep *nep;
-    const amlp_mlp *mlp;
-    float *d_F, *d_T;
-    double *d_pe;
-} amlp_shape_batch;
-/* amlp_multi_forces_adjoint for up to 4 shape buckets (each with its own bodies,
- * pair list, shape, net and outputs) in one launch: the tiles of all buckets
- * are spread over the CTAs, each CTA loading a bucket's points and weights when
- * its next tile is in that bucket. The same results as one call per bucket.
- * Nets of the fused kernel only (widths <= 64, D = 47). */
-amlp_status amlp_multi_forces_adjoint_shapes(const amlp_shape_batch *batches, int n, void *stream);
 amlp_status amlp_multi_forces_adjoint_wide(const float *d_pos, const float *d_quat, const int *d_rep,
                                            const amlp_replica *d_rp, const int *d_pairs, const long long *d_npairs,
                                            long long cap, const amlp_nep *nep, const amlp_mlp *mlp,

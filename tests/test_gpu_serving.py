@@ -116,23 +116,3 @@ def test_wide_nets_same_alone_and_in_the_mix():
                          (mixed.angmom, alone.angmom)):
             ref = ref.cpu().numpy()
             assert np.abs(got - ref).max() <= 2e-6 * max(1.0, np.abs(ref).max()), r.rid
-
-
-def test_one_force_launch_equals_one_per_bucket():
-    """amlp_multi_forces_adjoint_shapes (one launch, each tile dispatched to its
-    bucket's shape and net) against one amlp_multi_forces_adjoint per bucket:
-    the same states after one step, within the rounding of the force atomics."""
-    nets = _nets()
-    out = {}
-    for merged in (True, False):
-        reqs = _mix()
-        for r in reqs:
-            r.steps = 1
-        srv = Server(nets, hbm_budget=8 << 30, segment=1, device=DEV, merge_forces=merged)
-        assert srv._merged() == merged
-        srv.run(reqs, keep_states=True)
-        out[merged] = srv.results
-    for rid, a in out[True].items():
-        b = out[False][rid]
-        for x, y in ((a.pos, b.pos), (a.vel, b.vel), (a.orient, b.orient), (a.angmom, b.angmom)):
-            assert np.abs(x - y).max() <= 2e-6 * max(1.0, np.abs(y).max()), rid
