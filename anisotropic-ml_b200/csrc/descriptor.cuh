@@ -93,12 +93,16 @@ __device__ __forceinline__ void sh_eval(float x, float y, float z, float *Y) {
     }
 }
 
-// Radial basis f_n, n = 0..NR-1, of a point at distance d.
+// Radial basis f_n, n = 0..NR-1, of a point at distance d. The cutoff cosine
+// comes from the hardware cosine (__cosf: an absolute error of a few 1e-7 for
+// the arguments here, smooth in u, so that it cancels in the finite
+// differences of neighbouring clouds); cospif costs about twenty more
+// instructions per point and finite-difference variant.
 template <int NR>
 __device__ __forceinline__ void radial_basis(float d, float inv_rc, float *f) {
     float u = d * inv_rc;
     float x = fmaf(2.0f * (u - 1.0f), (u - 1.0f), -1.0f);
-    float fc = 0.5f * (1.0f + cospif(u));
+    float fc = 0.5f * (1.0f + __cosf(3.14159265358979f * u));
     float hfc = 0.5f * fc;
     float tm1 = 1.0f, t = x;
     f[0] = fc;
