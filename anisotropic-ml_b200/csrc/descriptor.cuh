@@ -116,21 +116,14 @@ __device__ __forceinline__ void radial_basis(float d, float inv_rc, float *f) {
     }
 }
 
-// Descriptor of one point cloud. `pt(a)` returns point a (a < Nd). The D
-// values are written to g[d * gstride] (a column of a transposed tile).
+// Descriptor of one point cloud. `pt(a)` returns point a (a < Nd) and
+// `pt.point_sum()` the sum of all Nd points. The D values are written to
+// g[d * gstride] (a column of a transposed tile).
 template <class Cfg, class PointFn>
 __device__ __forceinline__ void nep_descriptor(const PointFn &pt, int Nd, float inv_rc, float *g, int gstride) {
-    float cx = 0.f, cy = 0.f, cz = 0.f;
-    for (int a = 0; a < Nd; ++a) {
-        float3 p = pt(a);
-        cx += p.x;
-        cy += p.y;
-        cz += p.z;
-    }
+    const float3 ps = pt.point_sum();
     float inv_nd = 1.0f / (float)Nd;
-    cx *= inv_nd;
-    cy *= inv_nd;
-    cz *= inv_nd;
+    const float cx = ps.x * inv_nd, cy = ps.y * inv_nd, cz = ps.z * inv_nd;
     float gang[Cfg::NA * Cfg::LMAX];
 #pragma unroll
     for (int i = 0; i < Cfg::NA * Cfg::LMAX; ++i) gang[i] = 0.f;
@@ -199,6 +192,26 @@ struct VariantPoints {
     int v;
     float dx;
     float4 q;              // rotation of variants 4..9 (identity otherwise)
+    // Sum of the variant's points. The rotated half enters as the rotation of its
+    // point sum (one rotation instead of one per point; the same sum up to
+    // rounding, as the order of a float sum is not the reference's either).
+    __device__ __forceinline__ float3 point_sum() const {
+        const bool c2 = v >= 7;
+        const float *A = c2 ? Rj : Ri, *B = c2 ? Ri : Rj;
+        float ax = 0.f, ay = 0.f, az = 0.f, bx = 0.f, by = 0.f, bz = 0.f;
+        for (int a = 0; a < h; ++a) {
+            ax += A[3 * a], ay += A[3 * a + 1], az += A[3 * a + 2];
+            bx += B[3 * a], by += B[3 * a + 1], bz += B[3 * a + 2];
+        }
+        float3 sa = make_float3(ax, ay, az);
+        if (v >= 4) sa = rotate_ref(q, sa);
+        const float n = (float)h;
+        if (v == 1) sa.x = fmaf(n, dx, sa.x);
+        if (v == 2) sa.y = fmaf(n, dx, sa.y);
+        if (v == 3) sa.z = fmaf(n, dx, sa.z);
+        const float s = c2 ? -1.0f : 1.0f;  // the second half is translated by +t (cloud 1) or -t (cloud 2)
+        return make_float3(sa.x + fmaf(s * n, tx, bx), sa.y + fmaf(s * n, ty, by), sa.z + fmaf(s * n, tz, bz));
+    }
     __device__ __forceinline__ float3 operator()(int a) const {
         const bool c2 = v >= 7;
         if (a < h) {
