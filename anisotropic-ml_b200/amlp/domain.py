@@ -1,16 +1,20 @@
 """Spatial domain decomposition of one periodic system over several GPUs.
 
 The reference runs one system on one GPU (``Sim.py:22-25``). Here the box is
-cut into slabs along x, one per rank (one process per GPU, ``torch.distributed``
-over NCCL; gloo on the CPU for tests). Each rank owns the bodies whose centre
-lies in its slab and, every step:
+cut into a grid of px x py x pz bricks, one per rank (one process per GPU,
+``torch.distributed`` over NCCL; gloo on the CPU for tests); slabs along x are
+the case py = pz = 1. Each rank owns the bodies whose centre lies in its brick
+and, every step:
 
-1. receives a halo from both neighbouring slabs: the positions and
-   orientations of their bodies within ``halo`` (pair cutoff + Verlet skin) of
-   the shared boundary, with ``send``/``recv`` to the neighbours only (no
-   collective on the data path). The halo's membership is chosen when the
-   Verlet lists are rebuilt and kept until the next rebuild, so that the list
-   indices stay valid; in between only the coordinates travel;
+1. receives a halo: the positions and orientations of the bodies of other
+   bricks within ``halo`` (pair cutoff + Verlet skin) of its own, in one pass
+   per cut axis with ``send``/``recv`` to the two neighbours along that axis
+   (no collective on the data path). A pass forwards what the earlier passes
+   received, so the bodies of the edge and corner neighbours arrive through the
+   face neighbours (six messages for a 3-D grid, not 26). The halo's membership
+   is chosen when the Verlet lists are rebuilt and kept until the next
+   rebuild, so that the list indices stay valid; in between only the
+   coordinates travel;
 2. evaluates the pair forces of every pair with at least one owned body over
    owned + halo bodies (owned bodies first, so that these pairs are the prefix
    of the (i, j)-sorted Verlet list with i < n_owned; each pair then oriented by
@@ -20,14 +24,12 @@ lies in its slab and, every step:
 3. integrates its owned bodies; the thermostat, which needs the kinetic
    energies of the whole system, takes one all-reduce of two numbers.
 
-At each Verlet rebuild bodies that left the slab move to the rank that now
-owns them (``migrate``). Positions stay wrapped in the periodic box, and the
-minimum image of the force kernels handles pairs across the periodic boundary
-(slabs are at least one halo wide).
+At each Verlet rebuild bodies that left the brick move to the rank that now
+owns them (``migrate``, axis by axis). Positions stay wrapped in the periodic
+box, and the minimum image of the force kernels handles pairs across the
+periodic boundary (bricks are at least two halos wide along every cut axis).
 """
 from __future__ import annotations
-
-from dataclasses import dataclass
 
 import numpy as np
 import torch
@@ -35,45 +37,96 @@ import torch
 FIELDS = ("pos", "quat", "vel", "angmom", "mass", "ids")
 
 
-@dataclass
-class Slab:
-    """Slab ``rank`` of ``world`` along x in a periodic box of edge L centred on 0."""
-    L: float
-    world: int
-    rank: int
+def brick_dims(world: int, L: float, width: float) -> tuple:
+    """(px, py, pz) with px py pz = world, as close to a cube as the box allows:
+    every cut axis keeps bricks at least 2 * width wide."""
+    best = None
+    for px in range(1, world + 1):
+        if world % px:
+            continue
+        for py in range(1, world // px + 1):
+            if (world // px) % py:
+                continue
+            dims = (px, py, world // px // py)
+            if any(p > 1 and L / p < 2.0 * width for p in dims):
+                continue
+            # the smallest largest cut, then the most even, then the cuts along x first
+            key = (max(dims), -min(dims), tuple(-p for p in dims))
+            if best is None or key < best[0]:
+                best = (key, dims)
+    if best is None:
+        raise ValueError(f"{world} bricks of a box of {L:.3g} cannot all be two halos of {width:.3g} wide")
+    return best[1]
 
-    @property
-    def lo(self) -> float:
-        return -0.5 * self.L + self.rank * self.L / self.world
 
-    @property
-    def hi(self) -> float:
-        return -0.5 * self.L + (self.rank + 1) * self.L / self.world
+class Brick:
+    """Brick ``rank`` of a px x py x pz grid over a periodic box of edge L centred
+    on 0; rank = (cx py + cy) pz + cz for the brick's grid coordinates."""
 
-    def owner(self, x: np.ndarray) -> np.ndarray:
-        """Owning rank of each x (wrapped into [-L/2, L/2))."""
+    def __init__(self, L: float, dims, rank: int):
+        self.L, self.dims, self.rank = float(L), tuple(int(p) for p in dims), int(rank)
+        self.world = int(np.prod(self.dims))
+        px, py, pz = self.dims
+        self.coords = (rank // (py * pz), (rank // pz) % py, rank % pz)
+
+    def lo(self, axis: int) -> float:
+        return -0.5 * self.L + self.coords[axis] * self.L / self.dims[axis]
+
+    def hi(self, axis: int) -> float:
+        return -0.5 * self.L + (self.coords[axis] + 1) * self.L / self.dims[axis]
+
+    def coord(self, x: np.ndarray, axis: int) -> np.ndarray:
+        """Grid coordinate along `axis` of each coordinate x (wrapped into [-L/2, L/2))."""
+        p = self.dims[axis]
         u = (np.asarray(x, np.float64) + 0.5 * self.L) / self.L
-        return np.clip(np.floor((u - np.floor(u)) * self.world).astype(np.int64), 0, self.world - 1)
+        return np.clip(np.floor((u - np.floor(u)) * p).astype(np.int64), 0, p - 1)
 
-    def near_lo(self, x: np.ndarray, width: float) -> np.ndarray:
-        """Owned x within `width` of the lower boundary (periodic distance)."""
-        d = np.mod(np.asarray(x, np.float64) - self.lo, self.L)
-        return d < width
+    def rank_of(self, c) -> int:
+        px, py, pz = self.dims
+        return int((c[0] * py + c[1]) * pz + c[2])
 
-    def near_hi(self, x: np.ndarray, width: float) -> np.ndarray:
-        d = np.mod(self.hi - np.asarray(x, np.float64), self.L)
-        return d <= width
+    def owner(self, pos: np.ndarray) -> np.ndarray:
+        """Owning rank of each position (rows x, y, z)."""
+        pos = np.asarray(pos)
+        px, py, pz = self.dims
+        return (self.coord(pos[:, 0], 0) * py + self.coord(pos[:, 1], 1)) * pz + self.coord(pos[:, 2], 2)
+
+    def neighbour(self, axis: int, step: int) -> int:
+        c = list(self.coords)
+        c[axis] = (c[axis] + step) % self.dims[axis]
+        return self.rank_of(c)
+
+    def near_lo(self, x: np.ndarray, width: float, axis: int) -> np.ndarray:
+        """Coordinates within `width` above the lower face along `axis` (periodic distance)."""
+        return np.mod(np.asarray(x, np.float64) - self.lo(axis), self.L) < width
+
+    def near_hi(self, x: np.ndarray, width: float, axis: int) -> np.ndarray:
+        return np.mod(self.hi(axis) - np.asarray(x, np.float64), self.L) <= width
+
+
+class Slab(Brick):
+    """Slab ``rank`` of ``world`` along x (a world x 1 x 1 grid of bricks)."""
+
+    def __init__(self, L: float, world: int, rank: int):
+        super().__init__(L, (world, 1, 1), rank)
 
 
 class Comm:
-    """Point-to-point exchange with the two neighbouring slabs over
-    ``torch.distributed`` (any backend with send/recv: NCCL, gloo). For two
-    ranks both neighbours are the same rank; the messages keep a fixed order
-    (towards the lower neighbour first), so they pair up on both sides."""
+    """Point-to-point exchange with the two neighbouring bricks along an axis of
+    a px x py x pz grid, over ``torch.distributed`` (any backend with send/recv:
+    NCCL, gloo). When an axis has two bricks both neighbours are the same rank;
+    the messages keep a fixed order (towards the lower neighbour first), so they
+    pair up on both sides."""
 
-    def __init__(self, dist, rank: int, world: int, device):
+    def __init__(self, dist, rank: int, world: int, device, dims=None):
         self.dist, self.rank, self.world, self.device = dist, rank, world, torch.device(device)
-        self.lower, self.upper = (rank - 1) % world, (rank + 1) % world
+        self.dims = tuple(dims) if dims is not None else (world, 1, 1)
+        if int(np.prod(self.dims)) != world:
+            raise ValueError(f"a grid of {self.dims} bricks is not {world} ranks")
+        self.brick_of_rank = Brick(1.0, self.dims, rank)
+
+    def neighbours(self, axis: int):
+        return self.brick_of_rank.neighbour(axis, -1), self.brick_of_rank.neighbour(axis, +1)
 
     def _p2p(self, ops) -> None:
         # one group of sends and receives (NCCL would deadlock on a send whose
@@ -97,15 +150,16 @@ class Comm:
             self._p2p(ops)
         return recv
 
-    def shift(self, to_lower: torch.Tensor, to_upper: torch.Tensor):
-        """Send `to_lower` to the lower neighbour and `to_upper` to the upper one;
-        returns (from_upper, from_lower): what the upper neighbour sent to its
-        lower side and what the lower neighbour sent to its upper side. One rank
-        has no neighbour: nothing comes back."""
-        if self.world == 1:
+    def shift(self, to_lower: torch.Tensor, to_upper: torch.Tensor, axis: int = 0):
+        """Send `to_lower` to the lower neighbour along `axis` and `to_upper` to
+        the upper one; returns (from_upper, from_lower): what the upper neighbour
+        sent to its lower side and what the lower neighbour sent to its upper
+        side. An axis with one brick has no neighbour: nothing comes back."""
+        if self.dims[axis] == 1:
             return to_lower[:0].clone(), to_upper[:0].clone()
-        from_upper = self._exchange(to_lower, self.lower, self.upper)
-        from_lower = self._exchange(to_upper, self.upper, self.lower)
+        lower, upper = self.neighbours(axis)
+        from_upper = self._exchange(to_lower, lower, upper)
+        from_lower = self._exchange(to_upper, upper, lower)
         return from_upper, from_lower
 
     def sum(self, t: torch.Tensor) -> torch.Tensor:
@@ -115,74 +169,87 @@ class Comm:
 
 
 class Halo:
-    """Halo bookkeeping of one rank for one Verlet-list period: which owned
-    bodies go to each neighbour (chosen at the rebuild) and how many come back.
-    ``payload`` / ``receive`` split an exchange into its two halves, so that a
-    test can pass the messages of several ranks by hand in one process."""
+    """Halo bookkeeping of one rank for one Verlet-list period: per cut axis,
+    which rows of the extended array (owned bodies, then the halo received so
+    far) go to each neighbour along it, chosen at the rebuild and replayed at
+    every step until the next one."""
 
-    def __init__(self, slab: Slab, width: float):
-        # a body within the halo width of both boundaries would reach a two-rank
-        # neighbour twice, and a halo wider than a slab would need the slab beyond it
-        if slab.world > 1 and slab.L / slab.world < 2.0 * width:
-            raise ValueError(f"slabs of {slab.L / slab.world:.3g} are thinner than twice the halo of {width:.3g}")
-        self.slab, self.width = slab, float(width)
-        self.to_lower = self.to_upper = None
-        self.n_from_upper = self.n_from_lower = 0
+    def __init__(self, brick: Brick, width: float):
+        # a body within the halo width of both faces would reach a two-brick
+        # neighbour twice, and a halo wider than a brick would need the brick beyond it
+        for a, p in enumerate(brick.dims):
+            if p > 1 and brick.L / p < 2.0 * width:
+                raise ValueError(f"bricks of {brick.L / p:.3g} along axis {a} are thinner than twice the halo "
+                                 f"of {width:.3g}")
+        self.brick, self.width = brick, float(width)
+        self.axes = [a for a, p in enumerate(brick.dims) if p > 1]
+        self.sends = []   # per cut axis: (rows to the lower neighbour, rows to the upper neighbour)
 
-    def choose(self, pos_owned: np.ndarray) -> None:
-        """Owned bodies within the halo width of each boundary (at a rebuild)."""
-        x = np.asarray(pos_owned)[:, 0]
-        self.to_lower = np.nonzero(self.slab.near_lo(x, self.width))[0]
-        self.to_upper = np.nonzero(self.slab.near_hi(x, self.width))[0]
+    def _select(self, pos: np.ndarray, axis: int):
+        x = np.asarray(pos)[:, axis]
+        return (np.nonzero(self.brick.near_lo(x, self.width, axis))[0],
+                np.nonzero(self.brick.near_hi(x, self.width, axis))[0])
 
-    def payload(self, pos: torch.Tensor, quat: torch.Tensor):
-        """(to_lower, to_upper): (k, 7) float32 rows of position and orientation."""
-        pq = torch.cat([pos, quat], dim=1)
-        lo = torch.as_tensor(self.to_lower, device=pos.device, dtype=torch.long)
-        hi = torch.as_tensor(self.to_upper, device=pos.device, dtype=torch.long)
-        return pq[lo], pq[hi]
+    def _pass(self, comm: Comm, ext: torch.Tensor, k: int, axis: int) -> torch.Tensor:
+        lo, hi = (torch.as_tensor(i, device=ext.device, dtype=torch.long) for i in self.sends[k])
+        from_upper, from_lower = comm.shift(ext[lo], ext[hi], axis)
+        return torch.cat([ext, from_upper, from_lower], dim=0)
 
-    def receive(self, pos: torch.Tensor, quat: torch.Tensor, from_upper: torch.Tensor, from_lower: torch.Tensor):
-        """Owned + halo arrays: owned bodies first, then the upper neighbour's,
-        then the lower neighbour's."""
-        self.n_from_upper, self.n_from_lower = int(from_upper.shape[0]), int(from_lower.shape[0])
-        ext = torch.cat([torch.cat([pos, quat], dim=1), from_upper, from_lower], dim=0)
-        return ext[:, :3].contiguous(), ext[:, 3:].contiguous()
+    def choose_and_exchange(self, comm: Comm, pos: torch.Tensor, quat: torch.Tensor, ids: torch.Tensor):
+        """At a rebuild: choose each pass's rows from the positions of the array
+        extended so far and exchange them; returns the extended positions,
+        orientations and global indices (owned bodies first)."""
+        ext = torch.cat([pos, quat], dim=1)
+        ext_ids = ids
+        self.sends = []
+        for k, axis in enumerate(self.axes):
+            self.sends.append(self._select(ext[:, :3].cpu().numpy(), axis))
+            lo, hi = (torch.as_tensor(i, device=ids.device, dtype=torch.long) for i in self.sends[k])
+            id_up, id_lo = comm.shift(ext_ids[lo], ext_ids[hi], axis)
+            ext = self._pass(comm, ext, k, axis)
+            ext_ids = torch.cat([ext_ids, id_up, id_lo])
+        return ext[:, :3].contiguous(), ext[:, 3:].contiguous(), ext_ids
 
     def exchange(self, comm: Comm, pos: torch.Tensor, quat: torch.Tensor):
-        lo, hi = self.payload(pos, quat)
-        from_upper, from_lower = comm.shift(lo, hi)
-        return self.receive(pos, quat, from_upper, from_lower)
+        """Between rebuilds: the same rows as chosen at the rebuild, current coordinates."""
+        ext = torch.cat([pos, quat], dim=1)
+        for k, axis in enumerate(self.axes):
+            ext = self._pass(comm, ext, k, axis)
+        return ext[:, :3].contiguous(), ext[:, 3:].contiguous()
 
 
-def migrate(comm: Comm, slab: Slab, owned: dict) -> dict:
-    """Bodies whose centre left the slab go to the neighbour that owns them now
-    (a body moves at most one slab between two rebuilds: slabs are wider than
-    the skin). `owned` maps FIELDS to tensors of the owned bodies; returns the
-    new owned set (kept bodies first, then arrivals from the upper and the lower
-    neighbour)."""
-    pos = owned["pos"]
-    dest = slab.owner(pos[:, 0].detach().cpu().numpy())
-    world, r = slab.world, slab.rank
-    lower, upper = (r - 1) % world, (r + 1) % world
-    stay = dest == r
-    if world > 1 and not np.all(stay | (dest == lower) | (dest == upper)):
-        raise RuntimeError("a body moved more than one slab between two Verlet rebuilds")
+def migrate(comm: Comm, brick: Brick, owned: dict) -> dict:
+    """Bodies whose centre left the brick go to the rank that owns them now,
+    one cut axis after the other (a body moves at most one brick along each
+    axis between two rebuilds: bricks are wider than the skin; a body leaving
+    through an edge or a corner reaches its owner through the face
+    neighbours). `owned` maps FIELDS to tensors of the owned bodies; returns the
+    new owned set (kept bodies first, then the arrivals of each pass)."""
     rows = torch.cat([owned["pos"].double(), owned["quat"].double(), owned["vel"].double(),
                       owned["angmom"].double(), owned["mass"].double()[:, None], owned["ids"].double()[:, None]],
                      dim=1)
     dev = rows.device
-    keep = torch.as_tensor(np.nonzero(stay)[0], device=dev, dtype=torch.long)
-    go_lo = torch.as_tensor(np.nonzero((dest == lower) & ~stay)[0], device=dev, dtype=torch.long)
-    go_hi = torch.as_tensor(np.nonzero((dest == upper) & ~stay & (dest != lower))[0], device=dev, dtype=torch.long)
-    if world == 2:  # one neighbour on both sides: every leaving body goes "down"
-        go_lo = torch.as_tensor(np.nonzero(~stay)[0], device=dev, dtype=torch.long)
-        go_hi = go_hi[:0]
-    from_upper, from_lower = comm.shift(rows[go_lo], rows[go_hi])
-    new = torch.cat([rows[keep], from_upper, from_lower], dim=0)
-    return {"pos": new[:, 0:3].float().contiguous(), "quat": new[:, 3:7].float().contiguous(),
-            "vel": new[:, 7:10].float().contiguous(), "angmom": new[:, 10:14].float().contiguous(),
-            "mass": new[:, 14].float().contiguous(), "ids": new[:, 15].round().long()}
+    for axis, p in enumerate(brick.dims):
+        if p == 1:
+            continue
+        c = brick.coords[axis]
+        dest = brick.coord(rows[:, axis].detach().cpu().numpy(), axis)
+        lower, upper = (c - 1) % p, (c + 1) % p
+        stay = dest == c
+        if not np.all(stay | (dest == lower) | (dest == upper)):
+            raise RuntimeError("a body moved more than one brick between two Verlet rebuilds")
+        keep = torch.as_tensor(np.nonzero(stay)[0], device=dev, dtype=torch.long)
+        go_lo = torch.as_tensor(np.nonzero((dest == lower) & ~stay)[0], device=dev, dtype=torch.long)
+        go_hi = torch.as_tensor(np.nonzero((dest == upper) & ~stay & (dest != lower))[0], device=dev,
+                                dtype=torch.long)
+        if p == 2:  # one neighbour on both sides: every leaving body goes "down"
+            go_lo = torch.as_tensor(np.nonzero(~stay)[0], device=dev, dtype=torch.long)
+            go_hi = go_hi[:0]
+        from_upper, from_lower = comm.shift(rows[go_lo], rows[go_hi], axis)
+        rows = torch.cat([rows[keep], from_upper, from_lower], dim=0)
+    return {"pos": rows[:, 0:3].float().contiguous(), "quat": rows[:, 3:7].float().contiguous(),
+            "vel": rows[:, 7:10].float().contiguous(), "angmom": rows[:, 10:14].float().contiguous(),
+            "mass": rows[:, 14].float().contiguous(), "ids": rows[:, 15].round().long()}
 
 
 class OwnedForces:
@@ -285,9 +352,10 @@ class OwnedForces:
 
 
 class DomainSystem:
-    """One rank's part of a periodic system decomposed into slabs (see the module
-    docstring): owned bodies, halo exchange, forces, the NVT halves of the owned
-    bodies and the global thermostat. Every rank calls ``step`` in lockstep."""
+    """One rank's part of a periodic system decomposed into bricks (see the
+    module docstring; the grid is ``comm.dims``, e.g. from ``brick_dims``): owned
+    bodies, halo exchange, forces, the NVT halves of the owned bodies and the
+    global thermostat. Every rank calls ``step`` in lockstep."""
 
     def __init__(self, comm: Comm, state, shape, hypers, net, kT: float, dt: float, device, method: str = "adjoint",
                  nlist_every: int = 100, skin: float = 2.0):
@@ -297,11 +365,11 @@ class DomainSystem:
         self.ctypes, self.call, self.size_query, self.Thermostat = ctypes, call, size_query, Thermostat
         self.comm, self.device = comm, torch.device(device)
         self.L = float(np.float32(state.L))
-        self.slab = Slab(self.L, comm.world, comm.rank)
-        self.halo = Halo(self.slab, float(shape.cutoff) + float(skin))
+        self.brick = Brick(self.L, comm.dims, comm.rank)
+        self.halo = Halo(self.brick, float(shape.cutoff) + float(skin))
         self.forces_of = OwnedForces(shape, hypers, net, self.L, device, method, skin)
         self.nlist_every, self.timestep, self.N = int(nlist_every), 0, int(state.N)
-        mine = np.nonzero(self.slab.owner(np.asarray(state.pos)[:, 0]) == comm.rank)[0]
+        mine = np.nonzero(self.brick.owner(np.asarray(state.pos)) == comm.rank)[0]
         f32 = dict(dtype=torch.float32, device=self.device)
         self.owned = {"pos": torch.tensor(np.asarray(state.pos)[mine], **f32),
                       "quat": torch.tensor(np.asarray(state.orient)[mine], **f32),
@@ -334,7 +402,7 @@ class DomainSystem:
 
     def _resize(self) -> None:
         if self.n <= 0:
-            raise RuntimeError(f"rank {self.comm.rank} owns no body: too many slabs for this system")
+            raise RuntimeError(f"rank {self.comm.rank} owns no body: too many bricks for this system")
         f32 = dict(dtype=torch.float32, device=self.device)
         self.accel = torch.zeros(self.n, 3, **f32)
         self.dp = torch.zeros(self.n, 4, **f32)
@@ -350,15 +418,10 @@ class DomainSystem:
         o, c = self.owned, self.ctypes
         if self.timestep % self.nlist_every == 0:
             if self.timestep > 0:
-                self.owned = o = migrate(self.comm, self.slab, o)
+                self.owned = o = migrate(self.comm, self.brick, o)
                 self._resize()
-            self.halo.choose(o["pos"].cpu().numpy())
-            ext_pos, ext_quat = self.halo.exchange(self.comm, o["pos"], o["quat"])
-            ids = o["ids"]
-            lo = torch.as_tensor(self.halo.to_lower, device=ids.device, dtype=torch.long)
-            hi = torch.as_tensor(self.halo.to_upper, device=ids.device, dtype=torch.long)
-            from_upper, from_lower = self.comm.shift(ids[lo], ids[hi])  # the halo's global indices
-            self.forces_of.rebuild(ext_pos, self.n, torch.cat([ids, from_upper, from_lower]))
+            ext_pos, ext_quat, ext_ids = self.halo.choose_and_exchange(self.comm, o["pos"], o["quat"], o["ids"])
+            self.forces_of.rebuild(ext_pos, self.n, ext_ids)
         else:
             ext_pos, ext_quat = self.halo.exchange(self.comm, o["pos"], o["quat"])
         F, T, pe = self.forces_of.forces(ext_pos, ext_quat, self.n)

@@ -46,13 +46,17 @@ class _Hub:
 
 
 class LoopbackComm:
-    """The Comm interface of amlp.domain for ranks that are threads of one process."""
+    """The Comm interface of amlp.domain for ranks that are threads of one process
+    (a world x 1 x 1 grid: slabs along x)."""
 
     def __init__(self, hub, rank):
         self.hub, self.rank, self.world, self.device = hub, rank, hub.world, DEV
+        self.dims = (hub.world, 1, 1)
         self.lower, self.upper = (rank - 1) % self.world, (rank + 1) % self.world
 
-    def shift(self, to_lower, to_upper):
+    def shift(self, to_lower, to_upper, axis=0):
+        if self.dims[axis] == 1:
+            return to_lower[:0].clone(), to_upper[:0].clone()
         items = self.hub.round(self.rank, (to_lower.clone(), to_upper.clone()))
         return items[self.upper][0].clone(), items[self.lower][1].clone()
 
