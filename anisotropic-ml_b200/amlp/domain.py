@@ -135,12 +135,14 @@ class Comm:
         for r in d.batch_isend_irecv([d.P2POp(fn, t, peer) for fn, t, peer in ops]):
             r.wait()
 
-    def _exchange(self, send: torch.Tensor, dst: int, src: int) -> torch.Tensor:
+    def _exchange(self, send: torch.Tensor, dst: int, src: int, n_recv: int | None = None) -> torch.Tensor:
         d = self.dist
-        n_out = torch.tensor([send.shape[0]], dtype=torch.int64, device=self.device)
-        n_in = torch.zeros(1, dtype=torch.int64, device=self.device)
-        self._p2p([(d.isend, n_out, dst), (d.irecv, n_in, src)])
-        recv = torch.empty((int(n_in.item()),) + tuple(send.shape[1:]), dtype=send.dtype, device=self.device)
+        if n_recv is None:  # the count first (a host synchronisation), then the rows
+            n_out = torch.tensor([send.shape[0]], dtype=torch.int64, device=self.device)
+            n_in = torch.zeros(1, dtype=torch.int64, device=self.device)
+            self._p2p([(d.isend, n_out, dst), (d.irecv, n_in, src)])
+            n_recv = int(n_in.item())
+        recv = torch.empty((n_recv,) + tuple(send.shape[1:]), dtype=send.dtype, device=self.device)
         ops = []
         if send.shape[0]:
             ops.append((d.isend, send.contiguous(), dst))
@@ -150,16 +152,19 @@ class Comm:
             self._p2p(ops)
         return recv
 
-    def shift(self, to_lower: torch.Tensor, to_upper: torch.Tensor, axis: int = 0):
+    def shift(self, to_lower: torch.Tensor, to_upper: torch.Tensor, axis: int = 0, counts=None):
         """Send `to_lower` to the lower neighbour along `axis` and `to_upper` to
         the upper one; returns (from_upper, from_lower): what the upper neighbour
         sent to its lower side and what the lower neighbour sent to its upper
-        side. An axis with one brick has no neighbour: nothing comes back."""
+        side. An axis with one brick has no neighbour: nothing comes back. With
+        `counts` = (rows from upper, rows from lower) known, the rows travel
+        without a count exchange and without a host synchronisation."""
         if self.dims[axis] == 1:
             return to_lower[:0].clone(), to_upper[:0].clone()
         lower, upper = self.neighbours(axis)
-        from_upper = self._exchange(to_lower, lower, upper)
-        from_lower = self._exchange(to_upper, upper, lower)
+        n_up, n_lo = counts if counts is not None else (None, None)
+        from_upper = self._exchange(to_lower, lower, upper, n_up)
+        from_lower = self._exchange(to_upper, upper, lower, n_lo)
         return from_upper, from_lower
 
     def sum(self, t: torch.Tensor) -> torch.Tensor:
@@ -184,6 +189,7 @@ class Halo:
         self.brick, self.width = brick, float(width)
         self.axes = [a for a, p in enumerate(brick.dims) if p > 1]
         self.sends = []   # per cut axis: (rows to the lower neighbour, rows to the upper neighbour)
+        self.counts = []  # per cut axis: (rows from the upper neighbour, rows from the lower one)
 
     def _select(self, pos: np.ndarray, axis: int):
         x = np.asarray(pos)[:, axis]
@@ -192,7 +198,10 @@ class Halo:
 
     def _pass(self, comm: Comm, ext: torch.Tensor, k: int, axis: int) -> torch.Tensor:
         lo, hi = (torch.as_tensor(i, device=ext.device, dtype=torch.long) for i in self.sends[k])
-        from_upper, from_lower = comm.shift(ext[lo], ext[hi], axis)
+        from_upper, from_lower = comm.shift(ext[lo], ext[hi], axis,
+                                            self.counts[k] if k < len(self.counts) else None)
+        if k == len(self.counts):  # at the rebuild: the counts hold until the next one
+            self.counts.append((int(from_upper.shape[0]), int(from_lower.shape[0])))
         return torch.cat([ext, from_upper, from_lower], dim=0)
 
     def choose_and_exchange(self, comm: Comm, pos: torch.Tensor, quat: torch.Tensor, ids: torch.Tensor):
@@ -201,17 +210,18 @@ class Halo:
         orientations and global indices (owned bodies first)."""
         ext = torch.cat([pos, quat], dim=1)
         ext_ids = ids
-        self.sends = []
+        self.sends, self.counts = [], []
         for k, axis in enumerate(self.axes):
             self.sends.append(self._select(ext[:, :3].cpu().numpy(), axis))
             lo, hi = (torch.as_tensor(i, device=ids.device, dtype=torch.long) for i in self.sends[k])
-            id_up, id_lo = comm.shift(ext_ids[lo], ext_ids[hi], axis)
             ext = self._pass(comm, ext, k, axis)
+            id_up, id_lo = comm.shift(ext_ids[lo], ext_ids[hi], axis, self.counts[k])
             ext_ids = torch.cat([ext_ids, id_up, id_lo])
         return ext[:, :3].contiguous(), ext[:, 3:].contiguous(), ext_ids
 
     def exchange(self, comm: Comm, pos: torch.Tensor, quat: torch.Tensor):
-        """Between rebuilds: the same rows as chosen at the rebuild, current coordinates."""
+        """Between rebuilds: the same rows as chosen at the rebuild, current
+        coordinates, the counts known (no count exchange, no host synchronisation)."""
         ext = torch.cat([pos, quat], dim=1)
         for k, axis in enumerate(self.axes):
             ext = self._pass(comm, ext, k, axis)

@@ -78,6 +78,9 @@ def _worker(rank, world, port, outdir):
         # the halo copies arrive once each, with their global indices
         halo_ids = ext_ids[len(mine):].numpy()
         assert len(np.unique(halo_ids)) == len(halo_ids) and not np.isin(halo_ids, mine).any()
+        # between rebuilds the same rows travel with the counts known, without a count exchange
+        again_pos, again_quat = halo.exchange(comm, pos, quat)
+        assert torch.equal(again_pos, ext_pos) and torch.equal(again_quat, ext_quat)
         # migration after every body moved by (3, 3, 3) (less than the skin along each axis): bodies
         # leave through faces, edges and corners
         owned = {"pos": pos.clone(), "quat": quat.clone(), "vel": torch.tensor(s.vel[mine]),

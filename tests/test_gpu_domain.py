@@ -54,7 +54,7 @@ class LoopbackComm:
         self.dims = (hub.world, 1, 1)
         self.lower, self.upper = (rank - 1) % self.world, (rank + 1) % self.world
 
-    def shift(self, to_lower, to_upper, axis=0):
+    def shift(self, to_lower, to_upper, axis=0, counts=None):
         if self.dims[axis] == 1:
             return to_lower[:0].clone(), to_upper[:0].clone()
         items = self.hub.round(self.rank, (to_lower.clone(), to_upper.clone()))
