@@ -118,9 +118,14 @@ __device__ __forceinline__ void radial_basis(float d, float inv_rc, float *f) {
 
 // Descriptor of one point cloud. `pt(a)` returns point a (a < Nd) and
 // `pt.point_sum()` the sum of all Nd points. The D values are written to
-// g[d * gstride] (a column of a transposed tile).
+// g[d * gstride] (a column of a transposed tile). Only the harmonic passes in
+// pass_mask run (bit p: harmonics p KC .. p KC + KC - 1); the radial sums are
+// written with pass 0, and the angular entries hold the sums of the passes run
+// (zero where they have no harmonic), so that a descriptor split over threads
+// by passes is the sum of their outputs.
 template <class Cfg, class PointFn>
-__device__ __forceinline__ void nep_descriptor(const PointFn &pt, int Nd, float inv_rc, float *g, int gstride) {
+__device__ __forceinline__ void nep_descriptor(const PointFn &pt, int Nd, float inv_rc, float *g, int gstride,
+                                               unsigned pass_mask = (1u << Cfg::NPASS) - 1u) {
     const float3 ps = pt.point_sum();
     float inv_nd = 1.0f / (float)Nd;
     const float cx = ps.x * inv_nd, cy = ps.y * inv_nd, cz = ps.z * inv_nd;
@@ -129,6 +134,7 @@ __device__ __forceinline__ void nep_descriptor(const PointFn &pt, int Nd, float 
     for (int i = 0; i < Cfg::NA * Cfg::LMAX; ++i) gang[i] = 0.f;
 #pragma unroll
     for (int pass = 0; pass < Cfg::NPASS; ++pass) {
+        if (!((pass_mask >> pass) & 1u)) continue;  // uniform over the warp
         constexpr int KC = Cfg::KC;
         const int k0 = pass * KC;
         float A[Cfg::NA][KC];

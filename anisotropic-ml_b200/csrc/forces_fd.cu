@@ -9,7 +9,10 @@
 // per row; warp v evaluates variant v of the 32 pairs (lane = pair), so every
 // branch on the variant is warp-uniform. The rotated body points of the tile
 // are staged in shared memory once and each variant's points are derived from
-// them on the fly.
+// them on the fly. The fused kernel runs 12 warps: warps 8 and 9 take the first
+// harmonic pass of variants 8 and 9 and warps 10 and 11 the second, so that each
+// of the SM's four schedulers (warp % 4) holds five passes of the tile instead
+// of six, six, four and four.
 #include "descriptor.cuh"
 
 namespace amlp {
@@ -17,7 +20,9 @@ namespace amlp {
 constexpr int kPT = 32;             // pairs per tile
 constexpr int kRows = 10 * kPT;     // rows (pair-variants) per tile
 constexpr int kTileThreads = kRows;  // one thread per row
-static_assert(kTileThreads % (2 * kPT) == 0, "whole (pair, body) groups per thread stride");
+constexpr int kFusedThreads = kRows + 2 * kPT;  // the fused kernel: two more warps for the split variants
+static_assert(kTileThreads % (2 * kPT) == 0 && kFusedThreads % (2 * kPT) == 0,
+              "whole (pair, body) groups per thread stride");
 
 struct TileGeom {
     int npts, nd, rs;  // points per body, points per cloud, floats per pair in R (odd)
@@ -65,11 +70,13 @@ __device__ void load_tile(const float *pos, const float *quat, float L, const in
     }
 }
 
-// Descriptor of row (v = warp, p = lane) of the staged tile into gT[d*ld + col].
+// Descriptor of row (variant v, pair p = lane) of the staged tile into
+// gT[d*ld + col], the harmonic passes in pass_mask.
 template <class Cfg>
 __device__ __forceinline__ void tile_descriptor_row(const float *R, const float *t, const TileGeom &g, float dx,
-                                                    float dteta, float inv_rc, float *gT, int ld, int col) {
-    const int v = threadIdx.x >> 5, p = threadIdx.x & 31;
+                                                    float dteta, float inv_rc, float *gT, int ld, int col, int v,
+                                                    unsigned pass_mask = (1u << Cfg::NPASS) - 1u) {
+    const int p = threadIdx.x & 31;
     VariantPoints vp;
     vp.Ri = R + p * g.rs;
     vp.Rj = vp.Ri + 3 * g.npts;
@@ -80,7 +87,7 @@ __device__ __forceinline__ void tile_descriptor_row(const float *R, const float 
     vp.v = v;
     vp.dx = dx;
     vp.q = variant_quat(v, dteta);
-    nep_descriptor<Cfg>(vp, g.nd, inv_rc, gT + col, ld);
+    nep_descriptor<Cfg>(vp, g.nd, inv_rc, gT + col, ld, pass_mask);
 }
 
 // ---------------------------------------------------------------- g_all to HBM
@@ -103,7 +110,7 @@ __global__ void __launch_bounds__(kTileThreads) k_descriptors(const float *pos, 
         long long p0 = tile * kPT;
         load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
         __syncthreads();
-        tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld, threadIdx.x);
+        tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld, threadIdx.x, threadIdx.x >> 5);
         __syncthreads();
         int valid = (int)min((long long)kPT, P - p0);
         // rows v*P + p0 .. p0+valid-1 of variant v are contiguous in g_all
@@ -299,16 +306,23 @@ struct FusedNet {
 // of a quarter warp take consecutive rg, so their float4 loads and stores of
 // activations cover 128 contiguous bytes (no bank conflicts) and they share
 // the weight loads (broadcast).
-static_assert(kRows % 8 == 0, "rows come in groups of 8");
+static_assert(kRows % 8 == 0 && (kRows / 8) % 4 == 0, "rows come in groups of 8, a multiple of 4 groups");
+static_assert(kFusedThreads % 128 == 0, "the fused kernel's warps are a multiple of four");
 __host__ __device__ constexpr int act_col(int r) { return ((r >> 2) & 1) * (kRows / 2) + (r >> 3) * 4 + (r & 3); }
 
 // YT[n][r] = act(b[n] + sum_k XT[k][r] WT[k*npad + n]) for n < npad, rows in the
-// permuted layout above; 8x8 register tiles.
+// permuted layout above; 8x8 register tiles. The items are dealt to the SM's
+// four schedulers (warp % 4) in four equal consecutive ranges, a quarter of the
+// work each (the block holds the same number of warps per scheduler); inside a
+// range the scheduler's warps take consecutive items.
 __device__ __forceinline__ void tile_gemm(const float *XT, int K, const float *WT, const float *b, int npad, float *YT,
                                           int act) {
     constexpr int nrg = kRows / 8, hoff = kRows / 2;
-    const int items = nrg * (npad / 8);
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+    const int items = nrg * (npad / 8);  // a multiple of 4 (nrg is)
+    const int per = items / 4, warp = threadIdx.x >> 5, per_sched = (blockDim.x >> 7) * 32;
+    const int base = (warp & 3) * per;
+    for (int li = (warp >> 2) * 32 + (threadIdx.x & 31); li < per; li += per_sched) {
+        const int it = base + li;
         const int rg = it % nrg, cg = it / nrg;
         float acc[8][8];
 #pragma unroll
@@ -395,7 +409,7 @@ __device__ __forceinline__ void scatter_tile(const float *fd, const int *ij, int
 }
 
 template <class Cfg>
-__global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos, const float *quat, float L,
+__global__ void __launch_bounds__(kFusedThreads, 1) k_forces_fd(const float *pos, const float *quat, float L,
                                                                const int *pairs, const long long *d_np, long long cap,
                                                                const float *pts, int npts, float inv_rc, FdConst c,
                                                                FusedNet net, const float *w, float *F, float *T,
@@ -412,7 +426,14 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
     float *R = pts_s + 3 * npts;
     float *t = R + kPT * g.rs;
     int *ij = reinterpret_cast<int *>(t + 3 * kPT);
-    __shared__ double pe_s[kTileThreads / 32];
+    __shared__ double pe_s[kFusedThreads / 32];
+    static_assert(Cfg::NPASS == 2, "the variant split hands the second of two harmonic passes to warps 10 and 11");
+    const int warp = threadIdx.x >> 5;
+    // descriptor stage: (variant, passes) of this warp; warps 10 and 11 write the
+    // second pass of variants 8 and 9 into bufB (free until the first layer),
+    // column 32 (v - 8) + pair, and it is added to bufA after the stage
+    const int dv = warp < 10 ? warp : warp - 2;
+    const unsigned dmask = warp < 8 ? 3u : (warp < 10 ? 1u : 2u);
 
     for (int k = threadIdx.x; k < 3 * npts; k += blockDim.x) pts_s[k] = pts[k];
     // transposed, zero-padded weights of every layer
@@ -435,7 +456,13 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
         const int valid = (int)min((long long)kPT, P - p0);
         load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
         __syncthreads();
-        tile_descriptor_row<Cfg>(R, t, g, c.dx, c.dteta, inv_rc, bufA, kRows, act_col(threadIdx.x));
+        tile_descriptor_row<Cfg>(R, t, g, c.dx, c.dteta, inv_rc, warp < 10 ? bufA : bufB, warp < 10 ? kRows : 2 * kPT,
+                                 warp < 10 ? act_col(threadIdx.x) : threadIdx.x - kRows, dv, dmask);
+        __syncthreads();
+        if (warp == 8 || warp == 9) {  // the second pass's angular sums (rows NR..D-1; zero where it has none)
+            const int col = act_col(threadIdx.x), sc = threadIdx.x - 8 * kPT;
+            for (int d = Cfg::NR; d < Cfg::D; ++d) bufA[d * kRows + col] += bufB[d * (2 * kPT) + sc];
+        }
         __syncthreads();
         float *X = bufA, *Y = bufB;
         for (int L2 = 0; L2 + 1 < net.n_layers; ++L2) {
@@ -449,11 +476,13 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
             const int Ll = net.n_layers - 1, K = net.dims[Ll];
             const float *wl = wt + net.wt_off[Ll];
             float acc = wt[net.b_off[Ll]];
-            const int col = act_col(threadIdx.x);
-            for (int k = 0; k < K; ++k) acc = fmaf(wl[k * net.npad[Ll]], X[k * kRows + col], acc);
-            e[threadIdx.x] = acc;
-            if (e_out && (threadIdx.x & 31) < valid)  // row (variant v, pair p) of e_all: e_out[v P + p0 + p]
-                e_out[(long long)(threadIdx.x >> 5) * P + p0 + (threadIdx.x & 31)] = acc;
+            if (threadIdx.x < kRows) {
+                const int col = act_col(threadIdx.x);
+                for (int k = 0; k < K; ++k) acc = fmaf(wl[k * net.npad[Ll]], X[k * kRows + col], acc);
+                e[threadIdx.x] = acc;
+                if (e_out && (threadIdx.x & 31) < valid)  // row (variant v, pair p) of e_all: e_out[v P + p0 + p]
+                    e_out[(long long)(threadIdx.x >> 5) * P + p0 + (threadIdx.x & 31)] = acc;
+            }
         }
         __syncthreads();
         for (int idx = threadIdx.x; idx < 9 * kPT; idx += blockDim.x) {
@@ -475,7 +504,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_forces_fd(const float *pos,
         __syncthreads();
         if (threadIdx.x == 0) {
             double s = 0.0;
-            for (int k = 0; k < kTileThreads / 32; ++k) s += pe_s[k];
+            for (int k = 0; k < kFusedThreads / 32; ++k) s += pe_s[k];
             if (s != 0.0) atomicAdd(pe, s);
         }
     }
@@ -628,7 +657,7 @@ static amlp_status launch_fd(const float *d_pos, const float *d_quat, float box,
     int grid = kNumSM;
     if (hyper_kind(nep) == 1) {
         if ((st = set_smem(k_forces_fd<CfgA>, smem))) return st;
-        k_forces_fd<CfgA><<<grid, kTileThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts,
+        k_forces_fd<CfgA><<<grid, kFusedThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, d_npairs, cap, nep->d_pts,
                                                            nep->npts, inv_rc, c, net, mlp->d_w, d_F, d_T, d_pe, d_e);
     } else {
         return AMLP_ERR_UNSUPPORTED;
