@@ -129,9 +129,10 @@ __device__ __forceinline__ void nep_descriptor(const PointFn &pt, int Nd, float 
     const float3 ps = pt.point_sum();
     float inv_nd = 1.0f / (float)Nd;
     const float cx = ps.x * inv_nd, cy = ps.y * inv_nd, cz = ps.z * inv_nd;
-    float gang[Cfg::NA * Cfg::LMAX];
+    // the angular entries start at zero in g and every pass adds its sums of
+    // squares there, so that no register holds them across a pass
 #pragma unroll
-    for (int i = 0; i < Cfg::NA * Cfg::LMAX; ++i) gang[i] = 0.f;
+    for (int i = 0; i < Cfg::NA * Cfg::LMAX; ++i) g[(Cfg::NR + i) * gstride] = 0.f;
 #pragma unroll
     for (int pass = 0; pass < Cfg::NPASS; ++pass) {
         if (!((pass_mask >> pass) & 1u)) continue;  // uniform over the warp
@@ -169,19 +170,22 @@ __device__ __forceinline__ void nep_descriptor(const PointFn &pt, int Nd, float 
 #pragma unroll
             for (int n = 0; n < Cfg::NR; ++n) g[n * gstride] = R[n];
         }
+        // the l of the pass's harmonics (every index is a constant once the
+        // pass loop is unrolled)
 #pragma unroll
-        for (int kk = 0; kk < KC; ++kk) {
-            if (k0 + kk < Cfg::K) {
-                constexpr int dummy = 0;
-                (void)dummy;
-                const int l = sh_l_of(k0 + kk);
+        for (int l = 1; l <= Cfg::LMAX; ++l) {
+            if (l < sh_l_of(k0) || l > sh_l_of(min(k0 + KC, Cfg::K) - 1)) continue;
 #pragma unroll
-                for (int n = 0; n < Cfg::NA; ++n) gang[n * Cfg::LMAX + l - 1] = fmaf(A[n][kk], A[n][kk], gang[n * Cfg::LMAX + l - 1]);
+            for (int n = 0; n < Cfg::NA; ++n) {
+                float *e = g + (Cfg::NR + n * Cfg::LMAX + l - 1) * gstride;
+                float s = *e;
+#pragma unroll
+                for (int kk = 0; kk < KC; ++kk)
+                    if (k0 + kk < Cfg::K && sh_l_of(k0 + kk) == l) s = fmaf(A[n][kk], A[n][kk], s);
+                *e = s;
             }
         }
     }
-#pragma unroll
-    for (int i = 0; i < Cfg::NA * Cfg::LMAX; ++i) g[(Cfg::NR + i) * gstride] = gang[i];
 }
 
 // Points of finite-difference variant v of a pair from the rotated body points
