@@ -189,6 +189,7 @@ class System:
         self.vpairs = None
         self.fpairs = None
         self.f_ws = None
+        self._split_g = self._split_e = None
         self.timestep = 0
         self._graphs = {}
         self.build_nlist()
@@ -204,6 +205,7 @@ class System:
         self.f_ws = torch.empty(max(1, size_query("amlp_filter_workspace_bytes", self.cap)), dtype=torch.uint8,
                                 device=self.device)
         self.adj_ws = None
+        self._split_g = self._split_e = None  # g_all and e_all of the split path (grown on demand)
         if self.net.max_hidden > 64 or self.hypers.D > 48:  # beyond the fused adjoint kernel: the wide path
             self.adj_ws = torch.empty(size_query("amlp_adjoint_workspace_bytes", self.cap), dtype=torch.uint8,
                                       device=self.device)
@@ -268,8 +270,16 @@ class System:
     def _forces_split(self) -> None:
         P = int(self.nf.item())  # the reference's data-dependent pair count (cp.where sync)
         D = self.hypers.D
-        g = torch.empty(10 * max(P, 1), D, dtype=torch.float32, device=self.device)
-        e = torch.empty(10 * max(P, 1), dtype=torch.float32, device=self.device)
+        rows = 10 * max(P, 1)
+        if self._split_e is None or self._split_e.numel() < rows:
+            # g_all and e_all kept between steps, a quarter above the largest pair count so far:
+            # a new block per step (pair counts move a little every step) would go back to
+            # cudaMalloc, a synchronous call, whenever the count grows
+            keep = rows + rows // 4
+            self._split_g = self._split_e = None
+            self._split_g = torch.empty(keep * D, dtype=torch.float32, device=self.device)
+            self._split_e = torch.empty(keep, dtype=torch.float32, device=self.device)
+        g, e = self._split_g, self._split_e
         call("amlp_descriptors", self.pos.data_ptr(), self.quat.data_ptr(), self.L, self.fpairs.data_ptr(), P,
              ctypes.byref(self.nep), g.data_ptr(), _stream())
         call("amlp_mlp_energy", g.data_ptr(), 10 * P, ctypes.byref(self.net.struct), e.data_ptr(), _stream())

@@ -176,79 +176,164 @@ __global__ void __launch_bounds__(kMlpRows) k_mlp(const float *g, long long rows
 }
 
 // Register-tiled FP32 net for widths up to 160 (the reference's 150-wide models
-// on its own finite-difference data flow): tiles of 64 rows, 256 threads, the
-// activations feature-major in shared memory and one layer's transposed
-// weights beside them (row stride npad + 1, odd, so that the transposing
-// stores do not collide in a bank). Thread t owns rows 4 (t % 16) .. + 3 and
-// columns cw (t / 16) .. + cw - 1 (cw = npad / 16 <= 10): 4 x cw outputs, one
-// 16-byte activation load and cw weight loads per 4 cw multiply-adds.
-constexpr int kTRows = 64, kTThreads = 256, kTMaxW = 160, kTMaxCw = kTMaxW / 16;
+// on its own finite-difference data flow): tiles of 128 rows, 256 threads. The
+// activations are feature-major in one shared-memory buffer, XT[k][col] (row
+// stride kTLd), with the tile's rows permuted so that thread rg's eight rows
+// sit at columns 4 rg .. 4 rg + 3 and 64 + 4 rg .. + 3: a quarter warp's
+// 16-byte loads cover 128 contiguous bytes. Each layer's weights are staged
+// k-major, WT[k][n] (row stride kTWs), by cp.async in blocks of 8 k x 4 n per
+// warp instruction (four 32-byte global segments, 32 different banks), so that
+// every copy of a thread is in flight at once; the next layer's copies run
+// while a layer's outputs are written. Thread t owns rows rg = t % 16 and, for
+// a 160-wide layer, columns 8 cg .. 8 cg + 7 and 128 + 2 cg, + 1 (cg = t / 16):
+// per k two 16-byte activation loads and three weight loads (16, 16, 8 bytes)
+// feed 80 multiply-adds, the next k's operands loaded before this k's
+// multiply-adds. Narrower layers take columns cg cw .. cg cw + cw - 1
+// (cw = npad / 16). The outputs stay in registers until every thread has read
+// the layer's inputs, then overwrite them. Each output is bias + sum_k x_k w_k
+// in ascending k, one rounding per multiply-add.
+constexpr int kTRows = 128, kTThreads = 256, kTMaxW = 160, kTMaxCw = kTMaxW / 16;
+constexpr int kTLd = kTRows + 4;  // activation row stride (16-byte aligned rows)
+constexpr int kTWs = kTMaxW + 4;  // weight row stride: 16-byte aligned rows, 4 (mod 32) for the staging banks
+__host__ __device__ constexpr int tiled_col(int r) { return ((r >> 2) & 1) * (kTRows / 2) + (r >> 3) * 4 + (r & 3); }
+
+// Asynchronous 4-byte global -> shared copy (cp.async, no register staging).
+__device__ __forceinline__ void cp_async4(float *dst, const float *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Layer L's weights, k-major with zero columns up to npad, and its bias into
+// WT and Bs. Copies in flight until cp_async_wait_all.
+__device__ __forceinline__ void stage_layer(const MlpDesc &m, const float *w, int L, float *WT, float *Bs) {
+    const int K = m.dims[L], N = m.dims[L + 1], npad = (N + 15) / 16 * 16;
+    const float *W = w + m.woff[L], *b = W + (size_t)N * K;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int nb = npad / 4, nblk = nb * ((K + 7) / 8);
+    for (int blk = warp; blk < nblk; blk += kTThreads / 32) {
+        const int kb = blk / nb;
+        const int n = 4 * (blk - kb * nb) + (lane & 3), k = 8 * kb + (lane >> 2);
+        if (k < K) {
+            if (n < N) cp_async4(WT + k * kTWs + n, W + (size_t)n * K + k);
+            else WT[k * kTWs + n] = 0.f;
+        }
+    }
+    for (int n = t; n < npad; n += kTThreads) {
+        if (n < N) cp_async4(Bs + n, b + n);
+        else Bs[n] = 0.f;
+    }
+}
+
+// Column of output c (0..9) of thread group cg in a 160-wide layer.
+__device__ __forceinline__ int wide_col(int cg, int c) { return c < 8 ? 8 * cg + c : 128 + 2 * cg + (c - 8); }
 
 __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long long rows, MlpDesc m, const float *w,
                                                          float *e_out) {
     extern __shared__ __align__(16) float smem[];
-    float *A = smem, *B = A + kTMaxW * kTRows;
-    float *WT = B + kTMaxW * kTRows;  // (kmax) x (npad + 1), then the bias
+    float *XT = smem;                  // kTMaxW x kTLd
+    float *WT = XT + kTMaxW * kTLd;    // kTMaxW x kTWs
+    float *Bs = WT + kTMaxW * kTWs;    // kTMaxW
     const int t = threadIdx.x, rg = t & 15, cg = t >> 4;
     for (long long r0 = (long long)blockIdx.x * kTRows; r0 < rows; r0 += (long long)gridDim.x * kTRows) {
         const int D = m.dims[0];
+        const int nr = (int)min((long long)kTRows, rows - r0);
+        __syncthreads();  // the previous tile's last layer is done with XT, WT and Bs
+        // the tile's g rows are one contiguous block: coalesced reads
         for (int idx = t; idx < kTRows * D; idx += kTThreads) {
             const int rr = idx / D, d = idx - rr * D;
-            A[d * kTRows + rr] = r0 + rr < rows ? g[(r0 + rr) * D + d] : 0.f;
+            if (rr < nr) cp_async4(XT + d * kTLd + tiled_col(rr), g + r0 * D + idx);
+            else XT[d * kTLd + tiled_col(rr)] = 0.f;
         }
-        float *X = A, *Y = B;
+        stage_layer(m, w, 0, WT, Bs);
+        cp_async_wait_all();
+        __syncthreads();
         for (int L = 0; L < m.n_layers; ++L) {
             const int K = m.dims[L], N = m.dims[L + 1];
-            const int npad = (N + 15) / 16 * 16, S = npad + 1, cw = npad / 16;
-            const float *W = w + m.woff[L], *b = W + (size_t)N * K;
-            __syncthreads();  // the previous layer is done with WT
-            for (int idx = t; idx < npad * K; idx += kTThreads) {  // coalesced reads of W (N x K)
-                const int n = idx / K, k = idx - n * K;
-                WT[k * S + n] = n < N ? W[idx] : 0.f;
-            }
-            for (int n = t; n < npad; n += kTThreads) WT[K * S + n] = n < N ? b[n] : 0.f;
-            __syncthreads();
-            const bool last = L == m.n_layers - 1;
-            float acc[4][kTMaxCw];
-#pragma unroll
-            for (int c = 0; c < kTMaxCw; ++c) {
-                const float bc = c < cw ? WT[K * S + cg * cw + c] : 0.f;
-#pragma unroll
-                for (int i = 0; i < 4; ++i) acc[i][c] = bc;
-            }
-            for (int k = 0; k < K; ++k) {
-                const float4 x = *reinterpret_cast<const float4 *>(X + k * kTRows + 4 * rg);
-                const float *wk = WT + k * S + cg * cw;
+            const int npad = (N + 15) / 16 * 16, cw = npad / 16;
+            const bool last = L == m.n_layers - 1, wide = npad == kTMaxW;
+            float acc[8][kTMaxCw];
+            const float *xk = XT + 4 * rg;
+            if (wide) {
 #pragma unroll
                 for (int c = 0; c < kTMaxCw; ++c) {
-                    if (c < cw) {
-                        const float wv = wk[c];
-                        acc[0][c] = fmaf(x.x, wv, acc[0][c]);
-                        acc[1][c] = fmaf(x.y, wv, acc[1][c]);
-                        acc[2][c] = fmaf(x.z, wv, acc[2][c]);
-                        acc[3][c] = fmaf(x.w, wv, acc[3][c]);
+                    const float bc = Bs[wide_col(cg, c)];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[i][c] = bc;
+                }
+                const float *wk = WT + 8 * cg, *wk2 = WT + 128 + 2 * cg;
+                float4 x0 = *reinterpret_cast<const float4 *>(xk);
+                float4 x1 = *reinterpret_cast<const float4 *>(xk + kTRows / 2);
+                float4 w0 = *reinterpret_cast<const float4 *>(wk);
+                float4 w1 = *reinterpret_cast<const float4 *>(wk + 4);
+                float2 w2 = *reinterpret_cast<const float2 *>(wk2);
+                for (int k = 0; k < K; ++k) {
+                    const int kn = (k + 1 < K ? k + 1 : k);
+                    const float4 nx0 = *reinterpret_cast<const float4 *>(xk + kn * kTLd);
+                    const float4 nx1 = *reinterpret_cast<const float4 *>(xk + kn * kTLd + kTRows / 2);
+                    const float4 nw0 = *reinterpret_cast<const float4 *>(wk + kn * kTWs);
+                    const float4 nw1 = *reinterpret_cast<const float4 *>(wk + kn * kTWs + 4);
+                    const float2 nw2 = *reinterpret_cast<const float2 *>(wk2 + kn * kTWs);
+                    const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                    const float ws[10] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y};
+#pragma unroll
+                    for (int c = 0; c < kTMaxCw; ++c)
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) acc[i][c] = fmaf(xs[i], ws[c], acc[i][c]);
+                    x0 = nx0;
+                    x1 = nx1;
+                    w0 = nw0;
+                    w1 = nw1;
+                    w2 = nw2;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < kTMaxCw; ++c) {
+                    const float bc = c < cw ? Bs[cg * cw + c] : 0.f;
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[i][c] = bc;
+                }
+                const float *wk = WT + cg * cw;
+                for (int k = 0; k < K; ++k) {
+                    const float4 x0 = *reinterpret_cast<const float4 *>(xk + k * kTLd);
+                    const float4 x1 = *reinterpret_cast<const float4 *>(xk + k * kTLd + kTRows / 2);
+                    const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+                    for (int c = 0; c < kTMaxCw; ++c) {
+                        if (c < cw) {
+                            const float wv = wk[k * kTWs + c];
+#pragma unroll
+                            for (int i = 0; i < 8; ++i) acc[i][c] = fmaf(xs[i], wv, acc[i][c]);
+                        }
                     }
                 }
             }
+            if (last) {  // the output column 0 (the energy): thread group cg = 0 in either layout
+                if (cg == 0) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int rr = 8 * rg + i;
+                        if (rr < nr) e_out[r0 + rr] = acc[i][0];
+                    }
+                }
+                break;
+            }
+            __syncthreads();  // every thread has read this layer's inputs and weights
+            stage_layer(m, w, L + 1, WT, Bs);  // in flight while the outputs are written
 #pragma unroll
             for (int c = 0; c < kTMaxCw; ++c) {
                 if (c < cw) {
-                    float4 o;
-                    o.x = last ? acc[0][c] : act_f(m.act, acc[0][c]);
-                    o.y = last ? acc[1][c] : act_f(m.act, acc[1][c]);
-                    o.z = last ? acc[2][c] : act_f(m.act, acc[2][c]);
-                    o.w = last ? acc[3][c] : act_f(m.act, acc[3][c]);
-                    *reinterpret_cast<float4 *>(Y + (cg * cw + c) * kTRows + 4 * rg) = o;
+                    float o[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) o[i] = act_f(m.act, acc[i][c]);
+                    float *yp = XT + (wide ? wide_col(cg, c) : cg * cw + c) * kTLd + 4 * rg;
+                    *reinterpret_cast<float4 *>(yp) = make_float4(o[0], o[1], o[2], o[3]);
+                    *reinterpret_cast<float4 *>(yp + kTRows / 2) = make_float4(o[4], o[5], o[6], o[7]);
                 }
             }
-            float *tmp = X;
-            X = Y;
-            Y = tmp;
+            cp_async_wait_all();
+            __syncthreads();
         }
-        __syncthreads();
-        for (int rr = t; rr < kTRows; rr += kTThreads)
-            if (r0 + rr < rows) e_out[r0 + rr] = X[rr];
-        __syncthreads();
     }
 }
 
@@ -595,10 +680,10 @@ extern "C" amlp_status amlp_mlp_energy(const float *d_g, long long rows, const a
         off += (long long)mlp->dims[k + 1] * mlp->dims[k] + mlp->dims[k + 1];
     }
     if (amax <= kTMaxW) {  // the register-tiled kernel
-        size_t smem = sizeof(float) * (2 * (size_t)kTMaxW * kTRows + (size_t)(kTMaxW + 1) * (kTMaxW + 1));
+        size_t smem = sizeof(float) * ((size_t)kTMaxW * kTLd + (size_t)kTMaxW * kTWs + kTMaxW);
         if ((st = set_smem(k_mlp_tiled, smem))) return st;
         long long tiles = (rows + kTRows - 1) / kTRows;
-        int grid = (int)std::min<long long>(tiles, kNumSM);  // one CTA per SM (184 KB of shared memory)
+        int grid = (int)std::min<long long>(tiles, kNumSM);  // one CTA per SM (188 KB of shared memory)
         k_mlp_tiled<<<grid, kTThreads, smem, as_stream(stream)>>>(d_g, rows, m, mlp->d_w, d_e);
         return check_launch();
     }
