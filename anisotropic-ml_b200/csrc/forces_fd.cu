@@ -189,12 +189,13 @@ __global__ void __launch_bounds__(kMlpRows) k_mlp(const float *g, long long rows
 // per k two 16-byte activation loads and three weight loads (16, 16, 8 bytes)
 // feed 80 multiply-adds, the next k's operands loaded before this k's
 // multiply-adds. Narrower layers take columns cg cw .. cg cw + cw - 1
-// (cw = npad / 16). The outputs stay in registers until every thread has read
+// (cw = npad / 16), the last layer (one output) column cg alone. The outputs stay in registers until every thread has read
 // the layer's inputs, then overwrite them. Each output is bias + sum_k x_k w_k
 // in ascending k, one rounding per multiply-add.
 constexpr int kTRows = 128, kTThreads = 256, kTMaxW = 160, kTMaxCw = kTMaxW / 16;
 constexpr int kTLd = kTRows + 4;  // activation row stride (16-byte aligned rows)
 constexpr int kTWs = kTMaxW + 4;  // weight row stride: 16-byte aligned rows, 4 (mod 32) for the staging banks
+constexpr int kTRowsK = kTMaxW + 2;  // rows of XT and WT: K <= 160 plus the two that a prefetch may read past K
 __host__ __device__ constexpr int tiled_col(int r) { return ((r >> 2) & 1) * (kTRows / 2) + (r >> 3) * 4 + (r & 3); }
 
 // Asynchronous 4-byte global -> shared copy (cp.async, no register staging).
@@ -231,9 +232,9 @@ __device__ __forceinline__ int wide_col(int cg, int c) { return c < 8 ? 8 * cg +
 __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long long rows, MlpDesc m, const float *w,
                                                          float *e_out) {
     extern __shared__ __align__(16) float smem[];
-    float *XT = smem;                  // kTMaxW x kTLd
-    float *WT = XT + kTMaxW * kTLd;    // kTMaxW x kTWs
-    float *Bs = WT + kTMaxW * kTWs;    // kTMaxW
+    float *XT = smem;                  // kTRowsK x kTLd
+    float *WT = XT + kTRowsK * kTLd;   // kTRowsK x kTWs
+    float *Bs = WT + kTRowsK * kTWs;   // kTMaxW
     const int t = threadIdx.x, rg = t & 15, cg = t >> 4;
     for (long long r0 = (long long)blockIdx.x * kTRows; r0 < rows; r0 += (long long)gridDim.x * kTRows) {
         const int D = m.dims[0];
@@ -261,30 +262,50 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
 #pragma unroll
                     for (int i = 0; i < 8; ++i) acc[i][c] = bc;
                 }
-                const float *wk = WT + 8 * cg, *wk2 = WT + 128 + 2 * cg;
-                float4 x0 = *reinterpret_cast<const float4 *>(xk);
-                float4 x1 = *reinterpret_cast<const float4 *>(xk + kTRows / 2);
-                float4 w0 = *reinterpret_cast<const float4 *>(wk);
-                float4 w1 = *reinterpret_cast<const float4 *>(wk + 4);
-                float2 w2 = *reinterpret_cast<const float2 *>(wk2);
-                for (int k = 0; k < K; ++k) {
-                    const int kn = (k + 1 < K ? k + 1 : k);
-                    const float4 nx0 = *reinterpret_cast<const float4 *>(xk + kn * kTLd);
-                    const float4 nx1 = *reinterpret_cast<const float4 *>(xk + kn * kTLd + kTRows / 2);
-                    const float4 nw0 = *reinterpret_cast<const float4 *>(wk + kn * kTWs);
-                    const float4 nw1 = *reinterpret_cast<const float4 *>(wk + kn * kTWs + 4);
-                    const float2 nw2 = *reinterpret_cast<const float2 *>(wk2 + kn * kTWs);
-                    const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-                    const float ws[10] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y};
+                // operands of row k: x (8 rows) and w (10 columns); two sets alternate so
+                // that row k + 1 is loading while row k's 80 multiply-adds issue
+                struct Ops {
+                    float4 x0, x1, w0, w1;
+                    float2 w2;
+                };
+                auto load = [&](const float *px, const float *pw) {
+                    Ops o;
+                    o.x0 = *reinterpret_cast<const float4 *>(px);
+                    o.x1 = *reinterpret_cast<const float4 *>(px + kTRows / 2);
+                    o.w0 = *reinterpret_cast<const float4 *>(pw + 8 * cg);
+                    o.w1 = *reinterpret_cast<const float4 *>(pw + 8 * cg + 4);
+                    o.w2 = *reinterpret_cast<const float2 *>(pw + 128 + 2 * cg);
+                    return o;
+                };
+                auto fma80 = [&](const Ops &o) {
+                    const float xs[8] = {o.x0.x, o.x0.y, o.x0.z, o.x0.w, o.x1.x, o.x1.y, o.x1.z, o.x1.w};
+                    const float ws[10] = {o.w0.x, o.w0.y, o.w0.z, o.w0.w, o.w1.x, o.w1.y, o.w1.z, o.w1.w, o.w2.x, o.w2.y};
 #pragma unroll
                     for (int c = 0; c < kTMaxCw; ++c)
 #pragma unroll
                         for (int i = 0; i < 8; ++i) acc[i][c] = fmaf(xs[i], ws[c], acc[i][c]);
-                    x0 = nx0;
-                    x1 = nx1;
-                    w0 = nw0;
-                    w1 = nw1;
-                    w2 = nw2;
+                };
+                const float *px = xk, *pw = WT;
+                Ops a = load(px, pw);
+                for (int k = 0; k < K; k += 2, px += 2 * kTLd, pw += 2 * kTWs) {
+                    const Ops b = load(px + kTLd, pw + kTWs);  // row k + 1 (a padding row when k + 1 = K)
+                    fma80(a);
+                    if (k + 1 < K) {
+                        a = load(px + 2 * kTLd, pw + 2 * kTWs);  // row k + 2 (<= K + 1)
+                        fma80(b);
+                    }
+                }
+            } else if (cw == 1) {  // one column per thread group (the last layer: N = 1)
+#pragma unroll
+                for (int i = 0; i < 8; ++i) acc[i][0] = Bs[cg];
+                const float *px = xk, *pw = WT + cg;
+                for (int k = 0; k < K; ++k, px += kTLd, pw += kTWs) {
+                    const float4 x0 = *reinterpret_cast<const float4 *>(px);
+                    const float4 x1 = *reinterpret_cast<const float4 *>(px + kTRows / 2);
+                    const float wv = *pw;
+                    const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) acc[i][0] = fmaf(xs[i], wv, acc[i][0]);
                 }
             } else {
 #pragma unroll
@@ -680,7 +701,7 @@ extern "C" amlp_status amlp_mlp_energy(const float *d_g, long long rows, const a
         off += (long long)mlp->dims[k + 1] * mlp->dims[k] + mlp->dims[k + 1];
     }
     if (amax <= kTMaxW) {  // the register-tiled kernel
-        size_t smem = sizeof(float) * ((size_t)kTMaxW * kTLd + (size_t)kTMaxW * kTWs + kTMaxW);
+        size_t smem = sizeof(float) * ((size_t)kTRowsK * kTLd + (size_t)kTRowsK * kTWs + kTMaxW);
         if ((st = set_smem(k_mlp_tiled, smem))) return st;
         long long tiles = (rows + kTRows - 1) / kTRows;
         int grid = (int)std::min<long long>(tiles, kNumSM);  // one CTA per SM (188 KB of shared memory)
