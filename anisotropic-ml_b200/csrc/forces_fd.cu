@@ -176,7 +176,8 @@ __global__ void __launch_bounds__(kMlpRows) k_mlp(const float *g, long long rows
 }
 
 // Register-tiled FP32 net for widths up to 160 (the reference's 150-wide models
-// on its own finite-difference data flow): tiles of 128 rows, 256 threads. The
+// on its own finite-difference data flow): tiles of 128 rows, 512 threads (four
+// warps per scheduler, which the shared memory of one tile allows). The
 // activations are feature-major in one shared-memory buffer, XT[k][col] (row
 // stride kTLd), with the tile's rows permuted so that thread rg's eight rows
 // sit at columns 4 rg .. 4 rg + 3 and 64 + 4 rg .. + 3: a quarter warp's
@@ -185,14 +186,15 @@ __global__ void __launch_bounds__(kMlpRows) k_mlp(const float *g, long long rows
 // warp instruction (four 32-byte global segments, 32 different banks), so that
 // every copy of a thread is in flight at once; the next layer's copies run
 // while a layer's outputs are written. Thread t owns rows rg = t % 16 and, for
-// a 160-wide layer, columns 8 cg .. 8 cg + 7 and 128 + 2 cg, + 1 (cg = t / 16):
-// per k two 16-byte activation loads and three weight loads (16, 16, 8 bytes)
-// feed 80 multiply-adds, the next k's operands loaded before this k's
-// multiply-adds. Narrower layers take columns cg cw .. cg cw + cw - 1
-// (cw = npad / 16), the last layer (one output) column cg alone. The outputs stay in registers until every thread has read
-// the layer's inputs, then overwrite them. Each output is bias + sum_k x_k w_k
-// in ascending k, one rounding per multiply-add.
-constexpr int kTRows = 128, kTThreads = 256, kTMaxW = 160, kTMaxCw = kTMaxW / 16;
+// a 160-wide layer, columns 4 cg .. 4 cg + 3 and 128 + cg (cg = t / 16): per k
+// two 16-byte activation loads and two weight loads (16 and 4 bytes) feed 40
+// multiply-adds, the next k's operands loading while this k's multiply-adds
+// issue. Narrower layers take columns cg, cg + 32, ... below npad. The outputs
+// stay in registers until every thread has read the layer's inputs, then
+// overwrite them. Each output is bias + sum_k x_k w_k in ascending k, one
+// rounding per multiply-add.
+constexpr int kTRows = 128, kTThreads = 512, kTMaxW = 160, kTGroups = kTThreads / 16;
+constexpr int kTMaxCw = kTMaxW / kTGroups;  // outputs per row and thread: 5
 constexpr int kTLd = kTRows + 4;  // activation row stride (16-byte aligned rows)
 constexpr int kTWs = kTMaxW + 4;  // weight row stride: 16-byte aligned rows, 4 (mod 32) for the staging banks
 constexpr int kTRowsK = kTMaxW + 2;  // rows of XT and WT: K <= 160 plus the two that a prefetch may read past K
@@ -226,8 +228,10 @@ __device__ __forceinline__ void stage_layer(const MlpDesc &m, const float *w, in
     }
 }
 
-// Column of output c (0..9) of thread group cg in a 160-wide layer.
-__device__ __forceinline__ int wide_col(int cg, int c) { return c < 8 ? 8 * cg + c : 128 + 2 * cg + (c - 8); }
+// Column of output c of thread group cg: a 160-wide layer (4 contiguous, then
+// one of the last 32), or a narrower one (cg + 32 c; beyond npad unused).
+__device__ __forceinline__ int wide_col(int cg, int c) { return c < 4 ? 4 * cg + c : 128 + cg; }
+__device__ __forceinline__ int narrow_col(int cg, int c) { return cg + kTGroups * c; }
 
 __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long long rows, MlpDesc m, const float *w,
                                                          float *e_out) {
@@ -251,8 +255,9 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
         __syncthreads();
         for (int L = 0; L < m.n_layers; ++L) {
             const int K = m.dims[L], N = m.dims[L + 1];
-            const int npad = (N + 15) / 16 * 16, cw = npad / 16;
+            const int npad = (N + 15) / 16 * 16;
             const bool last = L == m.n_layers - 1, wide = npad == kTMaxW;
+            const int ncol = wide ? kTMaxCw : (npad - cg + kTGroups - 1) / kTGroups;  // this thread's columns
             float acc[8][kTMaxCw];
             const float *xk = XT + 4 * rg;
             if (wide) {
@@ -262,24 +267,23 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
 #pragma unroll
                     for (int i = 0; i < 8; ++i) acc[i][c] = bc;
                 }
-                // operands of row k: x (8 rows) and w (10 columns); two sets alternate so
-                // that row k + 1 is loading while row k's 80 multiply-adds issue
+                // operands of row k: x (8 rows) and w (5 columns); two sets alternate so
+                // that row k + 1 is loading while row k's 40 multiply-adds issue
                 struct Ops {
-                    float4 x0, x1, w0, w1;
-                    float2 w2;
+                    float4 x0, x1, w0;
+                    float w1;
                 };
                 auto load = [&](const float *px, const float *pw) {
                     Ops o;
                     o.x0 = *reinterpret_cast<const float4 *>(px);
                     o.x1 = *reinterpret_cast<const float4 *>(px + kTRows / 2);
-                    o.w0 = *reinterpret_cast<const float4 *>(pw + 8 * cg);
-                    o.w1 = *reinterpret_cast<const float4 *>(pw + 8 * cg + 4);
-                    o.w2 = *reinterpret_cast<const float2 *>(pw + 128 + 2 * cg);
+                    o.w0 = *reinterpret_cast<const float4 *>(pw + 4 * cg);
+                    o.w1 = pw[128 + cg];
                     return o;
                 };
-                auto fma80 = [&](const Ops &o) {
+                auto fma40 = [&](const Ops &o) {
                     const float xs[8] = {o.x0.x, o.x0.y, o.x0.z, o.x0.w, o.x1.x, o.x1.y, o.x1.z, o.x1.w};
-                    const float ws[10] = {o.w0.x, o.w0.y, o.w0.z, o.w0.w, o.w1.x, o.w1.y, o.w1.z, o.w1.w, o.w2.x, o.w2.y};
+                    const float ws[kTMaxCw] = {o.w0.x, o.w0.y, o.w0.z, o.w0.w, o.w1};
 #pragma unroll
                     for (int c = 0; c < kTMaxCw; ++c)
 #pragma unroll
@@ -289,13 +293,13 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
                 Ops a = load(px, pw);
                 for (int k = 0; k < K; k += 2, px += 2 * kTLd, pw += 2 * kTWs) {
                     const Ops b = load(px + kTLd, pw + kTWs);  // row k + 1 (a padding row when k + 1 = K)
-                    fma80(a);
+                    fma40(a);
                     if (k + 1 < K) {
                         a = load(px + 2 * kTLd, pw + 2 * kTWs);  // row k + 2 (<= K + 1)
-                        fma80(b);
+                        fma40(b);
                     }
                 }
-            } else if (cw == 1) {  // one column per thread group (the last layer: N = 1)
+            } else if (ncol == 1) {  // one column (the last layer, N = 1: column cg < 16)
 #pragma unroll
                 for (int i = 0; i < 8; ++i) acc[i][0] = Bs[cg];
                 const float *px = xk, *pw = WT + cg;
@@ -307,22 +311,21 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
 #pragma unroll
                     for (int i = 0; i < 8; ++i) acc[i][0] = fmaf(xs[i], wv, acc[i][0]);
                 }
-            } else {
+            } else if (ncol > 1) {
 #pragma unroll
                 for (int c = 0; c < kTMaxCw; ++c) {
-                    const float bc = c < cw ? Bs[cg * cw + c] : 0.f;
+                    const float bc = c < ncol ? Bs[narrow_col(cg, c)] : 0.f;
 #pragma unroll
                     for (int i = 0; i < 8; ++i) acc[i][c] = bc;
                 }
-                const float *wk = WT + cg * cw;
                 for (int k = 0; k < K; ++k) {
                     const float4 x0 = *reinterpret_cast<const float4 *>(xk + k * kTLd);
                     const float4 x1 = *reinterpret_cast<const float4 *>(xk + k * kTLd + kTRows / 2);
                     const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
                     for (int c = 0; c < kTMaxCw; ++c) {
-                        if (c < cw) {
-                            const float wv = wk[k * kTWs + c];
+                        if (c < ncol) {
+                            const float wv = WT[k * kTWs + narrow_col(cg, c)];
 #pragma unroll
                             for (int i = 0; i < 8; ++i) acc[i][c] = fmaf(xs[i], wv, acc[i][c]);
                         }
@@ -343,11 +346,11 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
             stage_layer(m, w, L + 1, WT, Bs);  // in flight while the outputs are written
 #pragma unroll
             for (int c = 0; c < kTMaxCw; ++c) {
-                if (c < cw) {
+                if (c < ncol) {
                     float o[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) o[i] = act_f(m.act, acc[i][c]);
-                    float *yp = XT + (wide ? wide_col(cg, c) : cg * cw + c) * kTLd + 4 * rg;
+                    float *yp = XT + (wide ? wide_col(cg, c) : narrow_col(cg, c)) * kTLd + 4 * rg;
                     *reinterpret_cast<float4 *>(yp) = make_float4(o[0], o[1], o[2], o[3]);
                     *reinterpret_cast<float4 *>(yp + kTRows / 2) = make_float4(o[4], o[5], o[6], o[7]);
                 }
