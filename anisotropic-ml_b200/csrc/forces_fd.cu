@@ -14,6 +14,7 @@
 // of the SM's four schedulers (warp % 4) holds five passes of the tile instead
 // of six, six, four and four.
 #include "descriptor.cuh"
+#include "descriptor_direct.cuh"
 
 namespace amlp {
 
@@ -118,6 +119,116 @@ __global__ void __launch_bounds__(kTileThreads) k_descriptors(const float *pos, 
             int v = idx / (kPT * Cfg::D), rem = idx - v * kPT * Cfg::D;
             int p = rem / Cfg::D, d = rem - p * Cfg::D;
             if (p < valid) g_out[((long long)v * P + p0 + p) * Cfg::D + d] = gT[d * ld + v * kPT + p];
+        }
+        __syncthreads();
+    }
+}
+
+// The same rows in the reference's direct form, g_ang[n,l] = sum_{a,b} f_n(a)
+// f_n(b) P_l(rhat_a . rhat_b) (NepDescriptorKernels.py:3-144): cheaper than the
+// harmonic passes for the clouds of the reference's th_v1 and cube_v2 shapes
+// (8 and 12 points) and for the hypers (10, 10, 10), whose 120 harmonics take
+// twelve passes. Each row thread centres its variant's cloud into its own
+// float4 (rhat_a, d_a) slots of shared memory (point-major, threads innermost),
+// then sums the unordered point pairs, doubled, plus the diagonal (c = 1,
+// P_l(1) = 1), like the adjoint's direct forward pass.
+template <int NR, int NA, int LM>
+__device__ __forceinline__ void direct_row_descriptor(const VariantPoints &vp, int nd, float inv_rc, float4 *S,
+                                                      int sstride, float *g, int gstride) {
+    const float3 ps = vp.point_sum();
+    const float inv_nd = 1.0f / (float)nd;
+    const float cx = ps.x * inv_nd, cy = ps.y * inv_nd, cz = ps.z * inv_nd;
+    for (int a = 0; a < nd; ++a) {
+        const float3 p = vp(a);
+        const float rx = p.x - cx, ry = p.y - cy, rz = p.z - cz;
+        const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+        const float inv_d = rsqrtf(d2);
+        S[a * sstride] = make_float4(rx * inv_d, ry * inv_d, rz * inv_d, d2 * inv_d);
+    }
+    float acc[NA][LM], rad[NR], dia[NA];
+#pragma unroll
+    for (int n = 0; n < NA; ++n) {
+        dia[n] = 0.f;
+#pragma unroll
+        for (int l = 0; l < LM; ++l) acc[n][l] = 0.f;
+    }
+#pragma unroll
+    for (int n = 0; n < NR; ++n) rad[n] = 0.f;
+    for (int a = 0; a < nd; ++a) {
+        const float4 A = S[a * sstride];
+        float fa[NR];
+        radial_basis<NR>(A.w, inv_rc, fa);
+#pragma unroll
+        for (int n = 0; n < NR; ++n) rad[n] += fa[n];
+#pragma unroll
+        for (int n = 0; n < NA; ++n) dia[n] = fmaf(fa[n], fa[n], dia[n]);
+        for (int b = a + 1; b < nd; ++b) {
+            const float4 B = S[b * sstride];
+            const float c = fmaf(A.x, B.x, fmaf(A.y, B.y, A.z * B.z));
+            float Pl[LM];
+            Pl[0] = c;
+            Pl[1] = direct::legendre_next(1, c, c, 1.0f);
+#pragma unroll
+            for (int l = 2; l < LM; ++l) Pl[l] = direct::legendre_next(l, c, Pl[l - 1], Pl[l - 2]);
+            float fb[NR];
+            radial_basis<NR>(B.w, inv_rc, fb);
+#pragma unroll
+            for (int n = 0; n < NA; ++n) {
+                const float ff = fa[n] * fb[n];
+#pragma unroll
+                for (int l = 0; l < LM; ++l) acc[n][l] = fmaf(ff, Pl[l], acc[n][l]);
+            }
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < NR; ++n) g[n * gstride] = rad[n];
+#pragma unroll
+    for (int n = 0; n < NA; ++n)
+#pragma unroll
+        for (int l = 0; l < LM; ++l) g[(NR + n * LM + l) * gstride] = fmaf(2.0f, acc[n][l], dia[n]);
+}
+
+template <int NR, int NA, int LM>
+__global__ void __launch_bounds__(kTileThreads) k_descriptors_direct(const float *pos, const float *quat, float L,
+                                                                     const int *pairs, long long P, const float *pts,
+                                                                     int npts, float dx, float dteta, float inv_rc,
+                                                                     float *g_out) {
+    constexpr int D = NR + NA * LM;
+    extern __shared__ __align__(16) float smem[];
+    const TileGeom g = tile_geom(npts);
+    constexpr int ld = kRows + 1;  // odd stride: conflict-free column reads below
+    float4 *cloud = reinterpret_cast<float4 *>(smem);  // g.nd x kTileThreads
+    float *pts_s = reinterpret_cast<float *>(cloud + (size_t)g.nd * kTileThreads);
+    float *R = pts_s + 3 * npts;
+    float *t = R + kPT * g.rs;
+    int *ij = reinterpret_cast<int *>(t + 3 * kPT);
+    float *gT = reinterpret_cast<float *>(ij + 2 * kPT);
+    for (int k = threadIdx.x; k < 3 * npts; k += blockDim.x) pts_s[k] = pts[k];
+    __syncthreads();
+    const int v = threadIdx.x >> 5, p = threadIdx.x & 31;
+    long long ntiles = (P + kPT - 1) / kPT;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        long long p0 = tile * kPT;
+        load_tile(pos, quat, L, pairs, P, p0, pts_s, g, R, t, ij);
+        __syncthreads();
+        VariantPoints vp;
+        vp.Ri = R + p * g.rs;
+        vp.Rj = vp.Ri + 3 * g.npts;
+        vp.tx = t[3 * p];
+        vp.ty = t[3 * p + 1];
+        vp.tz = t[3 * p + 2];
+        vp.h = g.npts;
+        vp.v = v;
+        vp.dx = dx;
+        vp.q = variant_quat(v, dteta);
+        direct_row_descriptor<NR, NA, LM>(vp, g.nd, inv_rc, cloud + threadIdx.x, kTileThreads, gT + threadIdx.x, ld);
+        __syncthreads();
+        int valid = (int)min((long long)kPT, P - p0);
+        // rows v*P + p0 .. p0+valid-1 of variant v are contiguous in g_all
+        for (int idx = threadIdx.x; idx < 10 * kPT * D; idx += blockDim.x) {
+            int vv = idx / (kPT * D), rem = idx - vv * kPT * D;
+            int pp = rem / D, d = rem - pp * D;
+            if (pp < valid) g_out[((long long)vv * P + p0 + pp) * D + d] = gT[d * ld + vv * kPT + pp];
         }
         __syncthreads();
     }
@@ -621,6 +732,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_forces_fd(const float *pos
 
 // ---------------------------------------------------------------- host side
 using CfgA = NepCfg<10, 8, 4, 12>;    // D = 47 (the C104 models and every large-scale config)
+constexpr int kDirectMaxNd47 = 12;    // clouds up to which the direct form is the cheaper one for D = 47
 using CfgB = NepCfg<10, 10, 10, 10>;  // D = 121 (the C100 models)
 
 int hyper_kind(const amlp_nep *n) {
@@ -671,7 +783,16 @@ extern "C" amlp_status amlp_descriptors(const float *d_pos, const float *d_quat,
     long long ntiles = (P + kPT - 1) / kPT;
     int grid = (int)std::min<long long>(ntiles, 8LL * kNumSM);
     float inv_rc = 1.0f / nep->nep_cutoff;
-    if (hyper_kind(nep) == 1) {
+    // the direct form where it costs less (the rule of the adjoint's descriptor passes) and its
+    // per-thread clouds fit the shared memory
+    const size_t smem_direct = smem + sizeof(float4) * (size_t)g.nd * kTileThreads;
+    const bool direct = (hyper_kind(nep) == 2 || g.nd <= kDirectMaxNd47) && smem_direct <= 227 * 1024;
+    if (direct) {
+        auto kern = hyper_kind(nep) == 2 ? k_descriptors_direct<11, 11, 10> : k_descriptors_direct<11, 9, 4>;
+        if ((st = set_smem(kern, smem_direct))) return st;
+        kern<<<grid, kTileThreads, smem_direct, s>>>(d_pos, d_quat, box, d_pairs, P, nep->d_pts, nep->npts, nep->dx,
+                                                     nep->dteta, inv_rc, d_g);
+    } else if (hyper_kind(nep) == 1) {
         if ((st = set_smem(k_descriptors<CfgA>, smem))) return st;
         k_descriptors<CfgA><<<grid, kTileThreads, smem, s>>>(d_pos, d_quat, box, d_pairs, P, nep->d_pts, nep->npts,
                                                              nep->dx, nep->dteta, inv_rc, d_g);
