@@ -551,19 +551,37 @@ __device__ __forceinline__ void tile_gemm(const float *XT, int K, const float *W
 #pragma unroll
             for (int i = 0; i < 8; ++i) acc[i][j] = bj;
         }
-        const float *xp = XT + rg * 4;
-        const float *wp = WT + cg * 8;
-        for (int k = 0; k < K; ++k) {
-            float4 x0 = *reinterpret_cast<const float4 *>(xp + k * kRows);
-            float4 x1 = *reinterpret_cast<const float4 *>(xp + k * kRows + hoff);
-            float4 w0 = *reinterpret_cast<const float4 *>(wp + k * npad);
-            float4 w1 = *reinterpret_cast<const float4 *>(wp + k * npad + 4);
-            float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-            float ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+        // operands of row k; two sets alternate so that row k + 1 loads while row k's 64
+        // multiply-adds issue. The load of row K (past the last) reads the next area of
+        // the shared memory (the following activation buffer, bias or layer) and is unused.
+        struct Ops {
+            float4 x0, x1, w0, w1;
+        };
+        auto load = [&](const float *xp, const float *wp) {
+            Ops o;
+            o.x0 = *reinterpret_cast<const float4 *>(xp);
+            o.x1 = *reinterpret_cast<const float4 *>(xp + hoff);
+            o.w0 = *reinterpret_cast<const float4 *>(wp);
+            o.w1 = *reinterpret_cast<const float4 *>(wp + 4);
+            return o;
+        };
+        auto fma64 = [&](const Ops &o) {
+            const float xs[8] = {o.x0.x, o.x0.y, o.x0.z, o.x0.w, o.x1.x, o.x1.y, o.x1.z, o.x1.w};
+            const float ws[8] = {o.w0.x, o.w0.y, o.w0.z, o.w0.w, o.w1.x, o.w1.y, o.w1.z, o.w1.w};
 #pragma unroll
             for (int i = 0; i < 8; ++i)
 #pragma unroll
                 for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(xs[i], ws[j], acc[i][j]);
+        };
+        const float *xp = XT + rg * 4, *wp = WT + cg * 8;
+        Ops a = load(xp, wp);
+        for (int k = 0; k < K; k += 2, xp += 2 * kRows, wp += 2 * npad) {
+            const Ops bo = load(xp + kRows, wp + npad);  // row k + 1 (row K when k + 1 = K: unused)
+            fma64(a);
+            if (k + 1 < K) {
+                a = load(xp + 2 * kRows, wp + 2 * npad);  // row k + 2 (<= K)
+                fma64(bo);
+            }
         }
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
