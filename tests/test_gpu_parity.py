@@ -173,6 +173,25 @@ def test_pair_descriptors_vs_fp64(shape_name, hyp, ld):
         assert np.all(g[:, D:] == 0.0)
 
 
+@pytest.mark.parametrize("shape_name,hyp", [("cube_v2", (10, 10, 10)), ("pbp_v3", (10, 10, 10)),
+                                            ("pbp_v3", (10, 8, 4))])
+def test_descriptors_both_forms(shape_name, hyp):
+    """amlp_descriptors (g_all of the ten finite-difference variants) in both of
+    its forms: the direct form for cube_v2's 12-point clouds, the harmonic passes
+    for pbp_v3's 14 points, with (10, 10, 10) because the direct form's
+    per-thread clouds would not fit the shared memory beside its 121-row tile."""
+    s = make_state(300, shape_name, 0.1, seed=6, L={"pbp_v3": 32.0}.get(shape_name, 24.0))
+    shape = SHAPES[shape_name]
+    vp = nlist.sorted_pairs(nlist.reference_pairs(s.pos, s.L, shape["cutoff"] + 2.0))
+    _, pairs, _ = nep.min_image_filter(s.pos, vp, s.L, shape["cutoff"])
+    pairs = pairs[:400]
+    g = gh.descriptors(s.pos, s.orient, s.L, pairs, shape, hyp)
+    _, _, t = nep.min_image_filter(s.pos, pairs, s.L, shape["cutoff"], np.float64)
+    c1, c2 = nep.pair_clouds(s.orient, pairs, t, shape["pts"], np.float64)
+    g64 = nep.descriptor(nep.fd_variants(c1, c2, 1e-5, 1e-5, np.float64), hyp, shape["nep_cutoff"], np.float64)
+    _check_desc(g, g64)
+
+
 # ----------------------------------------------------------------------------- net energies
 @pytest.mark.parametrize("widths,act", [((64, 64), "tanh"), ((128, 128, 128), "silu"), ((150, 150, 150, 150), "relu")])
 def test_mlp_energy_vs_torch(widths, act):
