@@ -193,8 +193,12 @@ def test_descriptors_both_forms(shape_name, hyp):
 
 
 # ----------------------------------------------------------------------------- net energies
-@pytest.mark.parametrize("widths,act", [((64, 64), "tanh"), ((128, 128, 128), "silu"), ((150, 150, 150, 150), "relu")])
+@pytest.mark.parametrize("widths,act", [((64, 64), "tanh"), ((128, 128, 128), "silu"), ((150, 150, 150, 150), "relu"),
+                                        ((160, 160), "relu"), ((100, 37), "tanh")])
 def test_mlp_energy_vs_torch(widths, act):
+    """amlp_mlp_energy against FP32 torch on 3001 rows (a partial last tile): the
+    160-wide layers' register tiling (150 padded, and 160 with no padding column),
+    the narrower layers' columns (64, 100 and 37 wide) and the one-output layer."""
     from amlp.engine import EnergyNet
     rng = np.random.default_rng(0)
     g = rng.standard_normal((3001, 47)).astype(np.float32)
