@@ -4,7 +4,8 @@ the reference's own run). All calls go through the C ABI of libamlp.
 Tolerances:
 * Verlet list and pair filter: bit-exact (same pairs, same order);
 * descriptors: |g_gpu - g_fp64| <= 5e-5 * max(1, |g|) -- the GPU evaluates the
-  angular sum through the addition theorem in FP32, the reference directly;
+  angular sum in FP32 through the addition theorem, or directly like the
+  reference for clouds of at most 12 points and the (10, 10, 10) hypers;
 * net energies: relative 1e-5 against torch FP32 on the same descriptors; on
   the GPU's own descriptors, the deviation from FP64 may not exceed twice the
   reference's own FP32 deviation from FP64 (plus 1e-6 of the energy scale);
