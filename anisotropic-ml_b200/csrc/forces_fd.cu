@@ -319,18 +319,23 @@ __device__ __forceinline__ void cp_async4(float *dst, const float *src) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Layer L's weights, k-major with zero columns up to npad, and its bias into
-// WT and Bs. Copies in flight until cp_async_wait_all.
+// WT and Bs, in blocks of 8 k x 4 n per warp instruction. Copies in flight
+// until cp_async_wait_all.
 __device__ __forceinline__ void stage_layer(const MlpDesc &m, const float *w, int L, float *WT, float *Bs) {
     const int K = m.dims[L], N = m.dims[L + 1], npad = (N + 15) / 16 * 16;
     const float *W = w + m.woff[L], *b = W + (size_t)N * K;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int nb = npad / 4, nblk = nb * ((K + 7) / 8);
-    for (int blk = warp; blk < nblk; blk += kTThreads / 32) {
-        const int kb = blk / nb;
-        const int n = 4 * (blk - kb * nb) + (lane & 3), k = 8 * kb + (lane >> 2);
-        if (k < K) {
-            if (n < N) cp_async4(WT + k * kTWs + n, W + (size_t)n * K + k);
-            else WT[k * kTWs + n] = 0.f;
+    // warp w takes the column blocks w, w + 16, ... and walks each down k with
+    // two pointer increments per copy (no index division)
+    for (int nbi = warp; 4 * nbi < npad; nbi += kTThreads / 32) {
+        const int n = 4 * nbi + (lane & 3);
+        int k = lane >> 2;
+        float *dst = WT + k * kTWs + n;
+        if (n < N) {
+            const float *src = W + (size_t)n * K + k;
+            for (; k < K; k += 8, src += 8, dst += 8 * kTWs) cp_async4(dst, src);
+        } else {
+            for (; k < K; k += 8, dst += 8 * kTWs) *dst = 0.f;
         }
     }
     for (int n = t; n < npad; n += kTThreads) {
