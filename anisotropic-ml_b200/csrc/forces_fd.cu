@@ -360,11 +360,19 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
         const int D = m.dims[0];
         const int nr = (int)min((long long)kTRows, rows - r0);
         __syncthreads();  // the previous tile's last layer is done with XT, WT and Bs
-        // the tile's g rows are one contiguous block: coalesced reads
-        for (int idx = t; idx < kTRows * D; idx += kTThreads) {
-            const int rr = idx / D, d = idx - rr * D;
-            if (rr < nr) cp_async4(XT + d * kTLd + tiled_col(rr), g + r0 * D + idx);
-            else XT[d * kTLd + tiled_col(rr)] = 0.f;
+        // the tile's g rows, a warp instruction per 4 rows x 8 columns (four 32-byte
+        // global segments; columns 4 apart in XT, 32 different banks), walked by
+        // pointer increments
+        for (int rb = t >> 5; 4 * rb < kTRows; rb += kTThreads / 32) {
+            const int rr = 4 * rb + (t & 3);
+            int d = (t & 31) >> 2;
+            float *dst = XT + d * kTLd + tiled_col(rr);
+            if (rr < nr) {
+                const float *src = g + (r0 + rr) * D + d;
+                for (; d < D; d += 8, src += 8, dst += 8 * kTLd) cp_async4(dst, src);
+            } else {
+                for (; d < D; d += 8, dst += 8 * kTLd) *dst = 0.f;
+            }
         }
         stage_layer(m, w, 0, WT, Bs);
         cp_async_wait_all();
