@@ -91,6 +91,23 @@ __device__ __forceinline__ void tile_descriptor_row(const float *R, const float 
     nep_descriptor<Cfg>(vp, g.nd, inv_rc, gT + col, ld, pass_mask);
 }
 
+// The tile's 10 x kPT descriptor rows from gT (column v kPT + p, row stride ld,
+// odd) to g_all, where rows v*P + p0 .. p0+valid-1 of variant v are
+// contiguous: a warp per row, lanes over the D columns (coalesced stores,
+// column reads on 32 banks), no index divisions.
+template <int D>
+__device__ __forceinline__ void store_tile_rows(const float *gT, int ld, float *g_out, long long P, long long p0,
+                                                int valid) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int r = warp; r < 10 * kPT; r += nw) {
+        const int v = r / kPT, p = r - v * kPT;
+        if (p >= valid) continue;
+        float *dst = g_out + ((long long)v * P + p0 + p) * D;
+        const float *src = gT + r;
+        for (int d = lane; d < D; d += 32) dst[d] = src[d * ld];
+    }
+}
+
 // ---------------------------------------------------------------- g_all to HBM
 template <class Cfg>
 __global__ void __launch_bounds__(kTileThreads) k_descriptors(const float *pos, const float *quat, float L,
@@ -114,12 +131,7 @@ __global__ void __launch_bounds__(kTileThreads) k_descriptors(const float *pos, 
         tile_descriptor_row<Cfg>(R, t, g, dx, dteta, inv_rc, gT, ld, threadIdx.x, threadIdx.x >> 5);
         __syncthreads();
         int valid = (int)min((long long)kPT, P - p0);
-        // rows v*P + p0 .. p0+valid-1 of variant v are contiguous in g_all
-        for (int idx = threadIdx.x; idx < 10 * kPT * Cfg::D; idx += blockDim.x) {
-            int v = idx / (kPT * Cfg::D), rem = idx - v * kPT * Cfg::D;
-            int p = rem / Cfg::D, d = rem - p * Cfg::D;
-            if (p < valid) g_out[((long long)v * P + p0 + p) * Cfg::D + d] = gT[d * ld + v * kPT + p];
-        }
+        store_tile_rows<Cfg::D>(gT, ld, g_out, P, p0, valid);
         __syncthreads();
     }
 }
@@ -224,12 +236,7 @@ __global__ void __launch_bounds__(kTileThreads) k_descriptors_direct(const float
         direct_row_descriptor<NR, NA, LM>(vp, g.nd, inv_rc, cloud + threadIdx.x, kTileThreads, gT + threadIdx.x, ld);
         __syncthreads();
         int valid = (int)min((long long)kPT, P - p0);
-        // rows v*P + p0 .. p0+valid-1 of variant v are contiguous in g_all
-        for (int idx = threadIdx.x; idx < 10 * kPT * D; idx += blockDim.x) {
-            int vv = idx / (kPT * D), rem = idx - vv * kPT * D;
-            int pp = rem / D, d = rem - pp * D;
-            if (pp < valid) g_out[((long long)vv * P + p0 + pp) * D + d] = gT[d * ld + vv * kPT + pp];
-        }
+        store_tile_rows<D>(gT, ld, g_out, P, p0, valid);
         __syncthreads();
     }
 }
