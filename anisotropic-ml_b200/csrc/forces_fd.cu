@@ -309,8 +309,9 @@ __global__ void __launch_bounds__(kMlpRows) k_mlp(const float *g, long long rows
 // multiply-adds, the next k's operands loading while this k's multiply-adds
 // issue. Narrower layers take columns cg, cg + 32, ... below npad. The outputs
 // stay in registers until every thread has read the layer's inputs, then
-// overwrite them. Each output is bias + sum_k x_k w_k in ascending k, one
-// rounding per multiply-add.
+// overwrite them. Each hidden output is bias + sum_k x_k w_k in ascending k, one
+// rounding per multiply-add; the energy (the one-column output layer) is the
+// bias plus the 32 column groups' partial sums over k = cg, cg + 32, ...
 constexpr int kTRows = 128, kTThreads = 512, kTMaxW = 160, kTGroups = kTThreads / 16;
 constexpr int kTMaxCw = kTMaxW / kTGroups;  // outputs per row and thread: 5
 constexpr int kTLd = kTRows + 4;  // activation row stride (16-byte aligned rows)
@@ -388,9 +389,37 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
             const int K = m.dims[L], N = m.dims[L + 1];
             const int npad = (N + 15) / 16 * 16;
             const bool last = L == m.n_layers - 1, wide = npad == kTMaxW;
+            const float *xk = XT + 4 * rg;
+            if (last) {
+                // the output layer (one column, N = 1): the 32 column groups split k (group
+                // cg sums k = cg, cg + 32, ... in ascending order over its 8 rows), the
+                // partial sums meet in the activation buffer and add up in group order
+                // after the bias
+                float part[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) part[i] = 0.f;
+                for (int k = cg; k < K; k += kTGroups) {
+                    const float4 x0 = *reinterpret_cast<const float4 *>(xk + k * kTLd);
+                    const float4 x1 = *reinterpret_cast<const float4 *>(xk + k * kTLd + kTRows / 2);
+                    const float wv = WT[k * kTWs];
+                    const float xs[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) part[i] = fmaf(xs[i], wv, part[i]);
+                }
+                __syncthreads();  // every thread has read the layer's inputs
+                float *sp = XT + cg * kTRows + 8 * rg;  // [group][row], rows 8 rg .. 8 rg + 7
+                *reinterpret_cast<float4 *>(sp) = make_float4(part[0], part[1], part[2], part[3]);
+                *reinterpret_cast<float4 *>(sp + 4) = make_float4(part[4], part[5], part[6], part[7]);
+                __syncthreads();
+                if (t < nr) {
+                    float e = Bs[0];
+                    for (int gq = 0; gq < kTGroups; ++gq) e += XT[gq * kTRows + t];
+                    e_out[r0 + t] = e;
+                }
+                break;
+            }
             const int ncol = wide ? kTMaxCw : (npad - cg + kTGroups - 1) / kTGroups;  // this thread's columns
             float acc[8][kTMaxCw];
-            const float *xk = XT + 4 * rg;
             if (wide) {
 #pragma unroll
                 for (int c = 0; c < kTMaxCw; ++c) {
@@ -430,7 +459,7 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
                         fma40(b);
                     }
                 }
-            } else if (ncol == 1) {  // one column (the last layer, N = 1: column cg < 16)
+            } else if (ncol == 1) {  // one column (a hidden layer of width 16 or less: column cg < 16)
 #pragma unroll
                 for (int i = 0; i < 8; ++i) acc[i][0] = Bs[cg];
                 const float *px = xk, *pw = WT + cg;
@@ -462,16 +491,6 @@ __global__ void __launch_bounds__(kTThreads) k_mlp_tiled(const float *g, long lo
                         }
                     }
                 }
-            }
-            if (last) {  // the output column 0 (the energy): thread group cg = 0 in either layout
-                if (cg == 0) {
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const int rr = 8 * rg + i;
-                        if (rr < nr) e_out[r0 + rr] = acc[i][0];
-                    }
-                }
-                break;
             }
             __syncthreads();  // every thread has read this layer's inputs and weights
             stage_layer(m, w, L + 1, WT, Bs);  // in flight while the outputs are written
